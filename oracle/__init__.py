@@ -1,0 +1,268 @@
+"""Test infrastructure only: Python access to the two CPU checkers of the Gaussian FIR path.
+
+* ``liboracle_gauss.so`` -- the plain-C restatement in ``gauss_oracle.c`` (always built).
+* ``_ref/libdipref.so`` -- the unmodified DIPlib sources compiled by ``oracle/Makefile``, reached
+  through ``ref_shim.cpp`` (only where the reference tree was present at build time).
+
+Nothing in the product imports this package; ``tests/``, ``__graft_entry__.smoke()`` and
+``bench.py``'s CPU-baseline leg use it as the checker.
+
+Arrays are numpy arrays in numpy axis order (slowest first).  Like PyDIP
+(pydip/src/image.cpp:25-33,148-151) the DIPlib axis order is the reverse, and per-axis
+parameters (sigmas, orders, boundary conditions) are listed x first.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_LIB = os.path.join(HERE, "liboracle_gauss.so")
+REF_LIB = os.path.join(HERE, "_ref", "libdipref.so")
+
+DTYPE_CODES = {
+    np.dtype(np.bool_): 0, np.dtype(np.uint8): 1, np.dtype(np.uint16): 2, np.dtype(np.uint32): 3,
+    np.dtype(np.uint64): 4, np.dtype(np.int8): 5, np.dtype(np.int16): 6, np.dtype(np.int32): 7,
+    np.dtype(np.int64): 8, np.dtype(np.float32): 9, np.dtype(np.float64): 10,
+}
+CODE_DTYPES = {v: k for k, v in DTYPE_CODES.items()}
+
+# dip::BoundaryCondition enumerators and their strings (include/diplib/boundary.h:65-109,
+# include/diplib/library/stringparams.h:259-272).
+BC_CODES = {
+    "": 0, "default": 0, "mirror": 0, "asym mirror": 1, "antisym reflect": 2, "periodic": 3,
+    "asym periodic": 4, "add zeros": 5, "add max": 6, "add min": 7, "zero order": 8,
+    "first order": 9, "second order": 10, "third order": 11, "already expanded": 12,
+}
+
+_i64p = ctypes.POINTER(ctypes.c_int64)
+
+
+def _load(path):
+    if not os.path.exists(path):
+        return None
+    return ctypes.CDLL(path)
+
+
+_oracle = None
+_ref = None
+
+
+def oracle_lib():
+    global _oracle
+    if _oracle is None:
+        _oracle = _load(ORACLE_LIB)
+        if _oracle is None:
+            raise RuntimeError(f"{ORACLE_LIB} is not built (run `make -C oracle`)")
+        _oracle.or_gauss_fir.restype = ctypes.c_int
+        _oracle.or_make_half_gaussian.restype = ctypes.c_int
+        _oracle.or_make_half_gaussian.argtypes = [ctypes.c_double, ctypes.c_uint, ctypes.c_double, ctypes.c_int,
+                                                  ctypes.c_void_p, ctypes.c_int]
+        _oracle.or_half_gaussian_size.restype = ctypes.c_size_t
+        _oracle.or_half_gaussian_size.argtypes = [ctypes.c_double, ctypes.c_uint, ctypes.c_double, ctypes.c_int]
+        for fn in (_oracle.or_expand_buffer_f32, _oracle.or_expand_buffer_f64):
+            fn.restype = ctypes.c_int
+            fn.argtypes = [ctypes.c_void_p, ctypes.c_ssize_t, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_size_t,
+                           ctypes.c_int]
+    return _oracle
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_LIB)
+
+
+def ref_lib():
+    global _ref
+    if _ref is None:
+        _ref = _load(REF_LIB)
+        if _ref is None:
+            raise RuntimeError(f"{REF_LIB} is not built (run `make -C oracle ref` where the reference tree exists)")
+        _ref.dipref_half_gaussian.argtypes = [ctypes.c_double, ctypes.c_uint32, ctypes.c_double, ctypes.c_int,
+                                              ctypes.c_void_p, ctypes.c_int]
+        _ref.dipref_expand_buffer.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_uint64,
+                                              ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int]
+        _ref.dipref_max_gauss_truncation.restype = ctypes.c_double
+        _ref.dipref_structure_tensor.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _i64p, ctypes.c_double,
+                                                 ctypes.c_double, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_double,
+                                                 ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.c_char_p,
+                                                 ctypes.c_int]
+    return _ref
+
+
+def bc_code(bc: str) -> int:
+    if bc not in BC_CODES:
+        raise ValueError("Boundary condition not recognized: " + bc)
+    return BC_CODES[bc]
+
+
+def suggest_flex(dtype) -> np.dtype:
+    """DataType::SuggestFlex (src/library/datatype.cpp:109-124) for real types."""
+    dt = np.dtype(dtype)
+    if dt in (np.dtype(np.uint32), np.dtype(np.int32), np.dtype(np.uint64), np.dtype(np.int64),
+              np.dtype(np.float64)):
+        return np.dtype(np.float64)
+    return np.dtype(np.float32)
+
+
+def _dip_geometry(a: np.ndarray):
+    """DIPlib sizes/strides (x first, in samples) of a numpy array."""
+    sizes = (ctypes.c_int64 * a.ndim)(*reversed(a.shape))
+    strides = (ctypes.c_int64 * a.ndim)(*(s // a.itemsize for s in reversed(a.strides)))
+    return sizes, strides
+
+
+def _broadcast(values, nd, default):
+    """ArrayUseParameter: 0 entries -> default, 1 entry -> broadcast, nd entries -> as is."""
+    values = list(values) if values is not None else []
+    if len(values) == 0:
+        return [default] * nd
+    if len(values) == 1:
+        return values * nd
+    if len(values) != nd:
+        raise ValueError("Array parameter has the wrong number of elements")
+    return values
+
+
+# ------------------------------------------------------------------------------------------------
+# The C restatement
+# ------------------------------------------------------------------------------------------------
+
+def half_gaussian(sigma: float, order: int, truncation: float = 3.0, dt_double: bool = False) -> np.ndarray:
+    lib = oracle_lib()
+    n = lib.or_make_half_gaussian(sigma, order, truncation, int(dt_double), None, 0)
+    if n < 0:
+        raise ValueError("Gaussian FIR filter not implemented for order > 3")
+    out = np.zeros(n, np.float64)
+    lib.or_make_half_gaussian(sigma, order, truncation, int(dt_double), out.ctypes.data, n)
+    return out
+
+
+def expand_buffer(line: np.ndarray, left: int, right: int, bc: str) -> np.ndarray:
+    """Returns `line` extended by `left`/`right` samples with boundary condition `bc`."""
+    line = np.ascontiguousarray(line)
+    buf = np.zeros(left + line.size + right, line.dtype)
+    buf[left:left + line.size] = line
+    fn = oracle_lib().or_expand_buffer_f64 if line.dtype == np.float64 else oracle_lib().or_expand_buffer_f32
+    ptr = buf.ctypes.data + left * buf.itemsize
+    st = fn(ptr, 1, line.size, left, right, bc_code(bc))
+    if st != 0:
+        raise RuntimeError(f"or_expand_buffer failed ({st})")
+    return buf
+
+
+def gauss_fir(x: np.ndarray, sigmas: Sequence[float] = (1.0,), orders: Sequence[int] = (0,),
+              bcs: Sequence[str] = (), truncation: float = 3.0, out_dtype=None) -> np.ndarray:
+    """The restated dip::GaussFIR on a numpy array (parameters in DIPlib order, x first)."""
+    nd = x.ndim
+    sig = _broadcast(sigmas, nd, 1.0)
+    ords = _broadcast(orders, nd, 0)
+    bcl = _broadcast(bcs, nd, "mirror")
+    out_dt = suggest_flex(x.dtype) if out_dtype is None else np.dtype(out_dtype)
+    out = np.zeros(x.shape, out_dt)
+    sizes, in_strides = _dip_geometry(x)
+    _, out_strides = _dip_geometry(out)
+    st = oracle_lib().or_gauss_fir(
+        ctypes.c_void_p(x.ctypes.data), DTYPE_CODES[x.dtype], nd, sizes, in_strides,
+        ctypes.c_void_p(out.ctypes.data), DTYPE_CODES[out_dt], out_strides,
+        (ctypes.c_double * nd)(*sig), (ctypes.c_uint * nd)(*ords), (ctypes.c_int * nd)(*[bc_code(b) for b in bcl]),
+        ctypes.c_double(truncation))
+    if st == 1:
+        raise ValueError("Gaussian FIR filter not implemented for order > 3")
+    if st != 0:
+        raise RuntimeError(f"or_gauss_fir failed ({st})")
+    return out
+
+
+def structure_tensor(x: np.ndarray, grad_sigma: float, tensor_sigma: float, bc: str = "mirror",
+                     truncation: float = 3.0) -> np.ndarray:
+    """dip::StructureTensor (src/analysis/structure_tensor.cpp:33-59) built from the restated
+    GaussFIR: gradient (order 1 along each axis), products g_i g_j, smoothing of each product.
+    Returns an array of shape (ncomp,) + x.shape with DIPlib's symmetric-matrix component order
+    (diagonal first, then the upper triangle row by row)."""
+    nd = x.ndim
+    grads = []
+    for d in range(nd):  # d in DIPlib order
+        o = [0] * nd
+        o[d] = 1
+        grads.append(gauss_fir(x, [grad_sigma] * nd, o, [bc], truncation))
+    pairs = [(i, i) for i in range(nd)] + [(i, j) for i in range(nd) for j in range(i + 1, nd)]
+    comps = [gauss_fir((grads[i] * grads[j]).astype(grads[0].dtype), [tensor_sigma] * nd, [0] * nd, [bc], truncation)
+             for i, j in pairs]
+    return np.stack(comps)
+
+
+# ------------------------------------------------------------------------------------------------
+# The reference itself
+# ------------------------------------------------------------------------------------------------
+
+def ref_set_threads(n: int) -> int:
+    return ref_lib().dipref_set_threads(n)
+
+
+def ref_half_gaussian(sigma: float, order: int, truncation: float = 3.0, dt_double: bool = False) -> np.ndarray:
+    lib = ref_lib()
+    buf = np.zeros(4096, np.float64)
+    n = lib.dipref_half_gaussian(sigma, order, truncation, int(dt_double), buf.ctypes.data, buf.size)
+    if n < 0:
+        raise ValueError("MakeHalfGaussian failed")
+    return buf[:n].copy()
+
+
+def ref_expand_buffer(line: np.ndarray, left: int, right: int, bc: str) -> np.ndarray:
+    line = np.ascontiguousarray(line)
+    buf = np.zeros(left + line.size + right, line.dtype)
+    buf[left:left + line.size] = line
+    st = ref_lib().dipref_expand_buffer(buf.ctypes.data + left * buf.itemsize, DTYPE_CODES[line.dtype], 1,
+                                        line.size, left, right, bc_code(bc))
+    if st != 0:
+        raise RuntimeError("ExpandBuffer failed")
+    return buf
+
+
+def ref_gauss(x: np.ndarray, sigmas: Sequence[float] = (1.0,), orders: Sequence[int] = (0,),
+              bcs: Sequence[str] | None = None, truncation: float = 3.0, method: str = "FIR",
+              out_dtype=None, strides: Sequence[int] | None = None) -> np.ndarray:
+    """dip::Gauss of the reference on a numpy array.  `bcs=None` passes an empty array.  With
+    `out_dtype` the output is a protected image of that type (the reference's protected path)."""
+    nd = x.ndim
+    sizes, st = _dip_geometry(x)
+    errbuf = ctypes.create_string_buffer(512)
+    sig = list(sigmas)
+    ords = list(orders)
+    bc_str = "\n".join(bcs) if bcs else ""
+    protect = out_dtype is not None
+    res_dt = np.dtype(out_dtype) if protect else suggest_flex(x.dtype)
+    out = np.zeros(x.shape, res_dt)
+    code = ctypes.c_int(DTYPE_CODES[res_dt])
+    rc = ref_lib().dipref_gauss(
+        ctypes.c_void_p(x.ctypes.data), DTYPE_CODES[x.dtype], nd, sizes, st,
+        (ctypes.c_double * max(1, len(sig)))(*sig), len(sig), (ctypes.c_uint32 * max(1, len(ords)))(*ords), len(ords),
+        bc_str.encode(), int(bcs is not None and len(bcs) > 0), ctypes.c_double(truncation), method.encode(),
+        ctypes.c_void_p(out.ctypes.data), ctypes.byref(code), int(protect), errbuf, 512)
+    if rc != 0:
+        raise RuntimeError(errbuf.value.decode())
+    if not protect and code.value != DTYPE_CODES[res_dt]:
+        raise RuntimeError(f"unexpected output type code {code.value}")
+    return out
+
+
+def ref_structure_tensor(x: np.ndarray, grad_sigma: float, tensor_sigma: float, bc: str = "mirror",
+                         truncation: float = 3.0, method: str = "gaussFIR") -> np.ndarray:
+    """dip::StructureTensor of the reference; returns (ncomp,) + x.shape."""
+    nd = x.ndim
+    ncomp = nd * (nd + 1) // 2
+    sizes, _ = _dip_geometry(x)
+    x = np.ascontiguousarray(x)
+    res_dt = suggest_flex(x.dtype)
+    out = np.zeros(x.shape + (ncomp,), res_dt)
+    code = ctypes.c_int(0)
+    errbuf = ctypes.create_string_buffer(512)
+    rc = ref_lib().dipref_structure_tensor(x.ctypes.data, DTYPE_CODES[x.dtype], nd, sizes, grad_sigma, tensor_sigma,
+                                           method.encode(), bc.encode(), truncation, out.ctypes.data,
+                                           ctypes.byref(code), errbuf, 512)
+    if rc != 0:
+        raise RuntimeError(errbuf.value.decode() or "StructureTensor failed")
+    return np.moveaxis(out, -1, 0).copy()

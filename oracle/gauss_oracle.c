@@ -1,0 +1,579 @@
+/* Test infrastructure only: plain-C restatement of DIPlib's Gaussian FIR path (the parity
+ * oracle).  Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg load it, and
+ * only as a checker.  Every function cites the reference code it restates; the floating-point
+ * operation order follows the reference so that, compiled without FMA contraction
+ * (-ffp-contract=off), results are bit-identical to the reference's own x86-64 build.
+ *
+ * Parity of this file is pinned against the reference itself (oracle/_ref/libdipref.so) and
+ * against fixtures generated from it (tests/golden/).
+ */
+#include "gauss_oracle.h"
+
+#include <float.h>
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define OR_PI 3.14159265358979323846264338327950288 /* dip::pi, include/diplib/library/numeric.h */
+
+/* ------------------------------------------------------------------------------------------ */
+/* Kernel weights                                                                             */
+/* ------------------------------------------------------------------------------------------ */
+
+/* maximum_gauss_truncation<T>(), include/diplib/library/numeric.h:69-76. */
+static double max_gauss_truncation( int dt_double ) {
+   return sqrt( -2.0 * log( dt_double ? DBL_EPSILON : (double)FLT_EPSILON ));
+}
+
+/* HalfGaussianSize, src/linear/gauss.cpp:38-51 (clamp_cast<dip::uint>(double) clamps at 0). */
+size_t or_half_gaussian_size( double sigma, unsigned order, double truncation, int dt_double ) {
+   if( truncation <= 0 ) {
+      truncation = 3;
+   }
+   double max_trunc = max_gauss_truncation( dt_double );
+   truncation = ( max_trunc < truncation ) ? max_trunc : truncation; /* std::min */
+   truncation += 0.5 * (double)order;
+   double v = ceil( truncation * sigma );
+   if( !( v > 0.0 )) {
+      return 0;
+   }
+   return (size_t)v;
+}
+
+/* MakeHalfGaussianInternal + MakeHalfGaussian, src/linear/gauss.cpp:53-165.  The half kernel
+ * has x=0 at the right end (index r0). */
+int or_make_half_gaussian( double sigma, unsigned order, double truncation, int dt_double, double* filter, int cap ) {
+   if( sigma == 0.0 ) {
+      if( cap >= 1 ) { filter[ 0 ] = 1.0; }
+      return 1;
+   }
+   if( order > 3 ) {
+      return -1;
+   }
+   size_t halfFilterSize = 1 + or_half_gaussian_size( sigma, order, truncation, dt_double );
+   if( order > 2 && halfFilterSize < 2 ) {
+      halfFilterSize = 2;
+   }
+   if( (size_t)cap < halfFilterSize ) {
+      return (int)halfFilterSize; /* caller retries with a larger buffer */
+   }
+   size_t r0 = halfFilterSize - 1;
+   double sigma2 = sigma * sigma;
+   switch( order ) {
+      case 0: {
+         double factor = -0.5 / sigma2;
+         double normalization = 0;
+         filter[ r0 ] = 1.0;
+         for( size_t rr = 1; rr < halfFilterSize; rr++ ) {
+            double rad = (double)rr;
+            double g = exp( factor * ( rad * rad ));
+            filter[ r0 - rr ] = g;
+            normalization += g;
+         }
+         normalization = 1.0 / ( normalization * 2 + 1 );
+         for( size_t rr = 0; rr < halfFilterSize; rr++ ) {
+            filter[ rr ] *= normalization;
+         }
+         break;
+      }
+      case 1: {
+         double factor = -0.5 / sigma2;
+         double moment = 0.0;
+         filter[ r0 ] = 0.0;
+         for( size_t rr = 1; rr < halfFilterSize; rr++ ) {
+            double rad = (double)rr;
+            double g = rad * exp( factor * ( rad * rad ));
+            filter[ r0 - rr ] = g;
+            moment += rad * g;
+         }
+         double normalization = 1.0 / ( 2.0 * moment );
+         for( size_t rr = 0; rr < halfFilterSize - 1; rr++ ) {
+            filter[ rr ] *= normalization;
+         }
+         break;
+      }
+      case 2: {
+         double norm = 1.0 / ( sqrt( 2.0 * OR_PI ) * sigma * sigma2 );
+         double mean = 0.0;
+         filter[ r0 ] = -norm;
+         for( size_t rr = 1; rr < halfFilterSize; rr++ ) {
+            double rad = (double)rr;
+            double sr2 = rad * rad / sigma2;
+            double g = ( sr2 - 1.0 ) * norm * exp( -0.5 * sr2 );
+            filter[ r0 - rr ] = g;
+            mean += g;
+         }
+         mean = ( mean * 2.0 + filter[ r0 ] ) / ( (double)r0 * 2.0 + 1.0 );
+         filter[ r0 ] -= mean;
+         double moment = 0.0;
+         for( size_t rr = 1; rr < halfFilterSize; rr++ ) {
+            double rad = (double)rr;
+            filter[ r0 - rr ] -= mean;
+            moment += rad * rad * filter[ r0 - rr ];
+         }
+         double normalization = 1.0 / moment;
+         for( size_t rr = 0; rr < halfFilterSize; rr++ ) {
+            filter[ rr ] *= normalization;
+         }
+         break;
+      }
+      case 3: {
+         double norm = 1.0 / ( sqrt( 2.0 * OR_PI ) * sigma * sigma2 * sigma2 );
+         filter[ r0 ] = 0.0;
+         double moment = 0.0;
+         for( size_t rr = 1; rr < halfFilterSize; rr++ ) {
+            double rad = (double)rr;
+            double rr2 = rad * rad;
+            double sr2 = rr2 / sigma2;
+            double g = norm * exp( -0.5 * sr2 ) * ( rad * ( 3.0 - sr2 ));
+            filter[ r0 - rr ] = g;
+            moment += g * rr2 * rad;
+         }
+         double normalization = 3.0 / moment;
+         for( size_t rr = 0; rr < halfFilterSize; rr++ ) {
+            filter[ rr ] *= normalization;
+         }
+         break;
+      }
+   }
+   return (int)halfFilterSize;
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* Boundary extension: detail::ExpandBuffer, src/library/copy_buffer.cpp:359-813               */
+/* The reference walks pointers; the index walks below visit the same samples in the same      */
+/* order.  Instantiated for float and double buffers (the only buffer types on this path).     */
+/* ------------------------------------------------------------------------------------------ */
+
+#define OR_DEFINE_EXPAND( T, SUFFIX, TMAX )                                                                 \
+static void expand_constant_##SUFFIX( T* b, ptrdiff_t s, size_t n, size_t left, size_t right, T lv, T rv ) { \
+   /* ExpandBufferConstant, copy_buffer.cpp:360-379 */                                                     \
+   for( size_t ii = 0; ii < left; ++ii ) { b[ -(ptrdiff_t)( ii + 1 ) * s ] = lv; }                        \
+   for( size_t ii = 0; ii < right; ++ii ) { b[ (ptrdiff_t)( n + ii ) * s ] = rv; }                       \
+}                                                                                                          \
+static void expand_first_##SUFFIX( T* b, ptrdiff_t s, size_t n, size_t left, size_t right ) {             \
+   /* ExpandBufferFirstOrder, copy_buffer.cpp:386-417 */                                                   \
+   if( left > 0 ) {                                                                                        \
+      double d0 = (double)b[ 0 ];                                                                          \
+      double d1 = d0 / (double)( left + 1 );                                                               \
+      for( size_t ii = 0; ii < left; ii++ ) { d0 -= d1; b[ -(ptrdiff_t)( ii + 1 ) * s ] = (T)d0; }          \
+   }                                                                                                       \
+   if( right > 0 ) {                                                                                       \
+      double d0 = (double)b[ (ptrdiff_t)( n - 1 ) * s ];                                                   \
+      double d1 = d0 / (double)( right + 1 );                                                              \
+      for( size_t ii = 0; ii < right; ii++ ) { d0 -= d1; b[ (ptrdiff_t)( n + ii ) * s ] = (T)d0; }          \
+   }                                                                                                       \
+}                                                                                                          \
+static void expand_second_##SUFFIX( T* b, ptrdiff_t s, size_t n, size_t left, size_t right ) {            \
+   /* ExpandBufferSecondOrder, copy_buffer.cpp:423-458 */                                                  \
+   if( left > 0 ) {                                                                                        \
+      double bb = (double)left + 1.0;                                                                      \
+      double d0 = (double)b[ 0 ];                                                                          \
+      double f1 = (double)b[ s ];                                                                          \
+      double d1 = ( bb - 1.0 ) / bb * d0 - bb / ( bb + 1.0 ) * f1;                                         \
+      double d2 = -1.0 / bb * d0 + 1.0 / ( bb + 1.0 ) * f1;                                                \
+      for( size_t ii = 1; ii <= left; ii++ ) {                                                             \
+         double x = (double)ii;                                                                            \
+         b[ -(ptrdiff_t)ii * s ] = (T)( d0 + x * d1 + x * x * d2 );                                        \
+      }                                                                                                    \
+   }                                                                                                       \
+   if( right > 0 ) {                                                                                       \
+      double bb = (double)right + 1.0;                                                                     \
+      double d0 = (double)b[ (ptrdiff_t)( n - 1 ) * s ];                                                   \
+      double f1 = (double)b[ (ptrdiff_t)( n - 2 ) * s ];                                                   \
+      double d1 = ( bb - 1.0 ) / bb * d0 - bb / ( bb + 1.0 ) * f1;                                         \
+      double d2 = -1.0 / bb * d0 + 1.0 / ( bb + 1.0 ) * f1;                                                \
+      for( size_t ii = 1; ii <= right; ii++ ) {                                                            \
+         double x = (double)ii;                                                                            \
+         b[ (ptrdiff_t)( n - 1 + ii ) * s ] = (T)( d0 + x * d1 + x * x * d2 );                             \
+      }                                                                                                    \
+   }                                                                                                       \
+}                                                                                                          \
+static void expand_third_##SUFFIX( T* b, ptrdiff_t s, size_t n, size_t left, size_t right ) {             \
+   /* ExpandBufferThirdOrder, copy_buffer.cpp:469-513 */                                                   \
+   if( left > 0 ) {                                                                                        \
+      double bb = (double)left + 1.0;                                                                      \
+      double b12 = ( bb + 1 ) * ( bb + 1 );                                                                \
+      double d0 = (double)b[ 0 ];                                                                          \
+      double f1 = (double)b[ s ];                                                                          \
+      double d1 = -( 2.0 * d0 ) / bb + d0 - ( bb * bb * f1 ) / b12;                                        \
+      double d2 = ( 2.0 * bb * f1 ) / b12 - ( d0 * ( 2.0 * bb - 1.0 )) / ( bb * bb );                      \
+      double d3 = d0 / ( bb * bb ) - f1 / b12;                                                             \
+      for( size_t ii = 1; ii <= left; ii++ ) {                                                             \
+         double x = (double)ii;                                                                            \
+         b[ -(ptrdiff_t)ii * s ] = (T)( d0 + x * d1 + x * x * d2 + x * x * x * d3 );                       \
+      }                                                                                                    \
+   }                                                                                                       \
+   if( right > 0 ) {                                                                                       \
+      double bb = (double)right + 1.0;                                                                     \
+      double b12 = ( bb + 1 ) * ( bb + 1 );                                                                \
+      double d0 = (double)b[ (ptrdiff_t)( n - 1 ) * s ];                                                   \
+      double f1 = (double)b[ (ptrdiff_t)( n - 2 ) * s ];                                                   \
+      double d1 = -( 2.0 * d0 ) / bb + d0 - ( bb * bb * f1 ) / b12;                                        \
+      double d2 = ( 2.0 * bb * f1 ) / b12 - ( d0 * ( 2.0 * bb - 1.0 )) / ( bb * bb );                      \
+      double d3 = d0 / ( bb * bb ) - f1 / b12;                                                             \
+      for( size_t ii = 1; ii <= right; ii++ ) {                                                            \
+         double x = (double)ii;                                                                            \
+         b[ (ptrdiff_t)( n - 1 + ii ) * s ] = (T)( d0 + x * d1 + x * x * d2 + x * x * x * d3 );            \
+      }                                                                                                    \
+   }                                                                                                       \
+}                                                                                                          \
+static void expand_mirror_##SUFFIX( T* b, ptrdiff_t s, size_t n, size_t left, size_t right, int asym ) {   \
+   /* ExpandBufferMirror, copy_buffer.cpp:516-549: bounce between the two end samples */                  \
+   ptrdiff_t last = (ptrdiff_t)n - 1;                                                                      \
+   ptrdiff_t in = 0;                                                                                       \
+   int sign = -1;                                                                                          \
+   for( size_t ii = 0; ii < left; ii++ ) {                                                                 \
+      in -= sign;                                                                                          \
+      T v = b[ in * s ];                                                                                   \
+      b[ -(ptrdiff_t)( ii + 1 ) * s ] = ( asym && sign < 0 ) ? -v : v;                                     \
+      if( in == last || in == 0 ) { sign = -sign; }                                                        \
+   }                                                                                                       \
+   in = last;                                                                                              \
+   sign = -1;                                                                                              \
+   for( size_t ii = 0; ii < right; ii++ ) {                                                                \
+      in += sign;                                                                                          \
+      T v = b[ in * s ];                                                                                   \
+      b[ ( last + 1 + (ptrdiff_t)ii ) * s ] = ( asym && sign < 0 ) ? -v : v;                               \
+      if( in == last || in == 0 ) { sign = -sign; }                                                        \
+   }                                                                                                       \
+}                                                                                                          \
+static void expand_antisym_##SUFFIX( T* b, ptrdiff_t s, size_t n, size_t left, size_t right ) {            \
+   /* ExpandBufferAntiSymReflect, copy_buffer.cpp:552-589 */                                               \
+   ptrdiff_t last = (ptrdiff_t)n - 1;                                                                      \
+   ptrdiff_t in = 0, out = 0;                                                                              \
+   int sign = -1;                                                                                          \
+   double offset = (double)b[ out * s ] - sign * (double)b[ in * s ];                                      \
+   for( size_t ii = 0; ii < left; ii++ ) {                                                                 \
+      in -= sign;                                                                                          \
+      out -= 1;                                                                                            \
+      b[ out * s ] = (T)( offset + sign * (double)b[ in * s ] );                                           \
+      if( in == last || in == 0 ) {                                                                        \
+         sign = -sign;                                                                                     \
+         offset = (double)b[ out * s ] - sign * (double)b[ in * s ];                                       \
+      }                                                                                                    \
+   }                                                                                                       \
+   in = last;                                                                                              \
+   out = last;                                                                                             \
+   sign = -1;                                                                                              \
+   offset = (double)b[ out * s ] - sign * (double)b[ in * s ];                                             \
+   for( size_t ii = 0; ii < right; ii++ ) {                                                                \
+      in += sign;                                                                                          \
+      out += 1;                                                                                            \
+      b[ out * s ] = (T)( offset + sign * (double)b[ in * s ] );                                           \
+      if( in == last || in == 0 ) {                                                                        \
+         sign = -sign;                                                                                     \
+         offset = (double)b[ out * s ] - sign * (double)b[ in * s ];                                       \
+      }                                                                                                    \
+   }                                                                                                       \
+}                                                                                                          \
+static void expand_periodic_##SUFFIX( T* b, ptrdiff_t s, size_t n, size_t left, size_t right, int asym ) { \
+   /* ExpandBufferPeriodic, copy_buffer.cpp:592-629 */                                                     \
+   ptrdiff_t last = (ptrdiff_t)n - 1;                                                                      \
+   ptrdiff_t in = last;                                                                                    \
+   int sign = -1;                                                                                          \
+   for( size_t ii = 0; ii < left; ii++ ) {                                                                 \
+      T v = b[ in * s ];                                                                                   \
+      b[ -(ptrdiff_t)( ii + 1 ) * s ] = ( asym && sign < 0 ) ? -v : v;                                     \
+      if( in == 0 ) { in = last; sign = -sign; } else { in -= 1; }                                         \
+   }                                                                                                       \
+   in = 0;                                                                                                 \
+   sign = -1;                                                                                              \
+   for( size_t ii = 0; ii < right; ii++ ) {                                                                \
+      T v = b[ in * s ];                                                                                   \
+      b[ ( last + 1 + (ptrdiff_t)ii ) * s ] = ( asym && sign < 0 ) ? -v : v;                               \
+      if( in == last ) { in = 0; sign = -sign; } else { in += 1; }                                         \
+   }                                                                                                       \
+}                                                                                                          \
+int or_expand_buffer_##SUFFIX( T* b, ptrdiff_t s, size_t n, size_t left, size_t right, int bc ) {          \
+   /* ExpandBufferFromTo, copy_buffer.cpp:632-747 (float buffers: saturated_inv is negation) */            \
+   if( left == 0 && right == 0 ) { return OR_OK; }                                                         \
+   if( n == 0 ) { return OR_ERR_ARG; }                                                                     \
+   switch( bc ) {                                                                                          \
+      case OR_BC_SYMMETRIC_MIRROR:                                                                         \
+         if( n == 1 ) { expand_constant_##SUFFIX( b, s, n, left, right, b[ 0 ], b[ 0 ] ); }                \
+         else { expand_mirror_##SUFFIX( b, s, n, left, right, 0 ); }                                       \
+         return OR_OK;                                                                                     \
+      case OR_BC_ASYMMETRIC_MIRROR:                                                                        \
+         if( n == 1 ) { expand_constant_##SUFFIX( b, s, n, left, right, -b[ 0 ], -b[ 0 ] ); }              \
+         else { expand_mirror_##SUFFIX( b, s, n, left, right, 1 ); }                                       \
+         return OR_OK;                                                                                     \
+      case OR_BC_ANTISYMMETRIC_REFLECT:                                                                    \
+         if( n == 1 ) { expand_constant_##SUFFIX( b, s, n, left, right, b[ 0 ], b[ 0 ] ); }                \
+         else { expand_antisym_##SUFFIX( b, s, n, left, right ); }                                         \
+         return OR_OK;                                                                                     \
+      case OR_BC_PERIODIC:                                                                                 \
+         if( n == 1 ) { expand_constant_##SUFFIX( b, s, n, left, right, b[ 0 ], b[ 0 ] ); }                \
+         else { expand_periodic_##SUFFIX( b, s, n, left, right, 0 ); }                                     \
+         return OR_OK;                                                                                     \
+      case OR_BC_ASYMMETRIC_PERIODIC:                                                                      \
+         if( n == 1 ) { expand_constant_##SUFFIX( b, s, n, left, right, -b[ 0 ], -b[ 0 ] ); }              \
+         else { expand_periodic_##SUFFIX( b, s, n, left, right, 1 ); }                                     \
+         return OR_OK;                                                                                     \
+      case OR_BC_ADD_ZEROS:                                                                                \
+         expand_constant_##SUFFIX( b, s, n, left, right, (T)0, (T)0 );                                     \
+         return OR_OK;                                                                                     \
+      case OR_BC_ADD_MAX_VALUE:                                                                            \
+         expand_constant_##SUFFIX( b, s, n, left, right, TMAX, TMAX );                                     \
+         return OR_OK;                                                                                     \
+      case OR_BC_ADD_MIN_VALUE:                                                                            \
+         expand_constant_##SUFFIX( b, s, n, left, right, -TMAX, -TMAX );                                   \
+         return OR_OK;                                                                                     \
+      case OR_BC_THIRD_ORDER_EXTRAPOLATE:                                                                  \
+         if( n > 1 ) { expand_third_##SUFFIX( b, s, n, left, right ); return OR_OK; }                      \
+         /* fallthrough */                                                                                 \
+      case OR_BC_SECOND_ORDER_EXTRAPOLATE:                                                                 \
+         if( n > 1 ) { expand_second_##SUFFIX( b, s, n, left, right ); return OR_OK; }                     \
+         /* fallthrough */                                                                                 \
+      case OR_BC_FIRST_ORDER_EXTRAPOLATE:                                                                  \
+         expand_first_##SUFFIX( b, s, n, left, right );                                                    \
+         return OR_OK;                                                                                     \
+      case OR_BC_ZERO_ORDER_EXTRAPOLATE:                                                                   \
+         expand_constant_##SUFFIX( b, s, n, left, right, b[ 0 ], b[ (ptrdiff_t)( n - 1 ) * s ] );          \
+         return OR_OK;                                                                                     \
+      default:                                                                                             \
+         return OR_ERR_BC;                                                                                 \
+   }                                                                                                       \
+}
+
+OR_DEFINE_EXPAND( float, f32, FLT_MAX )
+OR_DEFINE_EXPAND( double, f64, DBL_MAX )
+
+/* ------------------------------------------------------------------------------------------ */
+/* Sample access with DIPlib's conversions (clamp_cast, include/diplib/library/clamp_cast.h)   */
+/* ------------------------------------------------------------------------------------------ */
+
+static size_t dtype_size( int dt ) {
+   switch( dt ) {
+      case OR_BIN: case OR_UINT8: case OR_SINT8: return 1;
+      case OR_UINT16: case OR_SINT16: return 2;
+      case OR_UINT32: case OR_SINT32: case OR_SFLOAT: return 4;
+      case OR_UINT64: case OR_SINT64: case OR_DFLOAT: return 8;
+      default: return 0;
+   }
+}
+
+/* The value of a sample as a double.  Exact for every type except 64-bit integers above 2^53,
+ * where the reference's static_cast< dfloat > rounds identically. */
+static double get_sample( void const* p, int dt, ptrdiff_t idx ) {
+   switch( dt ) {
+      case OR_BIN: return ( (uint8_t const*)p )[ idx ] ? 1.0 : 0.0;
+      case OR_UINT8: return ( (uint8_t const*)p )[ idx ];
+      case OR_UINT16: return ( (uint16_t const*)p )[ idx ];
+      case OR_UINT32: return ( (uint32_t const*)p )[ idx ];
+      case OR_UINT64: return (double)( (uint64_t const*)p )[ idx ];
+      case OR_SINT8: return ( (int8_t const*)p )[ idx ];
+      case OR_SINT16: return ( (int16_t const*)p )[ idx ];
+      case OR_SINT32: return ( (int32_t const*)p )[ idx ];
+      case OR_SINT64: return (double)( (int64_t const*)p )[ idx ];
+      case OR_SFLOAT: return ( (float const*)p )[ idx ];
+      case OR_DFLOAT: return ( (double const*)p )[ idx ];
+      default: return 0.0;
+   }
+}
+
+/* clamp_cast< outT >( v ): clamp to the target range, then static_cast (truncation toward 0). */
+#define OR_CLAMP( v, lo, hi ) ( ( v ) < ( lo ) ? ( lo ) : ( ( v ) > ( hi ) ? ( hi ) : ( v )))
+static void put_sample( void* p, int dt, ptrdiff_t idx, double v ) {
+   switch( dt ) {
+      case OR_BIN: ( (uint8_t*)p )[ idx ] = ( v != 0.0 ); break;
+      case OR_UINT8: ( (uint8_t*)p )[ idx ] = (uint8_t)OR_CLAMP( v, 0.0, 255.0 ); break;
+      case OR_UINT16: ( (uint16_t*)p )[ idx ] = (uint16_t)OR_CLAMP( v, 0.0, 65535.0 ); break;
+      case OR_UINT32: ( (uint32_t*)p )[ idx ] = (uint32_t)OR_CLAMP( v, 0.0, 4294967295.0 ); break;
+      case OR_UINT64: ( (uint64_t*)p )[ idx ] = (uint64_t)OR_CLAMP( v, 0.0, 18446744073709549568.0 ); break;
+      case OR_SINT8: ( (int8_t*)p )[ idx ] = (int8_t)OR_CLAMP( v, -128.0, 127.0 ); break;
+      case OR_SINT16: ( (int16_t*)p )[ idx ] = (int16_t)OR_CLAMP( v, -32768.0, 32767.0 ); break;
+      case OR_SINT32: ( (int32_t*)p )[ idx ] = (int32_t)OR_CLAMP( v, -2147483648.0, 2147483647.0 ); break;
+      case OR_SINT64: ( (int64_t*)p )[ idx ] = (int64_t)OR_CLAMP( v, -9223372036854775808.0, 9223372036854774784.0 ); break;
+      case OR_SFLOAT: ( (float*)p )[ idx ] = (float)v; break;
+      case OR_DFLOAT: ( (double*)p )[ idx ] = v; break;
+      default: break;
+   }
+}
+
+/* DataType::SuggestFlex, src/library/datatype.cpp:109-124 (real types only). */
+int or_suggest_flex( int dt ) {
+   switch( dt ) {
+      case OR_UINT32: case OR_SINT32: case OR_UINT64: case OR_SINT64: case OR_DFLOAT:
+         return OR_DFLOAT;
+      default:
+         return OR_SFLOAT;
+   }
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* The line filter: SeparableConvolutionLineFilter::Filter, src/linear/convolution.cpp:184-241 */
+/* EVEN and ODD cases, with the filter reversed as InternOneDimensionalFilter does (:76-156):  */
+/* f[0] is the centre tap, f[k] the tap at distance k.                                         */
+/* ------------------------------------------------------------------------------------------ */
+
+static void line_filter_f32( float const* in, float* out, size_t length, float const* f, size_t dataSize, int odd ) {
+   for( size_t ii = 0; ii < length; ++ii ) {
+      float const* c = in + ii;
+      float sum = f[ 0 ] * c[ 0 ];
+      for( size_t k = 1; k < dataSize; ++k ) {
+         sum += f[ k ] * ( odd ? ( c[ k ] - c[ -(ptrdiff_t)k ] ) : ( c[ k ] + c[ -(ptrdiff_t)k ] ));
+      }
+      out[ ii ] = sum;
+   }
+}
+
+static void line_filter_f64( double const* in, double* out, size_t length, double const* f, size_t dataSize, int odd ) {
+   for( size_t ii = 0; ii < length; ++ii ) {
+      double const* c = in + ii;
+      double sum = f[ 0 ] * c[ 0 ];
+      for( size_t k = 1; k < dataSize; ++k ) {
+         sum += f[ k ] * ( odd ? ( c[ k ] - c[ -(ptrdiff_t)k ] ) : ( c[ k ] + c[ -(ptrdiff_t)k ] ));
+      }
+      out[ ii ] = sum;
+   }
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* GaussFIR -> SeparableConvolution -> Framework::Separable                                   */
+/* ------------------------------------------------------------------------------------------ */
+
+#define OR_MAX_DIMS 16
+
+int or_gauss_fir( void const* in, int in_dtype, int ndims, int64_t const* sizes, int64_t const* in_strides,
+                  void* out, int out_dtype, int64_t const* out_strides,
+                  double const* sigmas, unsigned const* orders, int const* bcs, double truncation ) {
+   if( ndims < 1 || ndims > OR_MAX_DIMS || dtype_size( in_dtype ) == 0 || dtype_size( out_dtype ) == 0 ) {
+      return OR_ERR_ARG;
+   }
+   /* GaussFIR: weight type (gauss.cpp:254) and per-dimension filters (:255-284). */
+   int weights_double = ( in_dtype == OR_DFLOAT );
+   /* SeparableConvolution: buffer type (convolution.cpp:341-343). */
+   int buf_type = or_suggest_flex( in_dtype );
+   int buf_double = ( buf_type == OR_DFLOAT );
+
+   int process[ OR_MAX_DIMS ];
+   size_t half[ OR_MAX_DIMS ];           /* border = dataSize - 1 */
+   double* taps[ OR_MAX_DIMS ] = { 0 };  /* reversed half kernel, f[0] = centre */
+   int odd[ OR_MAX_DIMS ];
+   int status = OR_OK;
+   size_t npix = 1;
+   for( int d = 0; d < ndims; ++d ) {
+      npix *= (size_t)sizes[ d ];
+   }
+   for( int d = 0; d < ndims; ++d ) {
+      process[ d ] = ( sigmas[ d ] > 0.0 ) && ( sizes[ d ] > 1 );
+      if( !process[ d ] ) { continue; }
+      if( orders[ d ] > 3 ) { status = OR_ERR_ORDER; goto done; }
+      int len = or_make_half_gaussian( sigmas[ d ], orders[ d ], truncation, weights_double, NULL, 0 );
+      double* h = (double*)malloc( sizeof( double ) * (size_t)len );
+      or_make_half_gaussian( sigmas[ d ], orders[ d ], truncation, weights_double, h, len );
+      taps[ d ] = (double*)malloc( sizeof( double ) * (size_t)len );
+      for( int k = 0; k < len; ++k ) {
+         /* CopyReverseData to float or double (convolution.cpp:50-58, 149-150). */
+         taps[ d ][ k ] = buf_double ? h[ len - 1 - k ] : (double)(float)h[ len - 1 - k ];
+      }
+      free( h );
+      half[ d ] = (size_t)len - 1;
+      odd[ d ] = ( orders[ d ] & 1 ) != 0;
+      /* IsMeaninglessFilter (convolution.cpp:304-314): a single tap equal to 1. */
+      if( len == 1 && taps[ d ][ 0 ] == 1.0 ) { process[ d ] = 0; }
+      if( bcs[ d ] < 0 || bcs[ d ] >= OR_BC_ALREADY_EXPANDED ) { status = OR_ERR_BC; goto done; }
+   }
+
+   /* Framework::Separable: processing order by input stride, stable insertion sort
+    * (framework_separable.cpp:146-165; sortIndices, dimension_array.h:907-924). */
+   int order[ OR_MAX_DIMS ];
+   int nproc = 0;
+   for( int d = 0; d < ndims; ++d ) {
+      if( process[ d ] ) { order[ nproc++ ] = d; }
+   }
+   for( int ii = 1; ii < nproc; ++ii ) {
+      int elem = order[ ii ];
+      int jj = ii;
+      while( jj > 0 && in_strides[ order[ jj - 1 ] ] > in_strides[ elem ] ) {
+         order[ jj ] = order[ jj - 1 ];
+         --jj;
+      }
+      order[ jj ] = elem;
+   }
+   if( nproc == 0 ) {
+      /* output.Copy( input ) with conversion (framework_separable.cpp:155-159). */
+      int64_t coord[ OR_MAX_DIMS ] = { 0 };
+      for( size_t p = 0; p < npix; ++p ) {
+         ptrdiff_t io = 0, oo = 0;
+         for( int d = 0; d < ndims; ++d ) { io += coord[ d ] * in_strides[ d ]; oo += coord[ d ] * out_strides[ d ]; }
+         put_sample( out, out_dtype, oo, get_sample( in, in_dtype, io ));
+         for( int d = 0; d < ndims; ++d ) { if( ++coord[ d ] < sizes[ d ] ) { break; } coord[ d ] = 0; }
+      }
+      goto done;
+   }
+
+   /* in -> output -> output ... (or via an intermediate of the buffer type when the output type
+    * differs, framework_separable.cpp:181-206). */
+   int use_intermediate = ( out_dtype != buf_type );
+   void* inter = NULL;
+   int64_t inter_strides[ OR_MAX_DIMS ];
+   if( use_intermediate ) {
+      inter = malloc( npix * dtype_size( buf_type ));
+      int64_t s = 1;
+      for( int d = 0; d < ndims; ++d ) { inter_strides[ d ] = s; s *= sizes[ d ]; }
+   }
+   size_t maxlen = 0, maxhalf = 0;
+   for( int ii = 0; ii < nproc; ++ii ) {
+      if( (size_t)sizes[ order[ ii ] ] > maxlen ) { maxlen = (size_t)sizes[ order[ ii ] ]; }
+      if( half[ order[ ii ] ] > maxhalf ) { maxhalf = half[ order[ ii ] ]; }
+   }
+   size_t esz = buf_double ? 8 : 4;
+   char* inbuf = (char*)malloc( esz * ( maxlen + 2 * maxhalf ));
+   char* outbuf = (char*)malloc( esz * maxlen );
+   float* ftaps = (float*)malloc( sizeof( float ) * ( maxhalf + 1 ));
+
+   void const* src = in;
+   int src_type = in_dtype;
+   int64_t const* src_strides = in_strides;
+   for( int rep = 0; rep < nproc; ++rep ) {
+      int pd = order[ rep ];
+      int last = ( rep == nproc - 1 );
+      void* dst = ( last || !use_intermediate ) ? out : inter;
+      int dst_type = ( last || !use_intermediate ) ? out_dtype : buf_type;
+      int64_t const* dst_strides = ( last || !use_intermediate ) ? out_strides : inter_strides;
+      size_t n = (size_t)sizes[ pd ];
+      size_t h = half[ pd ];
+      size_t nlines = npix / n;
+      for( size_t k = 0; k <= h; ++k ) { ftaps[ k ] = (float)taps[ pd ][ k ]; }
+      int64_t coord[ OR_MAX_DIMS ] = { 0 };
+      for( size_t line = 0; line < nlines; ++line ) {
+         ptrdiff_t so = 0, dof = 0;
+         for( int d = 0; d < ndims; ++d ) { so += coord[ d ] * src_strides[ d ]; dof += coord[ d ] * dst_strides[ d ]; }
+         /* CopyBuffer into the line buffer (framework_separable.cpp:357-368), ExpandBuffer
+          * (:369-380), filter (:389), write back (:384-417). */
+         if( buf_double ) {
+            double* b = (double*)inbuf + h;
+            double* o = (double*)outbuf;
+            for( size_t i = 0; i < n; ++i ) { b[ i ] = get_sample( src, src_type, so + (ptrdiff_t)i * src_strides[ pd ] ); }
+            or_expand_buffer_f64( b, 1, n, h, h, bcs[ pd ] );
+            line_filter_f64( b, o, n, taps[ pd ], h + 1, odd[ pd ] );
+            for( size_t i = 0; i < n; ++i ) { put_sample( dst, dst_type, dof + (ptrdiff_t)i * dst_strides[ pd ], o[ i ] ); }
+         } else {
+            float* b = (float*)inbuf + h;
+            float* o = (float*)outbuf;
+            for( size_t i = 0; i < n; ++i ) { b[ i ] = (float)get_sample( src, src_type, so + (ptrdiff_t)i * src_strides[ pd ] ); }
+            or_expand_buffer_f32( b, 1, n, h, h, bcs[ pd ] );
+            line_filter_f32( b, o, n, ftaps, h + 1, odd[ pd ] );
+            for( size_t i = 0; i < n; ++i ) { put_sample( dst, dst_type, dof + (ptrdiff_t)i * dst_strides[ pd ], (double)o[ i ] ); }
+         }
+         for( int d = 0; d < ndims; ++d ) {
+            if( d == pd ) { continue; }
+            if( ++coord[ d ] < sizes[ d ] ) { break; }
+            coord[ d ] = 0;
+         }
+      }
+      src = dst;
+      src_type = dst_type;
+      src_strides = dst_strides;
+   }
+   free( inbuf );
+   free( outbuf );
+   free( ftaps );
+   free( inter );
+
+done:
+   for( int d = 0; d < ndims; ++d ) { free( taps[ d ] ); }
+   return status;
+}

@@ -1,0 +1,206 @@
+// Test infrastructure only (linked into oracle/_ref/libdipref.so, never into the product).
+//
+// A thin extern "C" layer over the unmodified DIPlib sources so that Python tests and the bench's
+// CPU leg can call the reference's own Gaussian FIR path on raw host buffers:
+//   dip::Gauss               src/linear/derivative.cpp:62-86
+//   dip::StructureTensor     src/analysis/structure_tensor.cpp:33-59
+//   dip::MakeHalfGaussian    src/linear/gauss.cpp:151-165
+//   dip::detail::ExpandBuffer src/library/copy_buffer.cpp:751-813
+//   dip::ReadPixelWithBoundaryCondition src/library/boundary.cpp:47-128
+//
+// Sizes and strides are given in DIPlib order (x first), in samples.  Data type codes are the
+// ones of include/dipcu.h (DIPCU_BIN .. DIPCU_DFLOAT).  Every entry point returns 0 on success
+// and 1 on a dip::Error, whose message is copied into `err`.
+
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "diplib.h"
+#include "diplib/analysis.h"
+#include "diplib/boundary.h"
+#include "diplib/generation.h"
+#include "diplib/library/copy_buffer.h"
+#include "diplib/linear.h"
+#include "diplib/multithreading.h"
+
+namespace {
+
+dip::DataType CodeToType( int code ) {
+   switch( code ) {
+      case 0: return dip::DT_BIN;
+      case 1: return dip::DT_UINT8;
+      case 2: return dip::DT_UINT16;
+      case 3: return dip::DT_UINT32;
+      case 4: return dip::DT_UINT64;
+      case 5: return dip::DT_SINT8;
+      case 6: return dip::DT_SINT16;
+      case 7: return dip::DT_SINT32;
+      case 8: return dip::DT_SINT64;
+      case 9: return dip::DT_SFLOAT;
+      case 10: return dip::DT_DFLOAT;
+      default: DIP_THROW( "bad dtype code" );
+   }
+}
+
+int TypeToCode( dip::DataType dt ) {
+   for( int c = 0; c <= 10; ++c ) {
+      if( CodeToType( c ) == dt ) { return c; }
+   }
+   return -1;
+}
+
+void SetErr( char* err, int errlen, std::string const& msg ) {
+   if( err && errlen > 0 ) {
+      std::strncpy( err, msg.c_str(), static_cast< std::size_t >( errlen - 1 ));
+      err[ errlen - 1 ] = 0;
+   }
+}
+
+dip::StringArray SplitList( char const* s, bool present ) {
+   dip::StringArray out;
+   if( !present ) { return out; }
+   std::string str( s ? s : "" );
+   std::size_t start = 0;
+   while( true ) {
+      std::size_t pos = str.find( '\n', start );
+      out.push_back( str.substr( start, pos == std::string::npos ? std::string::npos : pos - start ));
+      if( pos == std::string::npos ) { break; }
+      start = pos + 1;
+   }
+   return out;
+}
+
+dip::Image Wrap( void const* data, int dtype, int ndims, int64_t const* sizes, int64_t const* strides ) {
+   dip::UnsignedArray sz( static_cast< dip::uint >( ndims ));
+   dip::IntegerArray st;
+   for( int ii = 0; ii < ndims; ++ii ) { sz[ ii ] = static_cast< dip::uint >( sizes[ ii ] ); }
+   if( strides ) {
+      st.resize( static_cast< dip::uint >( ndims ));
+      for( int ii = 0; ii < ndims; ++ii ) { st[ ii ] = strides[ ii ]; }
+   }
+   void* p = const_cast< void* >( data );
+   return dip::Image( dip::NonOwnedRefToDataSegment( p ), p, CodeToType( dtype ), sz, st );
+}
+
+void CopyOut( dip::Image const& img, void* out ) {
+   // `img` is freshly forged, so it has normal strides (contiguous, x fastest, tensor interleaved).
+   DIP_THROW_IF( !img.HasNormalStrides(), "unexpected strides" );
+   std::memcpy( out, img.Origin(), img.NumberOfSamples() * img.DataType().SizeOf() );
+}
+
+} // namespace
+
+extern "C" {
+
+int dipref_set_threads( int n ) {
+   dip::SetNumberOfThreads( static_cast< dip::uint >( n < 0 ? 0 : n ));
+   return static_cast< int >( dip::GetNumberOfThreads() );
+}
+
+// out_dtype: in/out.  If `protect_out` is 0, the reference allocates its own output (whose type
+// is returned in *out_dtype) and the samples are copied into `out` with normal strides.  If
+// `protect_out` is 1, `out` is wrapped as a protected image of type *out_dtype with normal
+// strides, and the reference writes into it directly (its protected-output path).
+int dipref_gauss(
+      void const* in, int in_dtype, int ndims, int64_t const* sizes, int64_t const* strides,
+      double const* sigmas, int nsigmas, uint32_t const* orders, int norders,
+      char const* bcs, int has_bcs, double truncation, char const* method,
+      void* out, int* out_dtype, int protect_out, char* err, int errlen ) {
+   try {
+      dip::Image img = Wrap( in, in_dtype, ndims, sizes, strides );
+      dip::FloatArray s( static_cast< dip::uint >( nsigmas ));
+      for( int ii = 0; ii < nsigmas; ++ii ) { s[ ii ] = sigmas[ ii ]; }
+      dip::UnsignedArray o( static_cast< dip::uint >( norders ));
+      for( int ii = 0; ii < norders; ++ii ) { o[ ii ] = orders[ ii ]; }
+      dip::StringArray bc = SplitList( bcs, has_bcs != 0 );
+      if( protect_out ) {
+         dip::Image res = Wrap( out, *out_dtype, ndims, sizes, nullptr );
+         res.Protect();
+         dip::Gauss( img, res, s, o, method, bc, truncation );
+      } else {
+         dip::Image res;
+         dip::Gauss( img, res, s, o, method, bc, truncation );
+         *out_dtype = TypeToCode( res.DataType() );
+         CopyOut( res, out );
+      }
+      return 0;
+   } catch( dip::Error const& e ) {
+      SetErr( err, errlen, e.what() );
+      return 1;
+   }
+}
+
+// Output: `ndims*(ndims+1)/2` tensor components per pixel, interleaved (normal strides), in the
+// reference's symmetric-matrix order (diagonal first).  Returns the output data type in *out_dtype.
+int dipref_structure_tensor(
+      void const* in, int in_dtype, int ndims, int64_t const* sizes,
+      double grad_sigma, double tensor_sigma, char const* method, char const* bc, double truncation,
+      void* out, int* out_dtype, char* err, int errlen ) {
+   try {
+      dip::Image img = Wrap( in, in_dtype, ndims, sizes, nullptr );
+      dip::Image res;
+      dip::StructureTensor( img, {}, res, { grad_sigma }, { tensor_sigma }, method, { bc }, truncation );
+      *out_dtype = TypeToCode( res.DataType() );
+      CopyOut( res, out );
+      return static_cast< int >( res.TensorElements() ) == ndims * ( ndims + 1 ) / 2 ? 0 : 1;
+   } catch( dip::Error const& e ) {
+      SetErr( err, errlen, e.what() );
+      return 1;
+   }
+}
+
+int dipref_half_gaussian( double sigma, uint32_t order, double truncation, int dt_double, double* out, int cap ) {
+   try {
+      std::vector< dip::dfloat > h = dip::MakeHalfGaussian( sigma, order, truncation, dt_double ? dip::DT_DFLOAT : dip::DT_SFLOAT );
+      int n = static_cast< int >( h.size() );
+      for( int ii = 0; ii < n && ii < cap; ++ii ) { out[ ii ] = h[ static_cast< dip::uint >( ii ) ]; }
+      return n;
+   } catch( dip::Error const& ) {
+      return -1;
+   }
+}
+
+// `buffer` points at the first of `pixels` samples; `left` samples before it and `right` after
+// it are written.  `bc` is a dip::BoundaryCondition enumerator value.
+int dipref_expand_buffer( void* buffer, int dtype, int64_t stride, uint64_t pixels, uint64_t left, uint64_t right, int bc ) {
+   try {
+      dip::detail::ExpandBuffer( buffer, CodeToType( dtype ), stride, 1, pixels, 1, left, right,
+                                 static_cast< dip::BoundaryCondition >( bc ));
+      return 0;
+   } catch( dip::Error const& ) {
+      return 1;
+   }
+}
+
+int dipref_string_to_bc( char const* s ) {
+   try {
+      return static_cast< int >( dip::StringToBoundaryCondition( s ));
+   } catch( dip::Error const& ) {
+      return -1;
+   }
+}
+
+double dipref_max_gauss_truncation( int dt_double ) {
+   return dt_double ? dip::maximum_gauss_truncation< dip::dfloat >() : dip::maximum_gauss_truncation< dip::sfloat >();
+}
+
+// Reads one sample of a scalar sfloat image at `coords` (which may lie outside the image).
+int dipref_read_pixel_bc( float const* img, int ndims, int64_t const* sizes, int64_t const* coords, int const* bcs, float* out ) {
+   try {
+      dip::Image im = Wrap( img, 9, ndims, sizes, nullptr );
+      dip::IntegerArray c( static_cast< dip::uint >( ndims ));
+      dip::BoundaryConditionArray b( static_cast< dip::uint >( ndims ));
+      for( int ii = 0; ii < ndims; ++ii ) {
+         c[ ii ] = coords[ ii ];
+         b[ ii ] = static_cast< dip::BoundaryCondition >( bcs[ ii ] );
+      }
+      *out = dip::ReadPixelWithBoundaryCondition( im, c, b ).As< float >();
+      return 0;
+   } catch( dip::Error const& ) {
+      return 1;
+   }
+}
+
+} // extern "C"
