@@ -1,0 +1,11 @@
+"""dipcu: DIPlib's Gaussian FIR filtering path (dip::Gauss "FIR" -> dip::GaussFIR ->
+dip::SeparableConvolution -> dip::Framework::Separable) on NVIDIA B200 (sm_100a).
+
+The Python API mirrors PyDIP's (``Gauss``, ``GaussFIR``, ``Derivative`` ...); all pixel work
+runs in libdipcu.so's CUDA kernels through the C-ABI declared in include/dipcu.h.
+"""
+from .filtering import (BestGaussMethod, BoundaryConditionFromString, Derivative, Error, Gauss, GaussFIR,
+                        ParameterError, RunTimeError, flex_dtype, image_desc)
+
+__all__ = ["BestGaussMethod", "BoundaryConditionFromString", "Derivative", "Error", "Gauss", "GaussFIR",
+           "ParameterError", "RunTimeError", "flex_dtype", "image_desc"]

@@ -1,0 +1,224 @@
+"""Python host layer of the Gaussian FIR path, mirroring PyDIP's filtering bindings
+(pydip/src/filtering.cpp:121-136 in DIPlib): ``Gauss``, ``GaussFIR``, ``Derivative``.
+
+Images are CUDA ``torch.Tensor`` objects (filtered in place on the device) or numpy arrays
+(copied to the current CUDA device and back).  As in PyDIP (pydip/src/image.cpp:25-33), the
+DIPlib axis order is the reverse of the array order: per-axis parameters (sigmas, orders,
+boundary conditions) are listed x first, i.e. for the LAST array axis first.
+
+Every filter call goes through libdipcu.so's C-ABI; nothing here computes pixels.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Iterable, Sequence
+
+import numpy as np
+import torch
+
+from . import _abi
+
+__all__ = ["Error", "ParameterError", "RunTimeError", "Gauss", "GaussFIR", "Derivative", "BestGaussMethod",
+           "BoundaryConditionFromString", "image_desc", "flex_dtype"]
+
+
+class Error(Exception):
+    """dip::Error."""
+
+
+class ParameterError(Error, ValueError):
+    """dip::ParameterError."""
+
+
+class RunTimeError(Error, RuntimeError):
+    """dip::RunTimeError."""
+
+
+_TORCH_CODES = {
+    torch.bool: _abi.BIN, torch.uint8: _abi.UINT8, torch.uint16: _abi.UINT16, torch.uint32: _abi.UINT32,
+    torch.uint64: _abi.UINT64, torch.int8: _abi.SINT8, torch.int16: _abi.SINT16, torch.int32: _abi.SINT32,
+    torch.int64: _abi.SINT64, torch.float32: _abi.SFLOAT, torch.float64: _abi.DFLOAT,
+}
+_NP_TO_TORCH = {
+    np.dtype(np.bool_): torch.bool, np.dtype(np.uint8): torch.uint8, np.dtype(np.uint16): torch.uint16,
+    np.dtype(np.uint32): torch.uint32, np.dtype(np.uint64): torch.uint64, np.dtype(np.int8): torch.int8,
+    np.dtype(np.int16): torch.int16, np.dtype(np.int32): torch.int32, np.dtype(np.int64): torch.int64,
+    np.dtype(np.float32): torch.float32, np.dtype(np.float64): torch.float64,
+}
+
+
+def flex_dtype(dtype: torch.dtype) -> torch.dtype:
+    """dip::DataType::SuggestFlex (src/library/datatype.cpp:109-124) for real types."""
+    if dtype in (torch.uint32, torch.int32, torch.uint64, torch.int64, torch.float64):
+        return torch.float64
+    if dtype.is_complex:
+        raise ParameterError("Data type not supported")
+    return torch.float32
+
+
+def image_desc(t: torch.Tensor) -> _abi.ImageDesc:
+    """A dipcu_image_desc of a CUDA tensor: DIPlib axis order (reversed), strides in samples."""
+    if t.dtype not in _TORCH_CODES:
+        raise ParameterError("Data type not supported")
+    if t.dim() > _abi.MAX_DIMS:
+        raise ParameterError("Dimensionality not supported")
+    d = _abi.ImageDesc()
+    d.data = t.data_ptr()
+    d.dtype = _TORCH_CODES[t.dtype]
+    if t.dim() == 0:
+        d.ndims = 1
+        d.sizes[0] = 1
+        d.strides[0] = 1
+        return d
+    d.ndims = t.dim()
+    for i, (s, st) in enumerate(zip(reversed(t.shape), reversed(t.stride()))):
+        d.sizes[i] = int(s)
+        d.strides[i] = int(st)
+    return d
+
+
+def _array_use_parameter(values, nd: int, default) -> list:
+    """dip::ArrayUseParameter: empty -> default for all, 1 value -> broadcast, nd values -> as is."""
+    if values is None:
+        values = []
+    elif isinstance(values, (int, float, np.integer, np.floating, str)):
+        values = [values]
+    values = list(values)
+    if len(values) == 0:
+        return [default] * nd
+    if len(values) == 1:
+        return values * nd
+    if len(values) != nd:
+        raise ParameterError("Array parameter has the wrong number of elements")
+    return values
+
+
+def BoundaryConditionFromString(bc: str) -> int:
+    """dip::StringToBoundaryCondition (include/diplib/boundary.h:87-103)."""
+    code = _abi.lib().dipcu_bc_from_string(bc.encode())
+    if code < 0:
+        raise ParameterError("Boundary condition not recognized: " + bc)
+    return code
+
+
+def BestGaussMethod(sigmas: Sequence[float], orders: Sequence[int]) -> str:
+    """BestGaussMethod, src/linear/derivative.cpp:35-58."""
+    if any(o > 3 for o in orders):
+        return "ft"
+    if any(0.0 < s < 0.8 for s in sigmas):
+        return "ft"
+    if any(s > 10 for s in sigmas):
+        return "iir"
+    return "fir"
+
+
+_STATUS_ERRORS = {
+    _abi.ERR_INVALID_ARG: ParameterError,
+    _abi.ERR_UNSUPPORTED_DTYPE: ParameterError,
+    _abi.ERR_UNSUPPORTED_BC: ParameterError,
+    _abi.ERR_ORDER_GT_3: ParameterError,
+    _abi.ERR_SIZES_DONT_MATCH: ParameterError,
+    _abi.ERR_KERNEL_TOO_LARGE: ParameterError,
+    _abi.ERR_CUDA: RunTimeError,
+    _abi.ERR_TIMEOUT: RunTimeError,
+}
+
+
+def check(status: int) -> None:
+    if status != _abi.OK:
+        raise _STATUS_ERRORS.get(status, RunTimeError)(_abi.last_error())
+
+
+def _to_device(img):
+    """(tensor on the current CUDA device, was_numpy)."""
+    if isinstance(img, torch.Tensor):
+        if not img.is_cuda:
+            raise ParameterError("tensor images must live on a CUDA device")
+        return img, False
+    arr = np.asarray(img)
+    if arr.dtype not in _NP_TO_TORCH:
+        raise ParameterError("Data type not supported")
+    # torch.from_numpy lacks some unsigned types; go through a byte view.
+    t = torch.from_numpy(np.ascontiguousarray(arr).view(np.uint8)).view(_NP_TO_TORCH[arr.dtype]).reshape(arr.shape)
+    return t.to("cuda", non_blocking=False), True
+
+
+def _to_host(t: torch.Tensor) -> np.ndarray:
+    np_dt = {v: k for k, v in _NP_TO_TORCH.items()}[t.dtype]
+    host = t.contiguous().cpu()
+    return host.view(torch.uint8).numpy().view(np_dt).reshape(tuple(host.shape))
+
+
+def _shares_memory(a: torch.Tensor, b: torch.Tensor) -> bool:
+    if a.device != b.device:
+        return False
+    a0, a1 = a.data_ptr(), a.data_ptr() + max(1, a.untyped_storage().nbytes())
+    b0, b1 = b.data_ptr(), b.data_ptr() + max(1, b.untyped_storage().nbytes())
+    return a.untyped_storage().data_ptr() == b.untyped_storage().data_ptr() or (a0 < b1 and b0 < a1)
+
+
+def GaussFIR(in_, sigmas: Iterable[float] | float = (1.0,), derivativeOrder: Iterable[int] | int = (0,),
+             boundaryCondition: Iterable[str] | str = (), truncation: float = 3.0, *, out=None):
+    """dip::GaussFIR (include/diplib/linear.h:300-318, src/linear/gauss.cpp:238-286).
+
+    ``out``: optional CUDA tensor of the input's shape.  Its type is kept (DIPlib's protected
+    output: computation in the flex type, clamp_cast on the final write); if it shares memory
+    with the input the result goes through a fresh buffer first, as DIPlib strips such outputs.
+    Returns the output (a tensor, or a numpy array for numpy input).
+    """
+    x, was_numpy = _to_device(in_)
+    nd = max(1, x.dim())
+    sig = [float(s) for s in _array_use_parameter(sigmas, nd, 1.0)]
+    ords = [int(o) for o in _array_use_parameter(derivativeOrder, nd, 0)]
+    bcs = [BoundaryConditionFromString(b) for b in _array_use_parameter(boundaryCondition, nd, "")]
+    if any(o < 0 for o in ords):
+        raise ParameterError("derivative orders must be non-negative")
+    if out is None:
+        res = torch.empty(x.shape, dtype=flex_dtype(x.dtype), device=x.device)
+        target = None
+    else:
+        if not isinstance(out, torch.Tensor) or out.device != x.device:
+            raise ParameterError("out must be a tensor on the input's device")
+        if tuple(out.shape) != tuple(x.shape):
+            raise ParameterError("Sizes don't match")
+        if _shares_memory(out, x):
+            res = torch.empty(out.shape, dtype=out.dtype, device=out.device)
+            target = out
+        else:
+            res = out
+            target = None
+    din = image_desc(x)
+    dout = image_desc(res)
+    stream = torch.cuda.current_stream(x.device).cuda_stream
+    with torch.cuda.device(x.device):
+        check(_abi.lib().dipcu_gauss_fir(
+            ctypes.byref(din), ctypes.byref(dout), (ctypes.c_double * nd)(*sig), (ctypes.c_uint32 * nd)(*ords),
+            (ctypes.c_int32 * nd)(*bcs), float(truncation), ctypes.c_void_p(stream)))
+    if target is not None:
+        target.copy_(res)
+        res = target
+    return _to_host(res) if was_numpy else res
+
+
+def Gauss(in_, sigmas=(1.0,), derivativeOrder=(0,), method: str = "best", boundaryCondition=(),
+          truncation: float = 3.0, *, out=None):
+    """dip::Gauss (src/linear/derivative.cpp:62-86): the "gauss" prefix is stripped and "best"
+    resolved by BestGaussMethod; this implementation provides the FIR method."""
+    m = method[5:] if method[:5] == "gauss" else method
+    x_nd = max(1, (in_.dim() if isinstance(in_, torch.Tensor) else np.asarray(in_).ndim))
+    if m == "best":
+        m = BestGaussMethod(_array_use_parameter(sigmas, x_nd, 1.0), _array_use_parameter(derivativeOrder, x_nd, 0))
+    if m in ("FIR", "fir"):
+        return GaussFIR(in_, sigmas, derivativeOrder, boundaryCondition, truncation, out=out)
+    if m in ("FT", "ft", "IIR", "iir"):
+        raise NotImplementedError(f"Gauss method {method!r} (resolved to {m!r}) is outside the B200 FIR path")
+    raise ParameterError("Invalid flag: " + m)
+
+
+def Derivative(in_, derivativeOrder=(0,), sigmas=(1.0,), method: str = "best", boundaryCondition=(),
+               truncation: float = 3.0, *, out=None):
+    """dip::Derivative (src/linear/derivative.cpp:88-116), Gaussian methods."""
+    if method == "best" or method[:5] == "gauss":
+        return Gauss(in_, sigmas, derivativeOrder, "best" if method == "gauss" else method, boundaryCondition,
+                     truncation, out=out)
+    raise ParameterError("Invalid flag: " + method)

@@ -1,0 +1,113 @@
+/*
+ * dipcu -- B200 (sm_100a) implementation of DIPlib's Gaussian FIR filtering path.
+ *
+ * C-ABI of libdipcu.so.  Plain pointers and sizes only.  Every image argument is a
+ * `dipcu_image_desc` whose `data` is a DEVICE pointer to the image origin; sizes and strides
+ * follow dip::Image (include/diplib/library/image.h:268+ in DIPlib): DIPlib axis order (x first),
+ * strides in samples (they may be negative).  Per-axis parameter arrays have exactly `ndims`
+ * entries (the caller has already broadcast them the way dip::ArrayUseParameter does).
+ *
+ * All entry points are asynchronous on `stream` (a cudaStream_t; NULL = the legacy default
+ * stream), return a dipcu_status, and record a message retrievable with
+ * dipcu_last_error_message() (thread-local).  None of them synchronises the device.
+ */
+#ifndef DIPCU_H
+#define DIPCU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DIPCU_MAX_DIMS 8
+
+/* Sample types: the real dip::DataType values (include/diplib/library/datatype.h). */
+typedef enum {
+   DIPCU_BIN = 0, DIPCU_UINT8 = 1, DIPCU_UINT16 = 2, DIPCU_UINT32 = 3, DIPCU_UINT64 = 4,
+   DIPCU_SINT8 = 5, DIPCU_SINT16 = 6, DIPCU_SINT32 = 7, DIPCU_SINT64 = 8,
+   DIPCU_SFLOAT = 9, DIPCU_DFLOAT = 10
+} dipcu_dtype;
+
+/* dip::BoundaryCondition enumerators, same values (include/diplib/boundary.h:65-80). */
+typedef enum {
+   DIPCU_BC_SYMMETRIC_MIRROR = 0, DIPCU_BC_ASYMMETRIC_MIRROR = 1, DIPCU_BC_ANTISYMMETRIC_REFLECT = 2,
+   DIPCU_BC_PERIODIC = 3, DIPCU_BC_ASYMMETRIC_PERIODIC = 4, DIPCU_BC_ADD_ZEROS = 5,
+   DIPCU_BC_ADD_MAX_VALUE = 6, DIPCU_BC_ADD_MIN_VALUE = 7, DIPCU_BC_ZERO_ORDER_EXTRAPOLATE = 8,
+   DIPCU_BC_FIRST_ORDER_EXTRAPOLATE = 9, DIPCU_BC_SECOND_ORDER_EXTRAPOLATE = 10,
+   DIPCU_BC_THIRD_ORDER_EXTRAPOLATE = 11, DIPCU_BC_ALREADY_EXPANDED = 12
+} dipcu_bc;
+
+typedef enum {
+   DIPCU_OK = 0,
+   DIPCU_ERR_INVALID_ARG = 1,       /* bad pointer, size, stride, dimensionality or parameter */
+   DIPCU_ERR_UNSUPPORTED_DTYPE = 2, /* e.g. complex data (dip::E::DATA_TYPE_NOT_SUPPORTED) */
+   DIPCU_ERR_UNSUPPORTED_BC = 3,    /* unknown value, or "already expanded" */
+   DIPCU_ERR_ORDER_GT_3 = 4,        /* "Gaussian FIR filter not implemented for order > 3" */
+   DIPCU_ERR_CUDA = 5,              /* a CUDA runtime call failed */
+   DIPCU_ERR_TIMEOUT = 6,           /* a bounded device-side wait gave up */
+   DIPCU_ERR_SIZES_DONT_MATCH = 7,  /* in/out size mismatch (dip::E::SIZES_DONT_MATCH) */
+   DIPCU_ERR_KERNEL_TOO_LARGE = 8   /* kernel half-width beyond the supported maximum */
+} dipcu_status;
+
+typedef struct {
+   void* data;                        /* device pointer to the origin sample */
+   int32_t dtype;                     /* dipcu_dtype */
+   int32_t ndims;                     /* 1 .. DIPCU_MAX_DIMS */
+   int64_t sizes[ DIPCU_MAX_DIMS ];   /* DIPlib order, x first */
+   int64_t strides[ DIPCU_MAX_DIMS ]; /* in samples */
+} dipcu_image_desc;
+
+/* ---- Forward filter ---------------------------------------------------------------------- */
+
+/* The body of dip::GaussFIR (src/linear/gauss.cpp:238-286 in DIPlib) and the path below it:
+ * dip::SeparableConvolution (src/linear/convolution.cpp:319-421) driven by
+ * dip::Framework::Separable (src/library/framework_separable.cpp:35-431).
+ *
+ * `in`: any real sample type.  `out`: same sizes; its type is normally the one DIPlib picks
+ * (dip::DataType::SuggestFlex: sfloat, or dfloat for 32/64-bit integer and dfloat input);
+ * another type reproduces DIPlib's protected-output path (computation in the flex type,
+ * clamp_cast on the final write).  `out` must not overlap `in` (DIPlib strips an overlapping
+ * output first; the C++ layer above does the same).
+ * `sigmas[d] <= 0` or `sizes[d] == 1` leaves axis d unfiltered; `orders[d]` in 0..3;
+ * `bcs[d]` a dipcu_bc; `truncation <= 0` means 3.
+ * Replaces the per-line, host-pointer callback Framework::SeparableLineFilter
+ * (include/diplib/framework.h:654-669) with fused device kernels. */
+int dipcu_gauss_fir( dipcu_image_desc const* in, dipcu_image_desc const* out,
+                     double const* sigmas, uint32_t const* orders, int32_t const* bcs,
+                     double truncation, void* stream );
+
+/* ---- Kernel weights ----------------------------------------------------------------------- */
+
+/* Half-kernel length of dip::MakeHalfGaussian (src/linear/gauss.cpp:38-62): returns
+ * 1 + HalfGaussianSize (at least 2 for order 3), 1 for sigma == 0, or -1 for order > 3.
+ * `dt_double` selects the dfloat truncation limit (maximum_gauss_truncation<dfloat>). */
+int dipcu_half_gaussian_length( double sigma, uint32_t order, double truncation, int dt_double );
+
+/* On-device construction of the weights of dip::MakeHalfGaussian (src/linear/gauss.cpp:53-165)
+ * for `count` (sigma, order) pairs read from DEVICE arrays.  Entry i writes its reversed half
+ * kernel (centre tap first, as InternOneDimensionalFilter stores it, convolution.cpp:76-156)
+ * to `weights + i * stride` as floats; with `dweights` non-NULL also d(weights)/d(sigma).
+ * `lengths` (device, optional) receives each half-kernel length; entries longer than `stride`
+ * are truncated and flagged with a negative length. */
+int dipcu_make_gauss_weights( double const* sigmas, uint32_t const* orders, int count, double truncation,
+                              float* weights, float* dweights, int32_t* lengths, int stride, void* stream );
+
+/* ---- Utilities ----------------------------------------------------------------------------- */
+
+/* dip::StringToBoundaryCondition (include/diplib/boundary.h:87-103): a dipcu_bc, or -1 when the
+ * string is not recognised ("Boundary condition not recognized: " + bc). */
+int dipcu_bc_from_string( char const* bc );
+
+/* Message of the last failing call on this host thread ("" if none). */
+char const* dipcu_last_error_message( void );
+
+/* Library version string. */
+char const* dipcu_version( void );
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DIPCU_H */

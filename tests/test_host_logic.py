@@ -1,0 +1,123 @@
+"""CPU tests of the host-side logic: libdipcu.so loads and exports every symbol include/dipcu.h
+declares; boundary-condition strings, kernel-weight construction and the closed-form boundary
+extension used by the kernels (diplib_b200/csrc/dipcu_common.cuh, compiled for the host by
+tests/native/host_logic_shim.cpp) agree with the oracle."""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import oracle
+from tests.conftest import HOSTLOGIC, ROOT
+
+HEADER = os.path.join(ROOT, "include", "dipcu.h")
+BCS = list(oracle.BC_CODES)
+
+
+def declared_symbols():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(dipcu_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    from diplib_b200 import _abi
+    lib = _abi.lib()
+    syms = declared_symbols()
+    assert "dipcu_gauss_fir" in syms
+    for s in syms:
+        assert hasattr(lib, s), s
+    assert set(syms) <= set(_abi.SIGNATURES), set(syms) - set(_abi.SIGNATURES)
+    assert b"sm_100a" in lib.dipcu_version()
+
+
+def test_bc_strings_match_reference_parser():
+    from diplib_b200 import _abi
+    lib = _abi.lib()
+    for s in BCS:
+        assert lib.dipcu_bc_from_string(s.encode()) == oracle.BC_CODES[s], s
+        if oracle.ref_available():
+            assert oracle.ref_lib().dipref_string_to_bc(s.encode()) == oracle.BC_CODES[s], s
+    assert lib.dipcu_bc_from_string(b"symmetric mirror") == -1
+    assert _abi.last_error() == "Boundary condition not recognized: symmetric mirror"
+    if oracle.ref_available():
+        assert oracle.ref_lib().dipref_string_to_bc(b"symmetric mirror") == -1
+
+
+def test_boundary_parsing_errors_python():
+    import diplib_b200 as dipcu
+    with pytest.raises(dipcu.ParameterError, match="Boundary condition not recognized: bogus"):
+        dipcu.BoundaryConditionFromString("bogus")
+
+
+def _hl():
+    l = ctypes.CDLL(HOSTLOGIC)
+    l.hl_extend_f32.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int32, ctypes.c_void_p]
+    l.hl_half_gaussian_length.restype = ctypes.c_int64
+    l.hl_half_gaussian_length.argtypes = [ctypes.c_double, ctypes.c_uint32, ctypes.c_double, ctypes.c_int]
+    l.hl_make_half_gaussian.argtypes = [ctypes.c_double, ctypes.c_uint32, ctypes.c_int64, ctypes.c_void_p,
+                                        ctypes.c_void_p]
+    return l
+
+
+def host_half_gaussian(sigma, order, trunc, dt_double, with_derivative=False):
+    l = _hl()
+    n = l.hl_half_gaussian_length(sigma, order, trunc, int(dt_double))
+    w = np.zeros(n)
+    dw = np.zeros(n)
+    l.hl_make_half_gaussian(sigma, order, n, w.ctypes.data, dw.ctypes.data if with_derivative else None)
+    return (w, dw) if with_derivative else w
+
+
+@pytest.mark.parametrize("dt_double", [False, True])
+def test_weights_match_oracle(dt_double):
+    from diplib_b200 import _abi
+    for sigma in [0.3, 0.5, 0.8, 1.0, 1.5, 2.0, 3.0, 4.0, 7.3, 8.0, 20.0]:
+        for order in range(4):
+            for trunc in [0.0, 1.0, 3.0, 4.5, 10.0]:
+                ref = oracle.half_gaussian(sigma, order, trunc, dt_double)[::-1]  # centre first
+                got = host_half_gaussian(sigma, order, trunc, dt_double)
+                assert got.shape == ref.shape, (sigma, order, trunc)
+                np.testing.assert_array_max_ulp(got, ref, maxulp=2)
+                assert _abi.lib().dipcu_half_gaussian_length(sigma, order, trunc, int(dt_double)) == ref.size
+    assert _abi.lib().dipcu_half_gaussian_length(1.0, 4, 3.0, 0) == -1
+
+
+@pytest.mark.parametrize("order", [0, 1, 2, 3])
+def test_sigma_derivative_of_weights(order):
+    for sigma in [0.9, 1.5, 3.0, 6.0]:
+        w, dw = host_half_gaussian(sigma, order, 3.0, False, with_derivative=True)
+        n = w.size
+        h = 1e-6
+        l = _hl()
+        wp = np.zeros(n)
+        wm = np.zeros(n)
+        l.hl_make_half_gaussian(sigma + h, order, n, wp.ctypes.data, None)
+        l.hl_make_half_gaussian(sigma - h, order, n, wm.ctypes.data, None)
+        fd = (wp - wm) / (2 * h)
+        np.testing.assert_allclose(dw, fd, rtol=1e-5, atol=1e-8 * np.abs(fd).max())
+
+
+def test_boundary_closed_forms_match_expand_buffer():
+    l = _hl()
+    rng = np.random.default_rng(7)
+    for bc in BCS:
+        code = oracle.BC_CODES[bc]
+        if code == 12:
+            continue
+        for n in [1, 2, 3, 4, 7, 10]:
+            for border in [1, 2, 5, 9, 23]:
+                line = (rng.random(n) * 10 - 3).astype(np.float32)
+                ref = oracle.expand_buffer(line, border, border, bc)
+                got = np.zeros(n + 2 * border, np.float32)
+                l.hl_extend_f32(line.ctypes.data, n, border, code, got.ctypes.data)
+                if bc in ("antisym reflect",):
+                    # Multiple reflections: the reference rounds each stored value before
+                    # deriving the next offset; the closed form rounds once.
+                    np.testing.assert_allclose(got, ref, rtol=1e-6, atol=1e-5)
+                else:
+                    assert np.array_equal(got, ref), (bc, n, border)

@@ -1,0 +1,96 @@
+"""Pins the C restatement of the Gaussian FIR path (oracle/gauss_oracle.c) to the reference:
+bit-exact against fixtures generated from the compiled DIPlib sources (tests/golden/), against
+the live reference library where it is present, and on the known-answer properties of
+DIPlib's own Gaussian tests (src/linear/gauss.cpp:496-540)."""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from tests.golden.make_golden import CASES, make_input
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def test_gauss_matches_reference_fixtures():
+    ref = np.load(os.path.join(GOLDEN, "gauss_ref.npz"))
+    for name, seed, shape, dtype, sig, ords, bcs, trunc in CASES:
+        x = make_input(seed, shape, dtype)
+        y = oracle.gauss_fir(x, sig, ords, bcs or ["mirror"], trunc)
+        assert y.dtype == ref[name].dtype, name
+        assert np.array_equal(y, ref[name], equal_nan=True), name
+
+
+def test_half_gaussian_matches_reference_fixtures():
+    ref = np.load(os.path.join(GOLDEN, "half_gaussian_ref.npz"))
+    for key in ref.files:
+        s, o, d = key[1:].split("_")
+        got = oracle.half_gaussian(float(s), int(o[1:]), 3.0, bool(int(d[1:])))
+        assert np.array_equal(got, ref[key]), key
+
+
+def test_expand_buffer_matches_reference_fixtures():
+    ref = np.load(os.path.join(GOLDEN, "expand_buffer_ref.npz"))
+    for key in ref.files:
+        if not key.endswith("|in"):
+            continue
+        bc, n, left, right, _ = key.split("|")
+        got = oracle.expand_buffer(ref[key], int(left), int(right), bc)
+        assert np.array_equal(got, ref[key[:-3] + "|out"]), key
+
+
+def test_structure_tensor_matches_reference_fixture():
+    ref = np.load(os.path.join(GOLDEN, "structure_tensor_ref.npz"))["st"]
+    x = make_input(21, (10, 12, 14), "float32")
+    got = oracle.structure_tensor(x, 1.0, 2.0, "mirror", 3.0)
+    np.testing.assert_allclose(got, ref, rtol=0, atol=1e-6 * np.abs(ref).max())
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference library not built here")
+def test_gauss_matches_live_reference_fuzz():
+    rng = np.random.default_rng(1234)
+    bcs = ["mirror", "asym mirror", "antisym reflect", "periodic", "asym periodic", "add zeros", "zero order",
+           "first order", "second order", "third order"]
+    for it in range(60):
+        nd = int(rng.integers(1, 4))
+        shape = tuple(int(rng.integers(1, 24)) for _ in range(nd))
+        dtype = [np.float32, np.uint16, np.uint8, np.int16, np.float64, np.int32][int(rng.integers(0, 6))]
+        x = make_input(int(rng.integers(0, 1 << 30)), shape, dtype)
+        sig = [float(rng.choice([0.0, 0.6, 1.0, 1.7, 2.5, 4.0])) for _ in range(nd)]
+        ords = [int(rng.integers(0, 4)) for _ in range(nd)]
+        bc = [str(rng.choice(bcs)) for _ in range(nd)]
+        tr = float(rng.choice([2.0, 3.0, 4.5]))
+        a = oracle.gauss_fir(x, sig, ords, bc, tr)
+        b = oracle.ref_gauss(x, sig, ords, bc, tr)
+        assert np.array_equal(a, b, equal_nan=True), (it, shape, dtype, sig, ords, bc, tr)
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference library not built here")
+def test_protected_output_matches_live_reference():
+    x = make_input(5, (30, 40), np.float32) * 300.0
+    for out_dt in (np.uint8, np.int16, np.float64):
+        a = oracle.gauss_fir(x, [2.0], [0], ["mirror"], 3.0, out_dtype=out_dt)
+        b = oracle.ref_gauss(x, [2.0], [0], ["mirror"], 3.0, out_dtype=out_dt)
+        assert np.array_equal(a, b), out_dt
+
+
+def test_known_answers_from_reference_tests():
+    # src/linear/gauss.cpp:496-540: delta at 128 of a 256-sample dfloat line, sigma 5.
+    img = np.zeros(256, np.float64)
+    img[128] = 1.0
+    fir = oracle.gauss_fir(img, [5.0], [0])
+    assert abs(fir.sum() - 1.0) < 1e-12
+    # The reference bounds FT vs the amplitude by 0.00015 and FIR vs FT by 0.0006.
+    assert abs(fir[128] - 1.0 / (np.sqrt(2 * np.pi) * 5.0)) < 0.00015 + 0.0006
+    ramp = np.arange(-128, 128, dtype=np.float64)
+    assert fir.dtype == np.float64
+    assert oracle.gauss_fir(ramp, [5.0], [1])[128] == pytest.approx(1.0)
+    assert oracle.gauss_fir(ramp * ramp, [5.0], [2])[128] == pytest.approx(2.0)
+
+
+def test_order_gt_3_rejected():
+    with pytest.raises(ValueError, match="order > 3"):
+        oracle.gauss_fir(np.zeros((8, 8), np.float32), [1.0], [4])
