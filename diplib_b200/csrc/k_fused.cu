@@ -2,15 +2,192 @@
 // per-axis half-widths and symmetry at compile time so that the tap loops unroll fully and the
 // weights are read as constant-bank operands; configurations without an entry run on the line
 // kernel (K2).
+#include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <utility>
+
 #include "fused.cuh"
+#include "fused3d_tma.cuh"
 
 namespace dipcu {
+
+// Device status word: kernels that give up a bounded wait store DIPCU_ERR_TIMEOUT here.
+__device__ int32_t g_device_status;
+
+int32_t* device_status_ptr() {
+   int dev = 0;
+   cudaGetDevice( &dev );
+   static std::mutex mu;
+   static int32_t* ptrs[ 64 ] = {};
+   std::lock_guard< std::mutex > lock( mu );
+   if( dev < 0 || dev >= 64 ) { return nullptr; }
+   if( !ptrs[ dev ] ) {
+      void* p = nullptr;
+      if( cudaGetSymbolAddress( &p, g_device_status ) != cudaSuccess ) { return nullptr; }
+      ptrs[ dev ] = static_cast< int32_t* >( p );
+   }
+   return ptrs[ dev ];
+}
 
 namespace {
 
 constexpr int kNT = 256;
+
+int sm_count() {
+   static int cached[ 64 ] = {};
+   int dev = 0;
+   cudaGetDevice( &dev );
+   if( dev < 0 || dev >= 64 ) { return 148; }
+   if( !cached[ dev ] ) {
+      int n = 148;
+      cudaDeviceGetAttribute( &n, cudaDevAttrMultiProcessorCount, dev );
+      cached[ dev ] = n;
+   }
+   return cached[ dev ];
+}
+
+// Small cache of encoded tensor maps: encoding costs host microseconds per call, and the same
+// images are filtered over and over.
+struct TmapEntry {
+   bool used;
+   int device;
+   void const* ptr;
+   cuuint64_t dims[ 4 ], strides[ 3 ];
+   cuuint32_t box[ 4 ];
+   CUtensorMapDataType dt;
+   CUtensorMap map;
+   uint64_t stamp;
+};
+
+CUresult encode_tmap( CUtensorMap* out, CUtensorMapDataType dt, void const* ptr, cuuint64_t const* dims,
+                      cuuint64_t const* strides, cuuint32_t const* box ) {
+   static std::mutex mu;
+   static TmapEntry cache[ 32 ];
+   static uint64_t clock = 0;
+   int dev = 0;
+   cudaGetDevice( &dev );
+   std::lock_guard< std::mutex > lock( mu );
+   TmapEntry* victim = &cache[ 0 ];
+   for( auto& e : cache ) {
+      if( e.used && e.device == dev && e.ptr == ptr && e.dt == dt &&
+          std::memcmp( e.dims, dims, sizeof( e.dims )) == 0 && std::memcmp( e.strides, strides, sizeof( e.strides )) == 0 &&
+          std::memcmp( e.box, box, sizeof( e.box )) == 0 ) {
+         e.stamp = ++clock;
+         *out = e.map;
+         return CUDA_SUCCESS;
+      }
+      if( !e.used || e.stamp < victim->stamp ) { victim = &e; }
+   }
+   // The driver entry point is resolved through the runtime, so that libdipcu.so has no
+   // link-time dependency on libcuda (it loads on machines without a GPU driver).
+   using EncodeFn = CUresult ( * )( CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, cuuint64_t const*,
+                                    cuuint64_t const*, cuuint32_t const*, cuuint32_t const*, CUtensorMapInterleave,
+                                    CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill );
+   static EncodeFn encode = nullptr;
+   if( !encode ) {
+      void* fn = nullptr;
+      cudaDriverEntryPointQueryResult q;
+      if( cudaGetDriverEntryPoint( "cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q ) != cudaSuccess ||
+          q != cudaDriverEntryPointSuccess || !fn ) {
+         return CUDA_ERROR_NOT_FOUND;
+      }
+      encode = reinterpret_cast< EncodeFn >( fn );
+   }
+   cuuint32_t estr[ 4 ] = { 1, 1, 1, 1 };
+   CUresult r = encode( out, dt, 4, const_cast< void* >( ptr ), dims, strides, box, estr,
+                                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE );
+   if( r != CUDA_SUCCESS ) { return r; }
+   victim->used = true;
+   victim->device = dev;
+   victim->ptr = ptr;
+   victim->dt = dt;
+   std::memcpy( victim->dims, dims, sizeof( victim->dims ));
+   std::memcpy( victim->strides, strides, sizeof( victim->strides ));
+   std::memcpy( victim->box, box, sizeof( victim->box ));
+   victim->map = *out;
+   victim->stamp = ++clock;
+   return CUDA_SUCCESS;
+}
+
+// Per-kernel, per-device launch set-up done once: the dynamic shared-memory opt-in and the
+// number of co-resident CTAs per SM.
+template< typename Kern >
+int prepare_kernel( Kern kern, int threads, size_t smem ) {
+   static std::mutex mu;
+   static std::map< std::pair< void const*, int >, int > per_sm;
+   int dev = 0;
+   cudaGetDevice( &dev );
+   auto key = std::make_pair( reinterpret_cast< void const* >( kern ), dev );
+   std::lock_guard< std::mutex > lock( mu );
+   auto it = per_sm.find( key );
+   if( it != per_sm.end() ) { return it->second; }
+   if( smem > 48 * 1024 &&
+       cudaFuncSetAttribute( kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast< int >( smem )) != cudaSuccess ) {
+      return -1;
+   }
+   int n = 0;
+   if( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &n, kern, threads, smem ) != cudaSuccess || n < 1 ) { return -1; }
+   per_sm[ key ] = n;
+   return n;
+}
+
+// TMA-pipelined 3D kernel; returns cudaErrorNotSupported when the layout does not allow TMA
+// (negative or unaligned strides), so that the caller falls back to the plain-load kernel.
+template< typename TIn, int HX, int HY, int HZ, bool OX, bool OY, bool OZ >
+cudaError_t run3d_tma( FusedArgs& a, cudaStream_t s ) {
+   using G = Z3Geom< TIn, HX, HY, HZ >;
+   constexpr int esz = sizeof( TIn );
+   if( a.ss[ 1 ] <= 0 || a.ss[ 2 ] <= 0 || ( a.nb > 1 && a.sb <= 0 )) { return cudaErrorNotSupported; }
+   if(( reinterpret_cast< uintptr_t >( a.src ) & 15 ) != 0 ) { return cudaErrorNotSupported; }
+   if(( a.ss[ 1 ] * esz ) % 16 || ( a.ss[ 2 ] * esz ) % 16 || ( a.nb > 1 && ( a.sb * esz ) % 16 )) { return cudaErrorNotSupported; }
+   if( a.n[ 0 ] > 0x7fffffff || a.n[ 1 ] > 0x7fffffff || a.n[ 2 ] > 0x7fffffff || a.nb > 0x7fffffff ) { return cudaErrorNotSupported; }
+   Z3Args z{};
+   CUtensorMapDataType dt = sizeof( TIn ) == 2 ? CU_TENSOR_MAP_DATA_TYPE_UINT16
+                          : sizeof( TIn ) == 1 ? CU_TENSOR_MAP_DATA_TYPE_UINT8 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+   cuuint64_t dims[ 4 ] = { static_cast< cuuint64_t >( a.n[ 0 ] ), static_cast< cuuint64_t >( a.n[ 1 ] ),
+                            static_cast< cuuint64_t >( a.n[ 2 ] ), static_cast< cuuint64_t >( a.nb ) };
+   cuuint64_t strides[ 3 ] = { static_cast< cuuint64_t >( a.ss[ 1 ] * esz ), static_cast< cuuint64_t >( a.ss[ 2 ] * esz ),
+                               static_cast< cuuint64_t >(( a.nb > 1 ? a.sb : a.ss[ 2 ] * a.n[ 2 ] ) * esz ) };
+   if( strides[ 2 ] % 16 ) { strides[ 2 ] = ( strides[ 2 ] + 15 ) / 16 * 16; }
+   cuuint32_t box[ 4 ] = { static_cast< cuuint32_t >( G::WXA ), static_cast< cuuint32_t >( G::WY ), 1, 1 };
+   if( encode_tmap( &z.tmap, dt, a.src, dims, strides, box ) != CUDA_SUCCESS ) { return cudaErrorNotSupported; }
+   z.src = a.src;
+   z.dst = a.dst;
+   for( int i = 0; i < 3; ++i ) {
+      z.n[ i ] = a.n[ i ];
+      z.ss[ i ] = a.ss[ i ];
+      z.ds[ i ] = a.ds[ i ];
+      z.bc[ i ] = a.bc[ i ];
+      for( int k = 0; k < kFusedMaxTaps; ++k ) { z.w[ i ][ k ] = make_float2( a.w[ i ][ k ], a.w[ i ][ k ] ); }
+   }
+   z.nb = a.nb;
+   z.sb = a.sb;
+   z.db = a.db;
+   z.tiles_x = static_cast< int32_t >(( a.n[ 0 ] + G::TX - 1 ) / G::TX );
+   z.tiles_y = static_cast< int32_t >(( a.n[ 1 ] + G::TY - 1 ) / G::TY );
+   z.units = static_cast< int64_t >( z.tiles_x ) * z.tiles_y * a.nb * a.n[ 2 ];
+   z.status = device_status_ptr();
+   if( !z.status ) { return cudaErrorUnknown; }
+   auto kern = fused3d_tma_kernel< TIn, HX, HY, HZ, OX, OY, OZ >;
+   size_t smem = G::BYTES;
+   int per_sm = prepare_kernel( kern, G::NT, smem );
+   if( per_sm < 1 ) { return cudaErrorInvalidConfiguration; }
+   static int const want = getenv( "DIPCU_Z3_CTAS_PER_SM" ) ? atoi( getenv( "DIPCU_Z3_CTAS_PER_SM" )) : 2;
+   if( per_sm > want ) { per_sm = want; }
+   if( per_sm < 1 ) { per_sm = 1; }
+   int64_t nctas = static_cast< int64_t >( sm_count() ) * per_sm;
+   int64_t max_ctas = z.units / ( 4 * HZ + 4 );   // keep chunks long against the 2*HZ halo planes
+   if( nctas > max_ctas ) { nctas = max_ctas; }
+   if( nctas < 1 ) { nctas = 1; }
+   kern<<< static_cast< unsigned >( nctas ), G::NT, smem, s >>>( z );
+   return cudaGetLastError();
+}
 
 template< typename TIn, int HX, int HY, bool OX, bool OY >
 cudaError_t run2d( FusedArgs& a, cudaStream_t s ) {
@@ -18,10 +195,7 @@ cudaError_t run2d( FusedArgs& a, cudaStream_t s ) {
    using L = TileLayout< TX, TY, HX, HY >;
    auto kern = fused2d_kernel< TIn, HX, HY, OX, OY, TX, TY, RX, RY, kNT >;
    size_t smem = L::bytes();
-   if( smem > 48 * 1024 ) {
-      cudaError_t e = cudaFuncSetAttribute( kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast< int >( smem ));
-      if( e != cudaSuccess ) { return e; }
-   }
+   if( prepare_kernel( kern, kNT, smem ) < 1 ) { return cudaErrorInvalidConfiguration; }
    a.tiles_x = static_cast< int32_t >(( a.n[ 0 ] + TX - 1 ) / TX);
    a.tiles_y = static_cast< int32_t >(( a.n[ 1 ] + TY - 1 ) / TY);
    a.zchunks = 1;
@@ -34,14 +208,15 @@ cudaError_t run2d( FusedArgs& a, cudaStream_t s ) {
 
 template< typename TIn, int HX, int HY, int HZ, bool OX, bool OY, bool OZ >
 cudaError_t run3d( FusedArgs& a, cudaStream_t s ) {
+   if( !getenv( "DIPCU_NO_TMA" )) {
+      cudaError_t e = run3d_tma< TIn, HX, HY, HZ, OX, OY, OZ >( a, s );
+      if( e != cudaErrorNotSupported ) { return e; }
+   }
    constexpr int TX = 64, TY = 16, RY = 8;
    using L = TileLayout< TX, TY, HX, HY >;
    auto kern = fused3d_kernel< TIn, HX, HY, HZ, OX, OY, OZ, TX, TY, RY, kNT >;
    size_t smem = L::bytes();
-   if( smem > 48 * 1024 ) {
-      cudaError_t e = cudaFuncSetAttribute( kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast< int >( smem ));
-      if( e != cudaSuccess ) { return e; }
-   }
+   if( prepare_kernel( kern, kNT, smem ) < 1 ) { return cudaErrorInvalidConfiguration; }
    a.tiles_x = static_cast< int32_t >(( a.n[ 0 ] + TX - 1 ) / TX);
    a.tiles_y = static_cast< int32_t >(( a.n[ 1 ] + TY - 1 ) / TY);
    int64_t base = static_cast< int64_t >( a.tiles_x ) * a.tiles_y * a.nb;

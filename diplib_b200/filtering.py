@@ -93,11 +93,17 @@ def _array_use_parameter(values, nd: int, default) -> list:
     return values
 
 
+_BC_CACHE: dict = {}
+
+
 def BoundaryConditionFromString(bc: str) -> int:
     """dip::StringToBoundaryCondition (include/diplib/boundary.h:87-103)."""
-    code = _abi.lib().dipcu_bc_from_string(bc.encode())
-    if code < 0:
-        raise ParameterError("Boundary condition not recognized: " + bc)
+    code = _BC_CACHE.get(bc)
+    if code is None:
+        code = _abi.lib().dipcu_bc_from_string(bc.encode())
+        if code < 0:
+            raise ParameterError("Boundary condition not recognized: " + bc)
+        _BC_CACHE[bc] = code
     return code
 
 
@@ -150,11 +156,10 @@ def _to_host(t: torch.Tensor) -> np.ndarray:
 
 
 def _shares_memory(a: torch.Tensor, b: torch.Tensor) -> bool:
-    if a.device != b.device:
-        return False
-    a0, a1 = a.data_ptr(), a.data_ptr() + max(1, a.untyped_storage().nbytes())
-    b0, b1 = b.data_ptr(), b.data_ptr() + max(1, b.untyped_storage().nbytes())
-    return a.untyped_storage().data_ptr() == b.untyped_storage().data_ptr() or (a0 < b1 and b0 < a1)
+    """True when the two tensors' storages overlap (DIPlib strips such an output first)."""
+    sa, sb = a.untyped_storage(), b.untyped_storage()
+    a0, b0 = sa.data_ptr(), sb.data_ptr()
+    return a0 < b0 + max(1, sb.nbytes()) and b0 < a0 + max(1, sa.nbytes())
 
 
 def GaussFIR(in_, sigmas: Iterable[float] | float = (1.0,), derivativeOrder: Iterable[int] | int = (0,),
@@ -189,11 +194,13 @@ def GaussFIR(in_, sigmas: Iterable[float] | float = (1.0,), derivativeOrder: Ite
             target = None
     din = image_desc(x)
     dout = image_desc(res)
-    stream = torch.cuda.current_stream(x.device).cuda_stream
-    with torch.cuda.device(x.device):
-        check(_abi.lib().dipcu_gauss_fir(
-            ctypes.byref(din), ctypes.byref(dout), (ctypes.c_double * nd)(*sig), (ctypes.c_uint32 * nd)(*ords),
-            (ctypes.c_int32 * nd)(*bcs), float(truncation), ctypes.c_void_p(stream)))
+    args = (ctypes.byref(din), ctypes.byref(dout), (ctypes.c_double * nd)(*sig), (ctypes.c_uint32 * nd)(*ords),
+            (ctypes.c_int32 * nd)(*bcs), float(truncation))
+    if x.device.index == torch.cuda.current_device():
+        check(_abi.lib().dipcu_gauss_fir(*args, ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+    else:
+        with torch.cuda.device(x.device):
+            check(_abi.lib().dipcu_gauss_fir(*args, ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
     if target is not None:
         target.copy_(res)
         res = target

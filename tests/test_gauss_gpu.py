@@ -88,6 +88,11 @@ def test_fuzz_against_oracle(cuda, seed):
     ((30, 40, 50), np.float32, [1.0, 1.0, 1.0], [0, 0, 1], ["asym mirror"]),
     ((40, 40, 40), np.float32, [4.0, 4.0, 4.0], [0, 0, 0], ["mirror"]),
     ((6, 50, 70), np.float32, [2.0, 2.0, 0.0], [0, 0, 0], ["mirror"]),   # z unfiltered: batch axis
+    ((30, 37, 70), np.uint16, [1.5, 1.5, 3.0], [0, 0, 0], ["asym mirror"]),             # mapped y pass
+    ((30, 37, 70), np.float32, [1.5, 1.5, 3.0], [0, 0, 0], ["asym mirror", "add zeros", "mirror"]),  # fix-up, negated
+    ((20, 9, 70), np.uint16, [1.5, 1.5, 3.0], [0, 0, 0], ["mirror"]),                   # halo leaves the box
+    ((25, 30, 130), np.uint16, [1.5, 1.5, 3.0], [1, 0, 0], ["zero order", "periodic", "asym periodic"]),
+    ((300, 16, 64), np.uint16, [1.5, 1.5, 3.0], [0, 0, 0], ["mirror"]),                 # long z, several chunks
 ])
 def test_fused_configs_against_oracle(cuda, case):
     shape, dtype, sig, ords, bcs = case
