@@ -145,6 +145,10 @@ bool try_fused( dipcu_image_desc const* in, dipcu_image_desc const* out, std::ve
 
 } // namespace
 
+int record_error( int code, char const* msg ) {
+   return fail( code, msg );
+}
+
 } // namespace dipcu
 
 using namespace dipcu;

@@ -60,6 +60,9 @@ struct FusedKey {
 
 // Returns cudaErrorNotSupported if no fused kernel exists for `key`.
 cudaError_t launch_fused( FusedKey const& key, FusedArgs& args, cudaStream_t stream );
+
+// Records `msg` as this thread's dipcu_last_error_message() and returns `code`.
+int record_error( int code, char const* msg );
 bool fused_available( FusedKey const& key );
 
 } // namespace dipcu

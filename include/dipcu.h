@@ -78,6 +78,24 @@ int dipcu_gauss_fir( dipcu_image_desc const* in, dipcu_image_desc const* out,
                      double const* sigmas, uint32_t const* orders, int32_t const* bcs,
                      double truncation, void* stream );
 
+/* The same filter for callers that cannot allocate device memory while they run: code whose GPU
+ * memory is all handed out by another allocator (a framework's caching allocator, or a pool
+ * reserved at start-up) so that the process must not grow its footprint behind that allocator's
+ * back, and long-running pipelines that must not fail for lack of memory once started.  No
+ * counterpart in DIPlib (whose CPU filter allocates its line buffers per thread).
+ *
+ * Allocates nothing: the pass intermediates live in a static device array of 32 MiB that the
+ * library holds on every GPU it is used on until the process exits.  Images are limited to
+ * 4 Mi samples when the filter computes in float and 2 Mi samples when it computes in double
+ * (32/64-bit integer or dfloat input); larger images return DIPCU_ERR_INVALID_ARG.  Runs the
+ * line kernel pass by pass.  All calls share the array: calls whose work overlaps on the GPU race
+ * and give wrong results, so order them on one stream.  The first call on a device looks up the
+ * array's address; make it before any stream capture on that device.  Arguments and results
+ * are those of dipcu_gauss_fir. */
+int dipcu_gauss_fir_noalloc( dipcu_image_desc const* in, dipcu_image_desc const* out,
+                             double const* sigmas, uint32_t const* orders, int32_t const* bcs,
+                             double truncation, void* stream );
+
 /* ---- Kernel weights ----------------------------------------------------------------------- */
 
 /* Half-kernel length of dip::MakeHalfGaussian (src/linear/gauss.cpp:38-62): returns
