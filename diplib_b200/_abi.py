@@ -49,6 +49,9 @@ SIGNATURES = {
     "dipcu_gauss_fir_noalloc": (ctypes.c_int, [_P(ImageDesc), _P(ImageDesc), _P(ctypes.c_double),
                                                _P(ctypes.c_uint32), _P(ctypes.c_int32), ctypes.c_double,
                                                ctypes.c_void_p]),
+    "dipcu_gauss_fir_backward": (ctypes.c_int, [_P(ImageDesc), _P(ImageDesc), _P(ImageDesc), ctypes.c_void_p,
+                                                _P(ctypes.c_double), _P(ctypes.c_uint32), _P(ctypes.c_int32),
+                                                ctypes.c_double, ctypes.c_void_p]),
     "dipcu_half_gaussian_length": (ctypes.c_int, [ctypes.c_double, ctypes.c_uint32, ctypes.c_double, ctypes.c_int]),
     "dipcu_make_gauss_weights": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_double,
                                                 ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,

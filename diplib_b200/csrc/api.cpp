@@ -45,15 +45,6 @@ int check_desc( dipcu_image_desc const* d, char const* name ) {
    return DIPCU_OK;
 }
 
-// Per-axis filter as dip::GaussFIR builds it (src/linear/gauss.cpp:255-284).
-struct AxisFilter {
-   bool process = false;
-   int64_t h = 0;
-   int32_t odd = 0;
-   int32_t bc = 0;
-   std::vector< double > taps;  // centre first, rounded to the compute precision
-};
-
 int64_t numel( dipcu_image_desc const* d ) {
    int64_t n = 1;
    for( int k = 0; k < d->ndims; ++k ) { n *= d->sizes[ k ]; }
@@ -149,52 +140,7 @@ int record_error( int code, char const* msg ) {
    return fail( code, msg );
 }
 
-} // namespace dipcu
-
-using namespace dipcu;
-
-extern "C" {
-
-char const* dipcu_last_error_message( void ) {
-   return g_last_error.c_str();
-}
-
-char const* dipcu_version( void ) {
-   return "dipcu 0.1 (sm_100a)";
-}
-
-int dipcu_bc_from_string( char const* bc ) {
-   // dip::StringToBoundaryCondition, include/diplib/boundary.h:87-103.
-   static char const* const names[] = {
-      "mirror", "asym mirror", "antisym reflect", "periodic", "asym periodic", "add zeros", "add max",
-      "add min", "zero order", "first order", "second order", "third order", "already expanded" };
-   if( !bc || bc[ 0 ] == 0 || std::strcmp( bc, "default" ) == 0 ) { return BC_SYMMETRIC_MIRROR; }
-   for( int i = 0; i < 13; ++i ) {
-      if( std::strcmp( bc, names[ i ] ) == 0 ) { return i; }
-   }
-   g_last_error = std::string( "Boundary condition not recognized: " ) + bc;
-   return -1;
-}
-
-int dipcu_half_gaussian_length( double sigma, uint32_t order, double truncation, int dt_double ) {
-   if( order > 3 ) { return -1; }
-   return static_cast< int >( half_gaussian_length( sigma, order, truncation, dt_double != 0 ));
-}
-
-int dipcu_make_gauss_weights( double const* sigmas, uint32_t const* orders, int count, double truncation,
-                              float* weights, float* dweights, int32_t* lengths, int stride, void* stream ) {
-   if( count < 0 || stride < 1 || ( count > 0 && ( !sigmas || !orders || !weights ))) {
-      return fail( DIPCU_ERR_INVALID_ARG, "dipcu_make_gauss_weights: bad arguments" );
-   }
-   cudaError_t e = launch_gauss_weights( sigmas, orders, count, truncation, weights, dweights, lengths, stride,
-                                         static_cast< cudaStream_t >( stream ));
-   if( e != cudaSuccess ) { return cuda_fail( e, "gauss_weights_kernel" ); }
-   return DIPCU_OK;
-}
-
-int dipcu_gauss_fir( dipcu_image_desc const* in, dipcu_image_desc const* out, double const* sigmas,
-                     uint32_t const* orders, int32_t const* bcs, double truncation, void* stream_ ) {
-   cudaStream_t stream = static_cast< cudaStream_t >( stream_ );
+int check_pair( dipcu_image_desc const* in, dipcu_image_desc const* out ) {
    if( int st = check_desc( in, "in" )) { return st; }
    if( int st = check_desc( out, "out" )) { return st; }
    int const nd = in->ndims;
@@ -205,22 +151,24 @@ int dipcu_gauss_fir( dipcu_image_desc const* in, dipcu_image_desc const* out, do
          return fail( DIPCU_ERR_INVALID_ARG, "out: zero stride along an axis of size > 1" );
       }
    }
-   if( !sigmas || !orders || !bcs ) { return fail( DIPCU_ERR_INVALID_ARG, "null parameter array" ); }
-   {
-      uintptr_t ilo, ihi, olo, ohi;
-      byte_range( in, ilo, ihi );
-      byte_range( out, olo, ohi );
-      if( ilo < ohi && olo < ihi ) {
-         return fail( DIPCU_ERR_INVALID_ARG, "out overlaps in (strip the output image first)" );
-      }
+   uintptr_t ilo, ihi, olo, ohi;
+   byte_range( in, ilo, ihi );
+   byte_range( out, olo, ohi );
+   if( ilo < ohi && olo < ihi ) {
+      return fail( DIPCU_ERR_INVALID_ARG, "out overlaps in (strip the output image first)" );
    }
+   return DIPCU_OK;
+}
 
+int build_filters( dipcu_image_desc const* in, double const* sigmas, uint32_t const* orders, int32_t const* bcs,
+                   double truncation, std::vector< AxisFilter >& f, std::vector< std::vector< double >>* dtaps ) {
    // dip::GaussFIR: weight precision follows the input (gauss.cpp:254); the line buffers and
    // the output use dip::DataType::SuggestFlex (convolution.cpp:341-343).
+   int const nd = in->ndims;
    bool const weights_double = in->dtype == DT_DFLOAT;
-   int32_t const buf_dt = suggest_flex( in->dtype );
-   bool const compute_double = buf_dt == DT_DFLOAT;
-   std::vector< AxisFilter > f( static_cast< size_t >( nd ));
+   bool const compute_double = suggest_flex( in->dtype ) == DT_DFLOAT;
+   f.assign( static_cast< size_t >( nd ), AxisFilter{} );
+   if( dtaps ) { dtaps->assign( static_cast< size_t >( nd ), {} ); }
    for( int d = 0; d < nd; ++d ) {
       if( !( sigmas[ d ] > 0.0 ) || in->sizes[ d ] <= 1 ) { continue; }
       if( orders[ d ] > 3 ) {
@@ -241,17 +189,23 @@ int dipcu_gauss_fir( dipcu_image_desc const* in, dipcu_image_desc const* out, do
       a.odd = static_cast< int32_t >( orders[ d ] & 1u );
       a.bc = bcs[ d ];
       a.taps.resize( static_cast< size_t >( len ));
-      make_half_gaussian< double >( sigmas[ d ], orders[ d ], len, a.taps.data(), nullptr );
+      std::vector< double >* dt = dtaps ? &( *dtaps )[ static_cast< size_t >( d ) ] : nullptr;
+      if( dt ) { dt->resize( static_cast< size_t >( len )); }
+      make_half_gaussian< double >( sigmas[ d ], orders[ d ], len, a.taps.data(), dt ? dt->data() : nullptr );
       if( !compute_double ) {
          for( auto& t : a.taps ) { t = static_cast< double >( static_cast< float >( t )); }
+         if( dt ) { for( auto& t : *dt ) { t = static_cast< double >( static_cast< float >( t )); } }
       }
       // IsMeaninglessFilter (convolution.cpp:304-314): a single unit tap.
       if( len == 1 && a.taps[ 0 ] == 1.0 ) { a.process = false; }
    }
+   return DIPCU_OK;
+}
 
-   // Pass order of Framework::Separable: by input stride, stable (framework_separable.cpp:146-165).
+std::vector< int > pass_order( dipcu_image_desc const* in, std::vector< AxisFilter > const& f ) {
+   // Framework::Separable: by input stride, stable (framework_separable.cpp:146-165).
    std::vector< int > order;
-   for( int d = 0; d < nd; ++d ) {
+   for( int d = 0; d < in->ndims; ++d ) {
       if( f[ static_cast< size_t >( d ) ].process ) { order.push_back( d ); }
    }
    for( size_t i = 1; i < order.size(); ++i ) {
@@ -260,7 +214,14 @@ int dipcu_gauss_fir( dipcu_image_desc const* in, dipcu_image_desc const* out, do
       while( j > 0 && in->strides[ order[ j - 1 ] ] > in->strides[ e ] ) { order[ j ] = order[ j - 1 ]; --j; }
       order[ j ] = e;
    }
+   return order;
+}
 
+int run_filters( dipcu_image_desc const* in, dipcu_image_desc const* out, std::vector< AxisFilter > const& f,
+                 bool compute_double, cudaStream_t stream ) {
+   int const nd = in->ndims;
+   int32_t const buf_dt = compute_double ? DT_DFLOAT : DT_SFLOAT;
+   std::vector< int > order = pass_order( in, f );
    if( order.empty() ) {
       ConvertArgs c{};
       c.src = in->data;
@@ -350,6 +311,59 @@ int dipcu_gauss_fir( dipcu_image_desc const* in, dipcu_image_desc const* out, do
    }
    for( int i = 0; i < nscratch; ++i ) { cudaFreeAsync( scratch[ i ], stream ); }
    return status;
+}
+
+} // namespace dipcu
+
+using namespace dipcu;
+
+extern "C" {
+
+char const* dipcu_last_error_message( void ) {
+   return g_last_error.c_str();
+}
+
+char const* dipcu_version( void ) {
+   return "dipcu 0.1 (sm_100a)";
+}
+
+int dipcu_bc_from_string( char const* bc ) {
+   // dip::StringToBoundaryCondition, include/diplib/boundary.h:87-103.
+   static char const* const names[] = {
+      "mirror", "asym mirror", "antisym reflect", "periodic", "asym periodic", "add zeros", "add max",
+      "add min", "zero order", "first order", "second order", "third order", "already expanded" };
+   if( !bc || bc[ 0 ] == 0 || std::strcmp( bc, "default" ) == 0 ) { return BC_SYMMETRIC_MIRROR; }
+   for( int i = 0; i < 13; ++i ) {
+      if( std::strcmp( bc, names[ i ] ) == 0 ) { return i; }
+   }
+   g_last_error = std::string( "Boundary condition not recognized: " ) + bc;
+   return -1;
+}
+
+int dipcu_half_gaussian_length( double sigma, uint32_t order, double truncation, int dt_double ) {
+   if( order > 3 ) { return -1; }
+   return static_cast< int >( half_gaussian_length( sigma, order, truncation, dt_double != 0 ));
+}
+
+int dipcu_make_gauss_weights( double const* sigmas, uint32_t const* orders, int count, double truncation,
+                              float* weights, float* dweights, int32_t* lengths, int stride, void* stream ) {
+   if( count < 0 || stride < 1 || ( count > 0 && ( !sigmas || !orders || !weights ))) {
+      return fail( DIPCU_ERR_INVALID_ARG, "dipcu_make_gauss_weights: bad arguments" );
+   }
+   cudaError_t e = launch_gauss_weights( sigmas, orders, count, truncation, weights, dweights, lengths, stride,
+                                         static_cast< cudaStream_t >( stream ));
+   if( e != cudaSuccess ) { return cuda_fail( e, "gauss_weights_kernel" ); }
+   return DIPCU_OK;
+}
+
+int dipcu_gauss_fir( dipcu_image_desc const* in, dipcu_image_desc const* out, double const* sigmas,
+                     uint32_t const* orders, int32_t const* bcs, double truncation, void* stream_ ) {
+   cudaStream_t stream = static_cast< cudaStream_t >( stream_ );
+   if( int st = check_pair( in, out )) { return st; }
+   if( !sigmas || !orders || !bcs ) { return fail( DIPCU_ERR_INVALID_ARG, "null parameter array" ); }
+   std::vector< AxisFilter > f;
+   if( int st = build_filters( in, sigmas, orders, bcs, truncation, f, nullptr )) { return st; }
+   return run_filters( in, out, f, suggest_flex( in->dtype ) == DT_DFLOAT, stream );
 }
 
 } // extern "C"

@@ -4,12 +4,23 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <vector>
+
 #include "../../include/dipcu.h"
 
 namespace dipcu {
 
 constexpr int kLineMaxHalf = 2048;  // longest half-width the line kernel accepts
 constexpr int kFusedMaxTaps = 65;   // per-axis tap capacity of the fused kernels' parameters
+constexpr int kFoldMaxHalf = 100;   // longest half-width the adjoint's halo fold accepts
+constexpr int kFoldMaxEntries = 1000;
+
+// One coefficient of the boundary extension: halo position j (line coordinate, outside [0, n))
+// takes c * sample i.  The adjoint folds the halo gradient back along these entries.
+struct FoldEntry {
+   int32_t j, i;
+   double c;
+};
 
 // One pass of the line kernel (K2).
 struct LinePass {
@@ -61,8 +72,52 @@ struct FusedKey {
 // Returns cudaErrorNotSupported if no fused kernel exists for `key`.
 cudaError_t launch_fused( FusedKey const& key, FusedArgs& args, cudaStream_t stream );
 
+bool fused_available( FusedKey const& key );
+
+// Adjoint halo fold along one axis (k_backward.cu).
+struct FoldPass {
+   void const* g;            // gradient w.r.t. the forward pass output (compute type)
+   void* xb;                 // gradient w.r.t. the forward pass input (compute type), correlation part
+   int32_t ndims, axis;
+   int64_t sizes[ DIPCU_MAX_DIMS ];
+   int64_t gst[ DIPCU_MAX_DIMS ], xst[ DIPCU_MAX_DIMS ];
+   int64_t h;
+   int32_t odd;
+   bool compute_double;
+   double const* taps;       // h + 1 forward taps, centre first
+   FoldEntry const* entries;
+   int32_t nentries;
+};
+cudaError_t launch_fold( FoldPass const& p, cudaStream_t stream );
+// atomically adds <src, dst> (both of the compute type, layouts as in ConvertArgs) to *out.
+cudaError_t launch_dot( ConvertArgs const& a, bool compute_double, double* out, cudaStream_t stream );
+
 // Records `msg` as this thread's dipcu_last_error_message() and returns `code`.
 int record_error( int code, char const* msg );
-bool fused_available( FusedKey const& key );
+
+// Per-axis filter as dip::GaussFIR builds it (src/linear/gauss.cpp:255-284).
+struct AxisFilter {
+   bool process = false;
+   int64_t h = 0;
+   int32_t odd = 0;
+   int32_t bc = 0;
+   std::vector< double > taps;  // centre first, rounded to the compute precision
+};
+
+// Checks an (in, out) image pair: forged, same sizes, valid types, non-overlapping.
+int check_pair( dipcu_image_desc const* in, dipcu_image_desc const* out );
+
+// dip::GaussFIR's per-axis set-up (sigma <= 0 / size-1 axes skipped, order and BC checks,
+// weights in the precision of the computation).  `dtaps` (optional) receives d(taps)/d(sigma).
+int build_filters( dipcu_image_desc const* in, double const* sigmas, uint32_t const* orders, int32_t const* bcs,
+                   double truncation, std::vector< AxisFilter >& f, std::vector< std::vector< double >>* dtaps );
+
+// Framework::Separable's pass order: processed axes by input stride, stable.
+std::vector< int > pass_order( dipcu_image_desc const* in, std::vector< AxisFilter > const& f );
+
+// Runs the separable filter `f` from `in` to `out` (fused tile kernel when possible, else the
+// line-kernel pass chain), computing in double when `compute_double`.
+int run_filters( dipcu_image_desc const* in, dipcu_image_desc const* out, std::vector< AxisFilter > const& f,
+                 bool compute_double, cudaStream_t stream );
 
 } // namespace dipcu

@@ -1,0 +1,147 @@
+// K3 pieces of the adjoint (backward) of the Gaussian FIR.
+//
+// Along one axis the forward pass is y = C E x: E extends each line by h samples with the
+// boundary condition (detail::ExpandBuffer, src/library/copy_buffer.cpp:751-813 in DIPlib) and C
+// is the tap sum of SeparableConvolutionLineFilter::Filter (src/linear/convolution.cpp:214-241).
+// Its adjoint is x_bar = E^T C^T y_bar.  C^T y_bar restricted to the line is a zero-padded
+// correlation with the flipped kernel (run by the line kernel with "add zeros" and mirrored taps);
+// the part of C^T y_bar that falls on the 2h halo positions is folded back onto the samples each
+// halo sample was made from, with the coefficients of E (host-computed from the same boundary code
+// the forward uses).  fold_kernel does that fold, one thread per line.
+//
+// dot_kernel reduces <a, b> over an image in double: the sigma gradient of axis a is
+// <y_bar, G_a'(x)>, with G_a' the forward filter whose axis-a taps are d(taps)/d(sigma).
+#include <cuda_runtime.h>
+
+#include "dipcu_common.cuh"
+#include "dipcu_internal.h"
+
+namespace dipcu {
+
+namespace {
+
+template< typename T >
+struct FoldArgs {
+   T const* g;               // gradient w.r.t. the pass output (input of this adjoint pass)
+   T* xb;                    // gradient w.r.t. the pass input, holding the correlation part already
+   int32_t ndims, axis;
+   int64_t sizes[ DIPCU_MAX_DIMS ];
+   int64_t gst[ DIPCU_MAX_DIMS ], xst[ DIPCU_MAX_DIMS ];
+   int64_t n, nlines;
+   int32_t h, odd, nentries;
+   T w[ kFoldMaxHalf + 1 ];  // forward taps, centre first
+   FoldEntry e[ kFoldMaxEntries ];
+};
+
+template< typename T >
+__global__ void fold_kernel( FoldArgs< T > const __grid_constant__ a ) {
+   int64_t const line = static_cast< int64_t >( blockIdx.x ) * blockDim.x + threadIdx.x;
+   if( line >= a.nlines ) { return; }
+   int64_t rem = line, gb = 0, xbb = 0;
+   for( int d = 0; d < a.ndims; ++d ) {
+      if( d == a.axis ) { continue; }
+      int64_t c = rem % a.sizes[ d ];
+      rem /= a.sizes[ d ];
+      gb += c * a.gst[ d ];
+      xbb += c * a.xst[ d ];
+   }
+   int64_t const gs = a.gst[ a.axis ], xs = a.xst[ a.axis ];
+   int32_t jprev = 0x7fffffff;
+   double zj = 0.0;
+   for( int k = 0; k < a.nentries; ++k ) {
+      FoldEntry const en = a.e[ k ];
+      if( en.j != jprev ) {
+         // Halo gradient: z_bar_j = sum_t g_t w_{j-t} over in-range t with |j - t| <= h.
+         jprev = en.j;
+         zj = 0.0;
+         int64_t t0 = en.j - a.h, t1 = en.j + a.h;
+         if( t0 < 0 ) { t0 = 0; }
+         if( t1 > a.n - 1 ) { t1 = a.n - 1; }
+         for( int64_t t = t0; t <= t1; ++t ) {
+            int64_t kk = en.j - t;
+            int64_t ak = kk < 0 ? -kk : kk;
+            double wk = static_cast< double >( a.w[ ak ] );
+            if( a.odd && kk < 0 ) { wk = -wk; }
+            zj += wk * static_cast< double >( a.g[ gb + t * gs ] );
+         }
+      }
+      T* p = a.xb + xbb + static_cast< int64_t >( en.i ) * xs;
+      *p = static_cast< T >( static_cast< double >( *p ) + en.c * zj );
+   }
+}
+
+template< typename T >
+__global__ void __launch_bounds__( 256 ) dot_kernel( ConvertArgs const __grid_constant__ a, double* out ) {
+   // <src, dst> over all samples; src/dst reuse ConvertArgs' layout fields (both of type T).
+   double acc = 0.0;
+   for( int64_t e = static_cast< int64_t >( blockIdx.x ) * blockDim.x + threadIdx.x; e < a.total;
+        e += static_cast< int64_t >( gridDim.x ) * blockDim.x ) {
+      int64_t rem = e, so = 0, doff = 0;
+      for( int d = 0; d < a.ndims; ++d ) {
+         int64_t c = rem % a.sizes[ d ];
+         rem /= a.sizes[ d ];
+         so += c * a.sst[ d ];
+         doff += c * a.dstst[ d ];
+      }
+      acc += static_cast< double >( static_cast< T const* >( a.src )[ so ] ) *
+             static_cast< double >( static_cast< T const* >( a.dst )[ doff ] );
+   }
+   for( int off = 16; off > 0; off >>= 1 ) { acc += __shfl_down_sync( 0xffffffffu, acc, off ); }
+   __shared__ double part[ 8 ];
+   int const lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+   if( lane == 0 ) { part[ warp ] = acc; }
+   __syncthreads();
+   if( warp == 0 ) {
+      acc = lane < static_cast< int >( blockDim.x >> 5 ) ? part[ lane ] : 0.0;
+      for( int off = 4; off > 0; off >>= 1 ) { acc += __shfl_down_sync( 0xffffffffu, acc, off ); }
+      if( lane == 0 ) { atomicAdd( out, acc ); }
+   }
+}
+
+template< typename T >
+cudaError_t run_fold( FoldPass const& p, cudaStream_t s ) {
+   FoldArgs< T > a{};
+   a.g = static_cast< T const* >( p.g );
+   a.xb = static_cast< T* >( p.xb );
+   a.ndims = p.ndims;
+   a.axis = p.axis;
+   a.n = p.sizes[ p.axis ];
+   a.nlines = 1;
+   for( int d = 0; d < p.ndims; ++d ) {
+      a.sizes[ d ] = p.sizes[ d ];
+      a.gst[ d ] = p.gst[ d ];
+      a.xst[ d ] = p.xst[ d ];
+      if( d != p.axis ) { a.nlines *= p.sizes[ d ]; }
+   }
+   a.h = static_cast< int32_t >( p.h );
+   a.odd = p.odd;
+   a.nentries = p.nentries;
+   for( int k = 0; k <= p.h; ++k ) { a.w[ k ] = static_cast< T >( p.taps[ k ] ); }
+   for( int k = 0; k < p.nentries; ++k ) { a.e[ k ] = p.entries[ k ]; }
+   if( a.nentries == 0 || a.nlines == 0 ) { return cudaSuccess; }
+   int64_t blocks = ( a.nlines + 127 ) / 128;
+   if( blocks > 0x7fffffff ) { return cudaErrorInvalidValue; }
+   fold_kernel< T ><<< static_cast< unsigned >( blocks ), 128, 0, s >>>( a );
+   return cudaGetLastError();
+}
+
+} // namespace
+
+cudaError_t launch_fold( FoldPass const& p, cudaStream_t stream ) {
+   if( p.h < 0 || p.h > kFoldMaxHalf || p.nentries > kFoldMaxEntries ) { return cudaErrorInvalidValue; }
+   return p.compute_double ? run_fold< double >( p, stream ) : run_fold< float >( p, stream );
+}
+
+cudaError_t launch_dot( ConvertArgs const& a, bool compute_double, double* out, cudaStream_t stream ) {
+   int64_t blocks = ( a.total + 255 ) / 256;
+   if( blocks > 148 * 8 ) { blocks = 148 * 8; }
+   if( blocks < 1 ) { blocks = 1; }
+   if( compute_double ) {
+      dot_kernel< double ><<< static_cast< unsigned >( blocks ), 256, 0, stream >>>( a, out );
+   } else {
+      dot_kernel< float ><<< static_cast< unsigned >( blocks ), 256, 0, stream >>>( a, out );
+   }
+   return cudaGetLastError();
+}
+
+} // namespace dipcu

@@ -96,6 +96,22 @@ int dipcu_gauss_fir_noalloc( dipcu_image_desc const* in, dipcu_image_desc const*
                              double const* sigmas, uint32_t const* orders, int32_t const* bcs,
                              double truncation, void* stream );
 
+/* ---- Backward (adjoint) ------------------------------------------------------------------- */
+
+/* Gradients of dipcu_gauss_fir (no DIPlib counterpart; DIPlib has no derivatives of its filters).
+ * `grad_out`: dL/d(out), of the filter's computation type (sfloat, or dfloat for 32/64-bit
+ * integer and dfloat input).  `grad_in` (optional, same type): receives dL/d(in), the adjoint of
+ * the forward pass by pass -- zero-padded correlation with the flipped kernel, then the halo
+ * gradients folded back through the boundary extension (every boundary condition; half-widths up to
+ * 100).  `grad_sigma` (optional, DEVICE array of ndims doubles): receives dL/d(sigma_d) for each
+ * filtered axis (0 elsewhere), from the analytic derivative of the normalised discrete kernel
+ * with its length held fixed; needs `in`.  Recomputes what it needs from `in`; allocates its
+ * intermediates with cudaMallocAsync on `stream`. */
+int dipcu_gauss_fir_backward( dipcu_image_desc const* grad_out, dipcu_image_desc const* in,
+                              dipcu_image_desc const* grad_in, double* grad_sigma,
+                              double const* sigmas, uint32_t const* orders, int32_t const* bcs,
+                              double truncation, void* stream );
+
 /* ---- Kernel weights ----------------------------------------------------------------------- */
 
 /* Half-kernel length of dip::MakeHalfGaussian (src/linear/gauss.cpp:38-62): returns

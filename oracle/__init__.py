@@ -176,6 +176,27 @@ def gauss_fir(x: np.ndarray, sigmas: Sequence[float] = (1.0,), orders: Sequence[
     return out
 
 
+def separable_fir(x: np.ndarray, taps, odd, bcs, out_dtype=None) -> np.ndarray:
+    """The restated dip::SeparableConvolution with given EVEN/ODD half kernels, centre tap first
+    (per axis, DIPlib order; None leaves an axis unfiltered)."""
+    nd = x.ndim
+    out_dt = suggest_flex(x.dtype) if out_dtype is None else np.dtype(out_dtype)
+    out = np.zeros(x.shape, out_dt)
+    sizes, in_strides = _dip_geometry(x)
+    _, out_strides = _dip_geometry(out)
+    keep = [None if t is None else np.ascontiguousarray(t, np.float64) for t in taps]
+    ptrs = (ctypes.c_void_p * nd)(*[None if t is None else t.ctypes.data for t in keep])
+    lens = (ctypes.c_int * nd)(*[0 if t is None else t.size for t in keep])
+    bcl = _broadcast(bcs, nd, "mirror")
+    st = oracle_lib().or_separable_fir(
+        ctypes.c_void_p(x.ctypes.data), DTYPE_CODES[x.dtype], nd, sizes, in_strides,
+        ctypes.c_void_p(out.ctypes.data), DTYPE_CODES[out_dt], out_strides, ptrs, lens,
+        (ctypes.c_int * nd)(*[int(o) for o in odd]), (ctypes.c_int * nd)(*[bc_code(b) for b in bcl]))
+    if st != 0:
+        raise RuntimeError(f"or_separable_fir failed ({st})")
+    return out
+
+
 def structure_tensor(x: np.ndarray, grad_sigma: float, tensor_sigma: float, bc: str = "mirror",
                      truncation: float = 3.0) -> np.ndarray:
     """dip::StructureTensor (src/analysis/structure_tensor.cpp:33-59) built from the restated

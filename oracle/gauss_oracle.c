@@ -435,45 +435,27 @@ static void line_filter_f64( double const* in, double* out, size_t length, doubl
 
 #define OR_MAX_DIMS 16
 
-int or_gauss_fir( void const* in, int in_dtype, int ndims, int64_t const* sizes, int64_t const* in_strides,
-                  void* out, int out_dtype, int64_t const* out_strides,
-                  double const* sigmas, unsigned const* orders, int const* bcs, double truncation ) {
+/* dip::SeparableConvolution (src/linear/convolution.cpp:319-421) for real EVEN / ODD filters given as
+ * half kernels with the centre FIRST (the reversed storage of InternOneDimensionalFilter), driven by
+ * Framework::Separable (src/library/framework_separable.cpp:35-431).  `taps[d]` NULL (or len 0) leaves
+ * axis d unprocessed.  Taps are rounded to float when the buffer type is sfloat (convolution.cpp:149-150). */
+int or_separable_fir( void const* in, int in_dtype, int ndims, int64_t const* sizes, int64_t const* in_strides,
+                      void* out, int out_dtype, int64_t const* out_strides,
+                      double const* const* taps, int const* lens, int const* odd, int const* bcs ) {
    if( ndims < 1 || ndims > OR_MAX_DIMS || dtype_size( in_dtype ) == 0 || dtype_size( out_dtype ) == 0 ) {
       return OR_ERR_ARG;
    }
-   /* GaussFIR: weight type (gauss.cpp:254) and per-dimension filters (:255-284). */
-   int weights_double = ( in_dtype == OR_DFLOAT );
-   /* SeparableConvolution: buffer type (convolution.cpp:341-343). */
    int buf_type = or_suggest_flex( in_dtype );
    int buf_double = ( buf_type == OR_DFLOAT );
-
    int process[ OR_MAX_DIMS ];
-   size_t half[ OR_MAX_DIMS ];           /* border = dataSize - 1 */
-   double* taps[ OR_MAX_DIMS ] = { 0 };  /* reversed half kernel, f[0] = centre */
-   int odd[ OR_MAX_DIMS ];
-   int status = OR_OK;
+   size_t half[ OR_MAX_DIMS ];
    size_t npix = 1;
    for( int d = 0; d < ndims; ++d ) {
       npix *= (size_t)sizes[ d ];
-   }
-   for( int d = 0; d < ndims; ++d ) {
-      process[ d ] = ( sigmas[ d ] > 0.0 ) && ( sizes[ d ] > 1 );
-      if( !process[ d ] ) { continue; }
-      if( orders[ d ] > 3 ) { status = OR_ERR_ORDER; goto done; }
-      int len = or_make_half_gaussian( sigmas[ d ], orders[ d ], truncation, weights_double, NULL, 0 );
-      double* h = (double*)malloc( sizeof( double ) * (size_t)len );
-      or_make_half_gaussian( sigmas[ d ], orders[ d ], truncation, weights_double, h, len );
-      taps[ d ] = (double*)malloc( sizeof( double ) * (size_t)len );
-      for( int k = 0; k < len; ++k ) {
-         /* CopyReverseData to float or double (convolution.cpp:50-58, 149-150). */
-         taps[ d ][ k ] = buf_double ? h[ len - 1 - k ] : (double)(float)h[ len - 1 - k ];
-      }
-      free( h );
-      half[ d ] = (size_t)len - 1;
-      odd[ d ] = ( orders[ d ] & 1 ) != 0;
-      /* IsMeaninglessFilter (convolution.cpp:304-314): a single tap equal to 1. */
-      if( len == 1 && taps[ d ][ 0 ] == 1.0 ) { process[ d ] = 0; }
-      if( bcs[ d ] < 0 || bcs[ d ] >= OR_BC_ALREADY_EXPANDED ) { status = OR_ERR_BC; goto done; }
+      process[ d ] = taps && taps[ d ] && lens[ d ] > 0 && sizes[ d ] > 1;
+      half[ d ] = process[ d ] ? (size_t)lens[ d ] - 1 : 0;
+      if( process[ d ] && lens[ d ] == 1 && taps[ d ][ 0 ] == 1.0 ) { process[ d ] = 0; }
+      if( process[ d ] && ( bcs[ d ] < 0 || bcs[ d ] >= OR_BC_ALREADY_EXPANDED )) { return OR_ERR_BC; }
    }
 
    /* Framework::Separable: processing order by input stride, stable insertion sort
@@ -501,7 +483,7 @@ int or_gauss_fir( void const* in, int in_dtype, int ndims, int64_t const* sizes,
          put_sample( out, out_dtype, oo, get_sample( in, in_dtype, io ));
          for( int d = 0; d < ndims; ++d ) { if( ++coord[ d ] < sizes[ d ] ) { break; } coord[ d ] = 0; }
       }
-      goto done;
+      return OR_OK;
    }
 
    /* in -> output -> output ... (or via an intermediate of the buffer type when the output type
@@ -572,7 +554,36 @@ int or_gauss_fir( void const* in, int in_dtype, int ndims, int64_t const* sizes,
    free( outbuf );
    free( ftaps );
    free( inter );
+   return OR_OK;
+}
 
+int or_gauss_fir( void const* in, int in_dtype, int ndims, int64_t const* sizes, int64_t const* in_strides,
+                  void* out, int out_dtype, int64_t const* out_strides,
+                  double const* sigmas, unsigned const* orders, int const* bcs, double truncation ) {
+   if( ndims < 1 || ndims > OR_MAX_DIMS || dtype_size( in_dtype ) == 0 || dtype_size( out_dtype ) == 0 ) {
+      return OR_ERR_ARG;
+   }
+   /* GaussFIR: weight type (gauss.cpp:254) and per-dimension filters (:255-284). */
+   int weights_double = ( in_dtype == OR_DFLOAT );
+   double* taps[ OR_MAX_DIMS ] = { 0 };  /* reversed half kernel, f[0] = centre */
+   int lens[ OR_MAX_DIMS ] = { 0 };
+   int odd[ OR_MAX_DIMS ] = { 0 };
+   int status = OR_OK;
+   for( int d = 0; d < ndims; ++d ) {
+      if( !(( sigmas[ d ] > 0.0 ) && ( sizes[ d ] > 1 ))) { continue; }
+      if( orders[ d ] > 3 ) { status = OR_ERR_ORDER; goto done; }
+      if( bcs[ d ] < 0 || bcs[ d ] >= OR_BC_ALREADY_EXPANDED ) { status = OR_ERR_BC; goto done; }
+      int len = or_make_half_gaussian( sigmas[ d ], orders[ d ], truncation, weights_double, NULL, 0 );
+      double* h = (double*)malloc( sizeof( double ) * (size_t)len );
+      or_make_half_gaussian( sigmas[ d ], orders[ d ], truncation, weights_double, h, len );
+      taps[ d ] = (double*)malloc( sizeof( double ) * (size_t)len );
+      for( int k = 0; k < len; ++k ) { taps[ d ][ k ] = h[ len - 1 - k ]; }   /* CopyReverseData */
+      free( h );
+      lens[ d ] = len;
+      odd[ d ] = ( orders[ d ] & 1 ) != 0;
+   }
+   status = or_separable_fir( in, in_dtype, ndims, sizes, in_strides, out, out_dtype, out_strides,
+                              (double const* const*)taps, lens, odd, bcs );
 done:
    for( int d = 0; d < ndims; ++d ) { free( taps[ d ] ); }
    return status;

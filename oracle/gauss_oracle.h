@@ -61,6 +61,12 @@ int or_gauss_fir( void const* in, int in_dtype, int ndims, int64_t const* sizes,
                   void* out, int out_dtype, int64_t const* out_strides,
                   double const* sigmas, unsigned const* orders, int const* bcs, double truncation );
 
+/* dip::SeparableConvolution with caller-supplied EVEN (odd[d] = 0) / ODD (odd[d] = 1) real filters:
+ * taps[d] holds lens[d] values, the centre tap FIRST; taps[d] == NULL leaves axis d unfiltered. */
+int or_separable_fir( void const* in, int in_dtype, int ndims, int64_t const* sizes, int64_t const* in_strides,
+                      void* out, int out_dtype, int64_t const* out_strides,
+                      double const* const* taps, int const* lens, int const* odd, int const* bcs );
+
 /* Output/compute type rule: DataType::SuggestFlex, src/library/datatype.cpp:109-124. */
 int or_suggest_flex( int dtype );
 
