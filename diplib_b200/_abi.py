@@ -52,6 +52,15 @@ SIGNATURES = {
     "dipcu_gauss_fir_backward": (ctypes.c_int, [_P(ImageDesc), _P(ImageDesc), _P(ImageDesc), ctypes.c_void_p,
                                                 _P(ctypes.c_double), _P(ctypes.c_uint32), _P(ctypes.c_int32),
                                                 ctypes.c_double, ctypes.c_void_p]),
+    "dipcu_batch_plan_create": (ctypes.c_int, [_P(ImageDesc), _P(ImageDesc), ctypes.c_int, _P(ctypes.c_double),
+                                               _P(ctypes.c_uint32), _P(ctypes.c_int32), ctypes.c_double, ctypes.c_int,
+                                               _P(ctypes.c_void_p)]),
+    "dipcu_batch_plan_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "dipcu_batch_plan_info": (ctypes.c_int, [ctypes.c_void_p, _P(ctypes.c_int), _P(ctypes.c_int), _P(ctypes.c_int),
+                                             _P(ctypes.c_int)]),
+    "dipcu_batch_plan_sigmas": (ctypes.c_void_p, [ctypes.c_void_p]),
+    "dipcu_batch_plan_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "dipcu_device_status": (ctypes.c_int, [_P(ctypes.c_int), ctypes.c_int]),
     "dipcu_half_gaussian_length": (ctypes.c_int, [ctypes.c_double, ctypes.c_uint32, ctypes.c_double, ctypes.c_int]),
     "dipcu_make_gauss_weights": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_double,
                                                 ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,

@@ -1,0 +1,554 @@
+// K4: batched Gaussian FIR -- many 2D sfloat images of uneven sizes, each with its own sigmas,
+// derivative orders and boundary conditions, filtered by ONE persistent launch.
+//
+// A plan (dipcu_batch_plan_*) uploads a table of per-image descriptors, a list of (image, tile)
+// work items sorted by cost, and a device table of (sigma, order) per image axis.  Each run:
+//   1. resets the work-queue counter,
+//   2. builds every image's kernel weights on the device (K0, gauss_weights_kernel), so that a
+//      captured run can be replayed after the sigma table is updated in place,
+//   3. launches the persistent kernel: #SMs x occupancy CTAs pop work items from the queue with
+//      one atomicAdd per tile (no waits) until it is empty, and filter their tile with the fused
+//      2D routine specialised for the image's half-width bucket (4, 8, 16 or 32; taps beyond the
+//      image's own half-width are zero).
+// The three steps are captured once into a CUDA graph; a run is one graph launch.  Tile shapes
+// are chosen by an autotuner that times the candidates on the plan's own batch.
+//
+// Items that name a non-existent image or tile (a corrupted queue) are skipped and reported as
+// DIPCU_ERR_INVALID_ARG in the device status word -- the kernel never waits on anything.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "dipcu_common.cuh"
+#include "dipcu_internal.h"
+#include "fused.cuh"
+
+namespace dipcu {
+
+cudaError_t launch_gauss_weights( double const* sigmas, uint32_t const* orders, int count, double truncation,
+                                  float* weights, float* dweights, int32_t* lengths, int stride, cudaStream_t stream );
+int32_t* device_status_ptr();
+
+namespace {
+
+constexpr int kBankStride = 40;   // weight-bank entry: up to 33 taps (half-width 32), padded
+constexpr int kBuckets[ 4 ] = { 4, 8, 16, 32 };
+
+struct BatchImage {
+   float const* src;
+   float* dst;
+   int64_t n[ 2 ];
+   int64_t ss[ 2 ], ds[ 2 ];     // x strides are 1
+   int32_t bc[ 2 ], h[ 2 ], odd[ 2 ];
+   int32_t wofs[ 2 ];            // weight-bank offsets (floats) of the x and y kernels
+   int32_t tiles_x, tiles_y;
+   int32_t bucket;
+   int32_t pad;
+};
+
+struct BatchItem {
+   int32_t image, tile;
+};
+
+struct BatchArgs {
+   BatchImage const* images;
+   BatchItem const* items;
+   float const* wbank;
+   int32_t* counter;
+   int32_t* status;
+   int32_t nimages, nitems;
+};
+
+template< int HB, int TX, int TY >
+struct BatchLayout {
+   static constexpr int WX = TX + 2 * HB;
+   static constexpr int WY = TY + 2 * HB;
+   static constexpr int PB = AlignUp4< WX >::value + 4;
+   static constexpr int A_FLOATS = AlignUp4< WY * WX >::value;
+   static constexpr int B_FLOATS = TY * PB;
+   static constexpr size_t bytes() {
+      return ( A_FLOATS + B_FLOATS ) * sizeof( float ) + WY * sizeof( int64_t ) + WX * sizeof( int32_t ) + WY + WX + 16;
+   }
+};
+
+// y pass of one column over RY output rows, centred at row HB of the staged block (push form:
+// every staged sample feeds the outputs it reaches; tap indices are compile-time constants).
+template< int HB, int RY, bool ODD >
+__device__ __forceinline__ void batch_ypass( float const* A, int pitch, int c, int r0, float const ( &w )[ HB + 1 ],
+                                             float* B, int pb ) {
+   float acc[ RY ];
+#pragma unroll
+   for( int i = 0; i < RY; ++i ) { acc[ i ] = 0.0f; }
+#pragma unroll
+   for( int j = 0; j < RY + 2 * HB; ++j ) {
+      float v = A[ ( r0 + j ) * pitch + c ];
+#pragma unroll
+      for( int i = 0; i < RY; ++i ) {
+         int const k = j - i - HB;                   // input row = output row + k
+         if( k >= -HB && k <= HB ) {
+            float const wk = w[ k < 0 ? -k : k ];
+            acc[ i ] = fmaf(( ODD && k < 0 ) ? -wk : wk, v, acc[ i ] );
+         }
+      }
+   }
+#pragma unroll
+   for( int i = 0; i < RY; ++i ) { B[ ( r0 + i ) * pb + c ] = acc[ i ]; }
+}
+
+template< int HB, int RX, bool ODD >
+__device__ __forceinline__ void batch_xpass( float const* Brow, int x, float const ( &w )[ HB + 1 ], float* out ) {
+   constexpr int NV = AlignUp4< RX + 2 * HB >::value;
+   float acc[ RX ];
+#pragma unroll
+   for( int i = 0; i < RX; ++i ) { acc[ i ] = 0.0f; }
+   float4 const* p = reinterpret_cast< float4 const* >( Brow + x );
+#pragma unroll
+   for( int q = 0; q < NV / 4; ++q ) {
+      float4 f = p[ q ];
+      float const vv[ 4 ] = { f.x, f.y, f.z, f.w };
+#pragma unroll
+      for( int e = 0; e < 4; ++e ) {
+         int const j = 4 * q + e;
+#pragma unroll
+         for( int i = 0; i < RX; ++i ) {
+            int const k = j - i - HB;
+            if( k >= -HB && k <= HB ) {
+               float const wk = w[ k < 0 ? -k : k ];
+               acc[ i ] = fmaf(( ODD && k < 0 ) ? -wk : wk, vv[ e ], acc[ i ] );
+            }
+         }
+      }
+   }
+#pragma unroll
+   for( int i = 0; i < RX; ++i ) { out[ i ] = acc[ i ]; }
+}
+
+template< int HB, int TX, int TY >
+__device__ void batch_tile( BatchImage const& im, int tile, float const* wbank, unsigned char* smem_raw ) {
+   using L = BatchLayout< HB, TX, TY >;
+   constexpr int NT = 256, RY = 8, RX = 4;
+   float* A = reinterpret_cast< float* >( smem_raw );
+   float* B = A + L::A_FLOATS;
+   int64_t* rowoff = reinterpret_cast< int64_t* >( B + L::B_FLOATS );
+   int32_t* colidx = reinterpret_cast< int32_t* >( rowoff + L::WY );
+   uint8_t* rfl = reinterpret_cast< uint8_t* >( colidx + L::WX );
+   uint8_t* cfl = rfl + L::WY;
+   int const tid = static_cast< int >( threadIdx.x );
+   int64_t const tx = tile % im.tiles_x, ty = tile / im.tiles_x;
+   int64_t const x0 = tx * TX, y0 = ty * TY;
+   float wx[ HB + 1 ], wy[ HB + 1 ];
+#pragma unroll
+   for( int k = 0; k <= HB; ++k ) {
+      wx[ k ] = k <= im.h[ 0 ] ? __ldg( wbank + im.wofs[ 0 ] + k ) : 0.0f;
+      wy[ k ] = k <= im.h[ 1 ] ? __ldg( wbank + im.wofs[ 1 ] + k ) : 0.0f;
+   }
+   // Boundary maps of the staged block (HB halo on every side; beyond the image's own
+   // half-width the taps are zero).
+   for( int r = tid; r < L::WY; r += NT ) {
+      int64_t yi; uint8_t fl;
+      map_coord( y0 - HB + r, im.n[ 1 ], im.bc[ 1 ], yi, fl );
+      rowoff[ r ] = yi * im.ss[ 1 ];
+      rfl[ r ] = fl;
+   }
+   for( int c = tid; c < L::WX; c += NT ) {
+      int64_t xi; uint8_t fl;
+      map_coord( x0 - HB + c, im.n[ 0 ], im.bc[ 0 ], xi, fl );
+      colidx[ c ] = static_cast< int32_t >( xi );
+      cfl[ c ] = fl;
+   }
+   __syncthreads();
+   for( int e = tid; e < L::WY * L::WX; e += NT ) {
+      int r = e / L::WX;
+      int c = e - r * L::WX;
+      uint8_t fl = static_cast< uint8_t >( rfl[ r ] | cfl[ c ] );
+      float v = 0.0f;
+      if( !( fl & 2 )) {
+         v = im.src[ rowoff[ r ] + colidx[ c ] ];
+         if(( rfl[ r ] ^ cfl[ c ] ) & 1 ) { v = -v; }
+      }
+      A[ e ] = v;
+   }
+   __syncthreads();
+   for( int item = tid; item < L::WX * ( TY / RY ); item += NT ) {
+      int c = item % L::WX;
+      int rb = item / L::WX;
+      if( im.odd[ 1 ] ) { batch_ypass< HB, RY, true >( A, L::WX, c, rb * RY, wy, B, L::PB ); }
+      else { batch_ypass< HB, RY, false >( A, L::WX, c, rb * RY, wy, B, L::PB ); }
+   }
+   __syncthreads();
+   constexpr int NSEG = TX / RX;
+   for( int item = tid; item < TY * NSEG; item += NT ) {
+      int s = item % NSEG;
+      int r = item / NSEG;
+      int64_t y = y0 + r;
+      int64_t x = x0 + s * RX;
+      if( y >= im.n[ 1 ] || x >= im.n[ 0 ] ) { continue; }
+      float out[ RX ];
+      if( im.odd[ 0 ] ) { batch_xpass< HB, RX, true >( B + r * L::PB, s * RX, wx, out ); }
+      else { batch_xpass< HB, RX, false >( B + r * L::PB, s * RX, wx, out ); }
+      store_row< RX >( im.dst + y * im.ds[ 1 ] + x, x, im.n[ 0 ], out );
+   }
+   __syncthreads();   // smem reused by the next item
+}
+
+template< int TX, int TY >
+__global__ void __launch_bounds__( 256 ) batch_kernel( BatchArgs const __grid_constant__ a ) {
+   extern __shared__ float4 smem4[];
+   __shared__ int item_s;
+   unsigned char* smem = reinterpret_cast< unsigned char* >( smem4 );
+   for( ;; ) {
+      if( threadIdx.x == 0 ) { item_s = atomicAdd( a.counter, 1 ); }
+      __syncthreads();
+      int const it = item_s;
+      __syncthreads();
+      if( it >= a.nitems ) { break; }
+      BatchItem const item = a.items[ it ];
+      if( item.image < 0 || item.image >= a.nimages ) {
+         if( threadIdx.x == 0 ) { atomicExch( a.status, DIPCU_ERR_INVALID_ARG ); }
+         continue;
+      }
+      BatchImage const im = a.images[ item.image ];
+      if( item.tile < 0 || item.tile >= im.tiles_x * im.tiles_y || im.bucket < 0 || im.bucket > 3 ) {
+         if( threadIdx.x == 0 ) { atomicExch( a.status, DIPCU_ERR_INVALID_ARG ); }
+         continue;
+      }
+      switch( im.bucket ) {
+         case 0: batch_tile< 4, TX, TY >( im, item.tile, a.wbank, smem ); break;
+         case 1: batch_tile< 8, TX, TY >( im, item.tile, a.wbank, smem ); break;
+         case 2: batch_tile< 16, TX, TY >( im, item.tile, a.wbank, smem ); break;
+         default: batch_tile< 32, TX, TY >( im, item.tile, a.wbank, smem ); break;
+      }
+   }
+}
+
+// Candidate tile shapes (the autotuner's search space).
+struct TileShape { int tx, ty; };
+constexpr TileShape kShapes[ 3 ] = { { 64, 32 }, { 64, 16 }, { 128, 32 } };
+
+template< int TX, int TY >
+size_t batch_smem() { return BatchLayout< 32, TX, TY >::bytes(); }
+
+size_t shape_smem( int s ) {
+   switch( s ) {
+      case 0: return batch_smem< 64, 32 >();
+      case 1: return batch_smem< 64, 16 >();
+      default: return batch_smem< 128, 32 >();
+   }
+}
+
+void const* shape_kernel( int s ) {
+   switch( s ) {
+      case 0: return reinterpret_cast< void const* >( &batch_kernel< 64, 32 > );
+      case 1: return reinterpret_cast< void const* >( &batch_kernel< 64, 16 > );
+      default: return reinterpret_cast< void const* >( &batch_kernel< 128, 32 > );
+   }
+}
+
+cudaError_t launch_shape( int s, int grid, BatchArgs const& a, cudaStream_t st ) {
+   size_t smem = shape_smem( s );
+   switch( s ) {
+      case 0: batch_kernel< 64, 32 ><<< grid, 256, smem, st >>>( a ); break;
+      case 1: batch_kernel< 64, 16 ><<< grid, 256, smem, st >>>( a ); break;
+      default: batch_kernel< 128, 32 ><<< grid, 256, smem, st >>>( a ); break;
+   }
+   return cudaGetLastError();
+}
+
+int shape_grid( int s ) {
+   static std::mutex mu;
+   static std::map< std::pair< int, int >, int > cache;
+   int dev = 0;
+   cudaGetDevice( &dev );
+   std::lock_guard< std::mutex > lock( mu );
+   auto key = std::make_pair( s, dev );
+   auto it = cache.find( key );
+   if( it != cache.end() ) { return it->second; }
+   size_t smem = shape_smem( s );
+   if( cudaFuncSetAttribute( shape_kernel( s ), cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast< int >( smem )) != cudaSuccess ) {
+      return -1;
+   }
+   int per_sm = 0, sms = 148;
+   if( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &per_sm, shape_kernel( s ), 256, smem ) != cudaSuccess || per_sm < 1 ) {
+      return -1;
+   }
+   cudaDeviceGetAttribute( &sms, cudaDevAttrMultiProcessorCount, dev );
+   cache[ key ] = per_sm * sms;
+   return per_sm * sms;
+}
+
+// Autotune results: batch signature -> tile shape.
+std::mutex g_tune_mu;
+std::map< std::string, int > g_tune_cache;
+
+} // namespace
+
+} // namespace dipcu
+
+using namespace dipcu;
+
+struct dipcu_batch_plan {
+   int device = 0;
+   int count = 0;
+   int shape = 0;
+   int grid = 0;
+   double truncation = 3.0;
+   std::vector< BatchImage > images;       // host copy (tiles depend on the shape)
+   std::vector< double > sig_host;
+   std::vector< uint32_t > ord_host;
+   BatchImage* d_images = nullptr;
+   BatchItem* d_items = nullptr;
+   double* d_sigmas = nullptr;
+   uint32_t* d_orders = nullptr;
+   float* d_bank = nullptr;
+   int32_t* d_counter = nullptr;
+   int nitems = 0;
+   cudaStream_t cap_stream = nullptr;
+   cudaGraph_t graph = nullptr;
+   cudaGraphExec_t exec = nullptr;
+};
+
+namespace {
+
+int plan_fail( int code, std::string const& msg ) { return record_error( code, msg.c_str() ); }
+
+// Tile the images for shape `s` and upload the work items, most expensive first.
+int plan_items( dipcu_batch_plan* p, int s, int inject ) {
+   TileShape const ts = kShapes[ s ];
+   std::vector< BatchItem > items;
+   for( int i = 0; i < p->count; ++i ) {
+      BatchImage& im = p->images[ static_cast< size_t >( i ) ];
+      im.tiles_x = static_cast< int32_t >(( im.n[ 0 ] + ts.tx - 1 ) / ts.tx );
+      im.tiles_y = static_cast< int32_t >(( im.n[ 1 ] + ts.ty - 1 ) / ts.ty );
+      for( int t = 0; t < im.tiles_x * im.tiles_y; ++t ) { items.push_back( BatchItem{ i, t } ); }
+   }
+   std::stable_sort( items.begin(), items.end(), [ & ]( BatchItem const& a, BatchItem const& b ) {
+      return p->images[ static_cast< size_t >( a.image ) ].bucket > p->images[ static_cast< size_t >( b.image ) ].bucket;
+   } );
+   if( inject == 1 && !items.empty() ) { items[ items.size() / 2 ].image = p->count + 7; }   // impossible item
+   if( inject == 2 && !items.empty() ) { items[ items.size() / 2 ].tile = 1 << 30; }
+   cudaFree( p->d_items );
+   p->d_items = nullptr;
+   p->nitems = static_cast< int >( items.size() );
+   if( cudaMalloc( &p->d_items, sizeof( BatchItem ) * std::max< size_t >( 1, items.size() )) != cudaSuccess ) {
+      return plan_fail( DIPCU_ERR_CUDA, "cudaMalloc (batch items)" );
+   }
+   if( cudaMemcpy( p->d_items, items.data(), sizeof( BatchItem ) * items.size(), cudaMemcpyHostToDevice ) != cudaSuccess ||
+       cudaMemcpy( p->d_images, p->images.data(), sizeof( BatchImage ) * p->images.size(), cudaMemcpyHostToDevice ) != cudaSuccess ) {
+      return plan_fail( DIPCU_ERR_CUDA, "cudaMemcpy (batch tables)" );
+   }
+   p->shape = s;
+   p->grid = shape_grid( s );
+   if( p->grid < 1 ) { return plan_fail( DIPCU_ERR_CUDA, "batch kernel set-up" ); }
+   return DIPCU_OK;
+}
+
+int enqueue_run( dipcu_batch_plan* p, cudaStream_t st ) {
+   if( cudaMemsetAsync( p->d_counter, 0, sizeof( int32_t ), st ) != cudaSuccess ) {
+      return plan_fail( DIPCU_ERR_CUDA, "cudaMemsetAsync (queue)" );
+   }
+   cudaError_t e = launch_gauss_weights( p->d_sigmas, p->d_orders, 2 * p->count, p->truncation, p->d_bank, nullptr,
+                                         nullptr, kBankStride, st );
+   if( e != cudaSuccess ) { return plan_fail( DIPCU_ERR_CUDA, "gauss_weights_kernel" ); }
+   BatchArgs a{};
+   a.images = p->d_images;
+   a.items = p->d_items;
+   a.wbank = p->d_bank;
+   a.counter = p->d_counter;
+   a.status = device_status_ptr();
+   a.nimages = p->count;
+   a.nitems = p->nitems;
+   e = launch_shape( p->shape, p->grid, a, st );
+   if( e != cudaSuccess ) { return plan_fail( DIPCU_ERR_CUDA, std::string( "batch_kernel: " ) + cudaGetErrorString( e )); }
+   return DIPCU_OK;
+}
+
+void destroy_graph( dipcu_batch_plan* p ) {
+   if( p->exec ) { cudaGraphExecDestroy( p->exec ); p->exec = nullptr; }
+   if( p->graph ) { cudaGraphDestroy( p->graph ); p->graph = nullptr; }
+}
+
+} // namespace
+
+extern "C" {
+
+int dipcu_batch_plan_create( dipcu_image_desc const* ins, dipcu_image_desc const* outs, int count,
+                             double const* sigmas, uint32_t const* orders, int32_t const* bcs, double truncation,
+                             int flags, dipcu_batch_plan** plan_out ) {
+   if( !plan_out || count < 1 || !ins || !outs || !sigmas || !orders || !bcs ) {
+      return plan_fail( DIPCU_ERR_INVALID_ARG, "dipcu_batch_plan_create: bad arguments" );
+   }
+   *plan_out = nullptr;
+   auto* p = new dipcu_batch_plan();
+   cudaGetDevice( &p->device );
+   p->count = count;
+   p->truncation = truncation;
+   p->images.resize( static_cast< size_t >( count ));
+   p->sig_host.resize( 2 * static_cast< size_t >( count ));
+   p->ord_host.resize( 2 * static_cast< size_t >( count ));
+   std::string sig;
+   for( int i = 0; i < count; ++i ) {
+      dipcu_image_desc const& in = ins[ i ];
+      dipcu_image_desc const& out = outs[ i ];
+      if( in.ndims != 2 || out.ndims != 2 || in.dtype != DT_SFLOAT || out.dtype != DT_SFLOAT || !in.data || !out.data ||
+          in.sizes[ 0 ] != out.sizes[ 0 ] || in.sizes[ 1 ] != out.sizes[ 1 ] || in.strides[ 0 ] != 1 || out.strides[ 0 ] != 1 ) {
+         delete p;
+         return plan_fail( DIPCU_ERR_INVALID_ARG, "batch images must be 2D sfloat with unit x stride and matching sizes (image " +
+                                                  std::to_string( i ) + ")" );
+      }
+      BatchImage& im = p->images[ static_cast< size_t >( i ) ];
+      im.src = static_cast< float const* >( in.data );
+      im.dst = static_cast< float* >( out.data );
+      int hb = 0;
+      for( int d = 0; d < 2; ++d ) {
+         double s = sigmas[ 2 * i + d ];
+         uint32_t o = orders[ 2 * i + d ];
+         int32_t bc = bcs[ 2 * i + d ];
+         if( o > 3 ) { delete p; return plan_fail( DIPCU_ERR_ORDER_GT_3, "Gaussian FIR filter not implemented for order > 3" ); }
+         if( !bc_is_index_map( bc )) {
+            delete p;
+            return plan_fail( DIPCU_ERR_UNSUPPORTED_BC, "the batched filter supports the index-mapping boundary conditions and \"add zeros\"" );
+         }
+         im.n[ d ] = in.sizes[ d ];
+         im.ss[ d ] = in.strides[ d ];
+         im.ds[ d ] = out.strides[ d ];
+         im.bc[ d ] = bc;
+         bool process = s > 0.0 && in.sizes[ d ] > 1;
+         int64_t h = process ? half_gaussian_length( s, o, truncation, false ) - 1 : 0;
+         if( h > 32 ) { delete p; return plan_fail( DIPCU_ERR_KERNEL_TOO_LARGE, "the batched filter supports half-widths up to 32" ); }
+         im.h[ d ] = static_cast< int32_t >( h );
+         im.odd[ d ] = process ? static_cast< int32_t >( o & 1u ) : 0;
+         im.wofs[ d ] = ( 2 * i + d ) * kBankStride;
+         // Unfiltered axes get the unit kernel (sigma 0 -> a single tap of 1).
+         p->sig_host[ 2 * static_cast< size_t >( i ) + d ] = process ? s : 0.0;
+         p->ord_host[ 2 * static_cast< size_t >( i ) + d ] = process ? o : 0;
+         hb = std::max( hb, static_cast< int >( h ));
+      }
+      im.bucket = hb <= 4 ? 0 : hb <= 8 ? 1 : hb <= 16 ? 2 : 3;
+      sig += std::to_string( im.bucket ) + ":" + std::to_string( im.n[ 0 ] / 64 ) + "x" + std::to_string( im.n[ 1 ] / 64 ) + ";";
+   }
+   bool ok = cudaMalloc( &p->d_images, sizeof( BatchImage ) * static_cast< size_t >( count )) == cudaSuccess &&
+             cudaMalloc( &p->d_sigmas, sizeof( double ) * 2 * static_cast< size_t >( count )) == cudaSuccess &&
+             cudaMalloc( &p->d_orders, sizeof( uint32_t ) * 2 * static_cast< size_t >( count )) == cudaSuccess &&
+             cudaMalloc( &p->d_bank, sizeof( float ) * kBankStride * 2 * static_cast< size_t >( count )) == cudaSuccess &&
+             cudaMalloc( &p->d_counter, sizeof( int32_t )) == cudaSuccess;
+   ok = ok && cudaMemcpy( p->d_sigmas, p->sig_host.data(), sizeof( double ) * p->sig_host.size(), cudaMemcpyHostToDevice ) == cudaSuccess &&
+        cudaMemcpy( p->d_orders, p->ord_host.data(), sizeof( uint32_t ) * p->ord_host.size(), cudaMemcpyHostToDevice ) == cudaSuccess;
+   if( !ok ) {
+      dipcu_batch_plan_destroy( p );
+      return plan_fail( DIPCU_ERR_CUDA, "batch plan allocation" );
+   }
+   int const inject = ( flags & DIPCU_BATCH_INJECT_INVALID_IMAGE ) ? 1 : ( flags & DIPCU_BATCH_INJECT_INVALID_TILE ) ? 2 : 0;
+   if( !device_status_ptr() ) {   // resolved before any capture
+      dipcu_batch_plan_destroy( p );
+      return plan_fail( DIPCU_ERR_CUDA, "device status word" );
+   }
+   // Tile shape: the autotuner times every candidate on this batch (the filter outputs are
+   // overwritten by the final runs), remembering the winner per batch signature.
+   int shape = 0;
+   if( char const* env = getenv( "DIPCU_BATCH_SHAPE" )) { shape = std::max( 0, std::min( 2, atoi( env ))); }
+   if( flags & DIPCU_BATCH_AUTOTUNE ) {
+      std::lock_guard< std::mutex > lock( g_tune_mu );
+      auto it = g_tune_cache.find( sig );
+      if( it != g_tune_cache.end() ) {
+         shape = it->second;
+      } else {
+         float best = 1e30f;
+         cudaEvent_t e0, e1;
+         cudaEventCreate( &e0 );
+         cudaEventCreate( &e1 );
+         for( int s = 0; s < 3; ++s ) {
+            if( plan_items( p, s, 0 ) != DIPCU_OK ) { continue; }
+            enqueue_run( p, nullptr );                    // warm-up
+            cudaEventRecord( e0, nullptr );
+            for( int r = 0; r < 3; ++r ) { enqueue_run( p, nullptr ); }
+            cudaEventRecord( e1, nullptr );
+            cudaEventSynchronize( e1 );
+            float ms = 0.0f;
+            cudaEventElapsedTime( &ms, e0, e1 );
+            if( ms < best ) { best = ms; shape = s; }
+         }
+         cudaEventDestroy( e0 );
+         cudaEventDestroy( e1 );
+         g_tune_cache[ sig ] = shape;
+      }
+   }
+   if( int st = plan_items( p, shape, inject )) { dipcu_batch_plan_destroy( p ); return st; }
+   if( flags & DIPCU_BATCH_GRAPH ) {
+      if( cudaStreamCreateWithFlags( &p->cap_stream, cudaStreamNonBlocking ) != cudaSuccess ||
+          cudaStreamBeginCapture( p->cap_stream, cudaStreamCaptureModeThreadLocal ) != cudaSuccess ) {
+         dipcu_batch_plan_destroy( p );
+         return plan_fail( DIPCU_ERR_CUDA, "batch graph capture" );
+      }
+      int st = enqueue_run( p, p->cap_stream );
+      cudaError_t ce = cudaStreamEndCapture( p->cap_stream, &p->graph );
+      if( st != DIPCU_OK || ce != cudaSuccess || cudaGraphInstantiate( &p->exec, p->graph, 0 ) != cudaSuccess ) {
+         dipcu_batch_plan_destroy( p );
+         return plan_fail( DIPCU_ERR_CUDA, "batch graph instantiation" );
+      }
+   }
+   *plan_out = p;
+   return DIPCU_OK;
+}
+
+int dipcu_batch_plan_run( dipcu_batch_plan* plan, void* stream ) {
+   if( !plan ) { return plan_fail( DIPCU_ERR_INVALID_ARG, "null plan" ); }
+   cudaStream_t st = static_cast< cudaStream_t >( stream );
+   if( plan->exec ) {
+      cudaError_t e = cudaGraphLaunch( plan->exec, st );
+      if( e != cudaSuccess ) { return plan_fail( DIPCU_ERR_CUDA, std::string( "cudaGraphLaunch: " ) + cudaGetErrorString( e )); }
+      return DIPCU_OK;
+   }
+   return enqueue_run( plan, st );
+}
+
+int dipcu_batch_plan_info( dipcu_batch_plan const* plan, int* nitems, int* tile_x, int* tile_y, int* grid ) {
+   if( !plan ) { return plan_fail( DIPCU_ERR_INVALID_ARG, "null plan" ); }
+   if( nitems ) { *nitems = plan->nitems; }
+   if( tile_x ) { *tile_x = kShapes[ plan->shape ].tx; }
+   if( tile_y ) { *tile_y = kShapes[ plan->shape ].ty; }
+   if( grid ) { *grid = plan->grid; }
+   return DIPCU_OK;
+}
+
+double* dipcu_batch_plan_sigmas( dipcu_batch_plan* plan ) {
+   return plan ? plan->d_sigmas : nullptr;
+}
+
+int dipcu_batch_plan_destroy( dipcu_batch_plan* plan ) {
+   if( !plan ) { return DIPCU_OK; }
+   destroy_graph( plan );
+   if( plan->cap_stream ) { cudaStreamDestroy( plan->cap_stream ); }
+   cudaFree( plan->d_images );
+   cudaFree( plan->d_items );
+   cudaFree( plan->d_sigmas );
+   cudaFree( plan->d_orders );
+   cudaFree( plan->d_bank );
+   cudaFree( plan->d_counter );
+   delete plan;
+   return DIPCU_OK;
+}
+
+int dipcu_device_status( int* status, int clear ) {
+   int32_t* p = device_status_ptr();
+   if( !p || !status ) { return plan_fail( DIPCU_ERR_INVALID_ARG, "dipcu_device_status" ); }
+   int32_t v = 0;
+   if( cudaMemcpy( &v, p, sizeof( v ), cudaMemcpyDeviceToHost ) != cudaSuccess ) {
+      return plan_fail( DIPCU_ERR_CUDA, "dipcu_device_status: cudaMemcpy" );
+   }
+   *status = v;
+   if( clear ) {
+      int32_t z = 0;
+      if( cudaMemcpy( p, &z, sizeof( z ), cudaMemcpyHostToDevice ) != cudaSuccess ) {
+         return plan_fail( DIPCU_ERR_CUDA, "dipcu_device_status: cudaMemcpy" );
+      }
+   }
+   return DIPCU_OK;
+}
+
+} // extern "C"

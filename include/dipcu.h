@@ -112,6 +112,39 @@ int dipcu_gauss_fir_backward( dipcu_image_desc const* grad_out, dipcu_image_desc
                               double const* sigmas, uint32_t const* orders, int32_t const* bcs,
                               double truncation, void* stream );
 
+/* ---- Batched filter ------------------------------------------------------------------------ */
+
+/* Many 2D sfloat images of uneven sizes, each with its own per-axis sigmas, orders (0..3) and
+ * boundary conditions (the index-mapping ones and "add zeros"; half-widths up to 32), filtered by
+ * one persistent launch that pulls (image, tile) work items from a device queue.  No DIPlib
+ * counterpart (DIPlib filters one image per call; this is dip::GaussFIR per image).
+ * `sigmas`, `orders`, `bcs`: host arrays of 2 * count entries (x then y of each image).
+ * Flags: DIPCU_BATCH_GRAPH captures the run (queue reset, on-device weights, persistent kernel)
+ * into a CUDA graph so that dipcu_batch_plan_run is one graph launch; DIPCU_BATCH_AUTOTUNE times
+ * the candidate tile shapes on this batch at creation (overwriting the outputs) and keeps the
+ * fastest, remembered per batch signature.  The two INJECT flags are test hooks that plant one
+ * impossible work item, which the kernel skips and reports through dipcu_device_status.
+ * The plan allocates its tables at creation; runs allocate nothing.  The images must stay alive
+ * while the plan is used.  The sigma table (dipcu_batch_plan_sigmas, device, 2 * count doubles)
+ * may be rewritten between runs, as long as no kernel length changes. */
+typedef struct dipcu_batch_plan dipcu_batch_plan;
+#define DIPCU_BATCH_GRAPH 1
+#define DIPCU_BATCH_AUTOTUNE 2
+#define DIPCU_BATCH_INJECT_INVALID_IMAGE 256
+#define DIPCU_BATCH_INJECT_INVALID_TILE 512
+int dipcu_batch_plan_create( dipcu_image_desc const* ins, dipcu_image_desc const* outs, int count,
+                             double const* sigmas, uint32_t const* orders, int32_t const* bcs, double truncation,
+                             int flags, dipcu_batch_plan** plan );
+int dipcu_batch_plan_run( dipcu_batch_plan* plan, void* stream );
+/* Work items, chosen tile shape and persistent grid size of a plan. */
+int dipcu_batch_plan_info( dipcu_batch_plan const* plan, int* nitems, int* tile_x, int* tile_y, int* grid );
+double* dipcu_batch_plan_sigmas( dipcu_batch_plan* plan );
+int dipcu_batch_plan_destroy( dipcu_batch_plan* plan );
+
+/* Reads (and with `clear`, resets) the device status word where kernels report a skipped invalid
+ * work item (DIPCU_ERR_INVALID_ARG) or a timed-out wait (DIPCU_ERR_TIMEOUT).  Synchronises. */
+int dipcu_device_status( int* status, int clear );
+
 /* ---- Kernel weights ----------------------------------------------------------------------- */
 
 /* Half-kernel length of dip::MakeHalfGaussian (src/linear/gauss.cpp:38-62): returns

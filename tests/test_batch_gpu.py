@@ -1,0 +1,99 @@
+"""The batched persistent launch (dipcu_batch_plan_*): every image of an uneven batch matches
+the oracle, CUDA-graph replays and in-place sigma updates give the new filter, the autotuner
+picks a valid tile shape, and a planted impossible work item is skipped and reported (the
+kernel finishes; nothing on the GPU is made to fault or wait)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+SIGMAS = [0.8, 1.0, 2.0, 4.0, 8.0]
+BCS = ["mirror", "periodic", "add zeros"]
+
+
+def make_batch(n, seed, lo=20, hi=300):
+    rng = np.random.default_rng(seed)
+    imgs, params = [], []
+    for _ in range(n):
+        h, w = (int(v) for v in rng.integers(lo, hi + 1, 2))
+        imgs.append(rng.random((h, w), dtype=np.float32))
+        s = float(rng.choice(SIGMAS))
+        params.append((s, [int(rng.integers(0, 3)), int(rng.integers(0, 3))], str(rng.choice(BCS))))
+    return imgs, params
+
+
+def run_plan(imgs, params, **kw):
+    from diplib_b200.batch import BatchPlan
+    ins = [torch.from_numpy(a).cuda() for a in imgs]
+    outs = [torch.full_like(t, float("nan")) for t in ins]
+    plan = BatchPlan(ins, outs, [p[0] for p in params], [p[1] for p in params], [p[2] for p in params], **kw)
+    plan.run()
+    torch.cuda.synchronize()
+    return plan, ins, outs
+
+
+def check_all(imgs, params, outs, sig_override=None):
+    for i, (a, (s, o, bc)) in enumerate(zip(imgs, params)):
+        sg = sig_override[i] if sig_override is not None else [s, s]
+        ref = oracle.gauss_fir(a, sg, o, [bc], 3.0)
+        got = outs[i].cpu().numpy()
+        err = np.abs(got - ref).max()
+        assert err <= 1e-5 * max(1.0, float(a.max() - a.min())), (i, a.shape, s, o, bc, err)
+
+
+def test_batch_matches_oracle_with_graph_and_autotune(cuda):
+    from diplib_b200.batch import device_status
+    device_status(clear=True)
+    imgs, params = make_batch(40, 1)
+    plan, ins, outs = run_plan(imgs, params, graph=True, autotune=True)
+    info = plan.info()
+    assert info["tile"] in [(64, 32), (64, 16), (128, 32)] and info["items"] > 0
+    check_all(imgs, params, outs)
+    for o in outs:
+        o.fill_(float("nan"))
+    plan.run()                       # graph replay
+    torch.cuda.synchronize()
+    check_all(imgs, params, outs)
+    assert device_status() == 0
+    plan.close()
+
+
+def test_batch_without_graph_and_small_images(cuda):
+    imgs, params = make_batch(25, 2, lo=1, hi=40)
+    plan, ins, outs = run_plan(imgs, params, graph=False, autotune=False)
+    check_all(imgs, params, outs)
+    plan.close()
+
+
+def test_batch_sigma_table_update_between_replays(cuda):
+    imgs, params = make_batch(12, 3)
+    plan, ins, outs = run_plan(imgs, params, graph=True, autotune=False)
+    tab = plan.sigma_table()
+    # Shrink every sigma by 1e-4 (relative): no kernel length (ceil((3 + o/2) sigma)) changes for
+    # this sigma set, so the captured graph stays valid and rebuilds the weights on the device.
+    new = [[s * 0.9999, s * 0.9999] for s, _, _ in params]
+    tab.copy_(torch.tensor([v for p in new for v in p], dtype=torch.float64, device=tab.device))
+    plan.run()
+    torch.cuda.synchronize()
+    check_all(imgs, params, outs, sig_override=new)
+    plan.close()
+
+
+@pytest.mark.parametrize("flag", ["image", "tile"])
+def test_batch_planted_invalid_item_is_skipped_and_reported(cuda, flag):
+    from diplib_b200 import _abi
+    from diplib_b200.batch import INJECT_INVALID_IMAGE, INJECT_INVALID_TILE, device_status
+    device_status(clear=True)
+    imgs, params = make_batch(10, 4)
+    f = INJECT_INVALID_IMAGE if flag == "image" else INJECT_INVALID_TILE
+    plan, ins, outs = run_plan(imgs, params, graph=True, autotune=False, flags=f)
+    assert device_status(clear=True) == _abi.ERR_INVALID_ARG
+    # Every other tile was filtered: at most one tile's outputs are missing.
+    nan_count = sum(int(torch.isnan(o).sum()) for o in outs)
+    assert 0 < nan_count <= 128 * 32
+    plan.close()
