@@ -6,6 +6,7 @@ runs in libdipcu.so's CUDA kernels through the C-ABI declared in include/dipcu.h
 """
 from .filtering import (BestGaussMethod, BoundaryConditionFromString, Derivative, Error, Gauss, GaussFIR,
                         ParameterError, RunTimeError, flex_dtype, image_desc)
+from .analysis import StructureTensor
 
 __all__ = ["BestGaussMethod", "BoundaryConditionFromString", "Derivative", "Error", "Gauss", "GaussFIR",
-           "ParameterError", "RunTimeError", "flex_dtype", "image_desc"]
+           "ParameterError", "StructureTensor", "RunTimeError", "flex_dtype", "image_desc"]

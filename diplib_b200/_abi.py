@@ -52,6 +52,11 @@ SIGNATURES = {
     "dipcu_gauss_fir_backward": (ctypes.c_int, [_P(ImageDesc), _P(ImageDesc), _P(ImageDesc), ctypes.c_void_p,
                                                 _P(ctypes.c_double), _P(ctypes.c_uint32), _P(ctypes.c_int32),
                                                 ctypes.c_double, ctypes.c_void_p]),
+    "dipcu_structure_tensor": (ctypes.c_int, [_P(ImageDesc), _P(ImageDesc), _P(ctypes.c_double), _P(ctypes.c_double),
+                                              _P(ctypes.c_int32), ctypes.c_double, ctypes.c_void_p]),
+    "dipcu_structure_tensor_backward": (ctypes.c_int, [_P(ImageDesc), _P(ImageDesc), _P(ImageDesc),
+                                                       _P(ctypes.c_double), _P(ctypes.c_double), _P(ctypes.c_int32),
+                                                       ctypes.c_double, ctypes.c_void_p]),
     "dipcu_batch_plan_create": (ctypes.c_int, [_P(ImageDesc), _P(ImageDesc), ctypes.c_int, _P(ctypes.c_double),
                                                _P(ctypes.c_uint32), _P(ctypes.c_int32), ctypes.c_double, ctypes.c_int,
                                                _P(ctypes.c_void_p)]),

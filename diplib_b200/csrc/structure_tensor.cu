@@ -1,0 +1,276 @@
+// Structure tensor on the Gaussian FIR path, forward and backward.
+//
+// Forward, as dip::StructureTensor (src/analysis/structure_tensor.cpp:33-59 in DIPlib) with a
+// Gaussian method and no mask: the gradient g_k = GaussFIR(in, sigma_g, order e_k) along each
+// axis of size > 1 (dip::Gradient, src/linear/derivative.cpp:142-172), the symmetric products
+// g_i g_j in DIPlib's symmetric-matrix order (diagonal first, then the upper triangle row by row;
+// dip::Multiply( g, Transpose( g ))), and each product smoothed by GaussFIR(sigma_t).  Products are
+// formed per component and smoothed immediately, so at most one product image exists at a time.
+//
+// Backward (no DIPlib counterpart): for L = sum_c <W_c, T_c>,
+//   Q_c = S^T W_c (the smoothing's adjoint),
+//   g_bar_k = sum over components (i, j) containing k of Q_c times the other factor,
+//   in_bar  = sum_k D_k^T g_bar_k (the gradient filters' adjoints).
+// The gradient images g_k are recomputed from the input here; the forward stores nothing.
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "dipcu_common.cuh"
+#include "dipcu_internal.h"
+
+extern "C" int dipcu_gauss_fir_backward( dipcu_image_desc const* grad_out, dipcu_image_desc const* in,
+                                          dipcu_image_desc const* grad_in, double* grad_sigma,
+                                          double const* sigmas, uint32_t const* orders, int32_t const* bcs,
+                                          double truncation, void* stream );
+
+namespace dipcu {
+
+namespace {
+
+// dst[i] = a[i] * b[i] * s        (mode 0)
+// dst[i] += a[i] * b[i] * s       (mode 1)
+// dst[i] += a[i]                  (mode 2)
+template< typename T >
+__global__ void elementwise_kernel( T* dst, T const* a, T const* b, T s, int64_t n, int mode ) {
+   for( int64_t i = static_cast< int64_t >( blockIdx.x ) * blockDim.x + threadIdx.x; i < n;
+        i += static_cast< int64_t >( gridDim.x ) * blockDim.x ) {
+      if( mode == 0 ) { dst[ i ] = a[ i ] * b[ i ] * s; }
+      else if( mode == 1 ) { dst[ i ] = fma( a[ i ] * b[ i ], s, dst[ i ] ); }
+      else { dst[ i ] += a[ i ]; }
+   }
+}
+
+cudaError_t elementwise( bool dbl, void* dst, void const* a, void const* b, double s, int64_t n, int mode, cudaStream_t st ) {
+   int64_t blocks = ( n + 255 ) / 256;
+   if( blocks > 148 * 16 ) { blocks = 148 * 16; }
+   if( blocks < 1 ) { blocks = 1; }
+   if( dbl ) {
+      elementwise_kernel< double ><<< static_cast< unsigned >( blocks ), 256, 0, st >>>(
+            static_cast< double* >( dst ), static_cast< double const* >( a ), static_cast< double const* >( b ), s, n, mode );
+   } else {
+      elementwise_kernel< float ><<< static_cast< unsigned >( blocks ), 256, 0, st >>>(
+            static_cast< float* >( dst ), static_cast< float const* >( a ), static_cast< float const* >( b ),
+            static_cast< float >( s ), n, mode );
+   }
+   return cudaGetLastError();
+}
+
+struct Scratch {
+   std::vector< void* > bufs;
+   cudaStream_t st;
+   ~Scratch() { for( void* p : bufs ) { cudaFreeAsync( p, st ); } }
+   void* get( size_t bytes ) {
+      void* p = nullptr;
+      if( cudaMallocAsync( &p, bytes, st ) != cudaSuccess ) { return nullptr; }
+      bufs.push_back( p );
+      return p;
+   }
+};
+
+// Common set-up of the forward and backward: gradient axes, component list, image geometry.
+struct StSetup {
+   int nd = 0;
+   std::vector< int > dims;                 // axes of the gradient (size > 1, sigma > 0)
+   std::vector< std::pair< int, int >> comps;
+   int64_t n = 0;
+   int32_t cdt = DT_SFLOAT;
+   bool cdouble = false;
+   dipcu_image_desc plain{};                // a normal-stride image of the compute type (data unset)
+};
+
+int st_setup( dipcu_image_desc const* in, double const* grad_sigmas, double const* tensor_sigmas, int32_t const* bcs,
+              StSetup& s ) {
+   if( !in || !in->data || in->ndims < 1 || in->ndims > 3 ) {
+      return record_error( DIPCU_ERR_INVALID_ARG, "structure tensor: the input must be a forged 1D-3D image" );
+   }
+   if( !grad_sigmas || !tensor_sigmas || !bcs ) {
+      return record_error( DIPCU_ERR_INVALID_ARG, "structure tensor: null parameter array" );
+   }
+   if( in->dtype <= DT_BIN || in->dtype > DT_DFLOAT ) {
+      return record_error( DIPCU_ERR_UNSUPPORTED_DTYPE, "Data type not supported" );
+   }
+   s.nd = in->ndims;
+   s.n = 1;
+   for( int d = 0; d < s.nd; ++d ) {
+      s.n *= in->sizes[ d ];
+      if( in->sizes[ d ] > 1 && grad_sigmas[ d ] > 0.0 ) { s.dims.push_back( d ); }
+   }
+   if( s.dims.empty() ) { return record_error( DIPCU_ERR_INVALID_ARG, "Dimensionality not supported" ); }
+   int const m = static_cast< int >( s.dims.size() );
+   for( int i = 0; i < m; ++i ) { s.comps.push_back( { i, i } ); }
+   for( int i = 0; i < m; ++i ) {
+      for( int j = i + 1; j < m; ++j ) { s.comps.push_back( { i, j } ); }
+   }
+   s.cdt = suggest_flex( in->dtype );
+   s.cdouble = s.cdt == DT_DFLOAT;
+   s.plain.dtype = s.cdt;
+   s.plain.ndims = s.nd;
+   int64_t st = 1;
+   for( int d = 0; d < s.nd; ++d ) {
+      s.plain.sizes[ d ] = in->sizes[ d ];
+      s.plain.strides[ d ] = st;
+      st *= in->sizes[ d ];
+   }
+   return DIPCU_OK;
+}
+
+int check_tensor_image( dipcu_image_desc const* t, StSetup const& s, char const* name ) {
+   if( !t || !t->data || t->ndims != s.nd + 1 || t->dtype != s.cdt ||
+       t->sizes[ s.nd ] != static_cast< int64_t >( s.comps.size() )) {
+      std::string msg = std::string( "structure tensor: `" ) + name + "` must have the input's sizes plus a last axis of " +
+                        std::to_string( s.comps.size() ) + " components, of the computation type";
+      return record_error( DIPCU_ERR_INVALID_ARG, msg.c_str() );
+   }
+   for( int d = 0; d < s.nd; ++d ) {
+      if( t->sizes[ d ] != s.plain.sizes[ d ] ) { return record_error( DIPCU_ERR_SIZES_DONT_MATCH, "Sizes don't match" ); }
+   }
+   return DIPCU_OK;
+}
+
+dipcu_image_desc component( dipcu_image_desc const* t, int c, int nd ) {
+   dipcu_image_desc d = *t;
+   d.ndims = nd;
+   d.data = static_cast< char* >( t->data ) + static_cast< int64_t >( c ) * t->strides[ nd ] * dtype_size( t->dtype );
+   return d;
+}
+
+// g_k for every gradient axis, into `g[k]` (normal strides).
+int gradients( dipcu_image_desc const* in, StSetup const& s, double const* grad_sigmas, int32_t const* bcs, double trunc,
+               std::vector< void* > const& g, cudaStream_t stream ) {
+   for( size_t k = 0; k < s.dims.size(); ++k ) {
+      std::vector< uint32_t > ord( static_cast< size_t >( s.nd ), 0u );
+      ord[ static_cast< size_t >( s.dims[ k ] ) ] = 1u;
+      std::vector< AxisFilter > f;
+      if( int st = build_filters( in, grad_sigmas, ord.data(), bcs, trunc, f, nullptr )) { return st; }
+      dipcu_image_desc out = s.plain;
+      out.data = g[ k ];
+      if( int st = run_filters( in, &out, f, s.cdouble, stream )) { return st; }
+   }
+   return DIPCU_OK;
+}
+
+} // namespace
+
+} // namespace dipcu
+
+using namespace dipcu;
+
+extern "C" {
+
+int dipcu_structure_tensor( dipcu_image_desc const* in, dipcu_image_desc const* out, double const* grad_sigmas,
+                            double const* tensor_sigmas, int32_t const* bcs, double truncation, void* stream_ ) {
+   cudaStream_t stream = static_cast< cudaStream_t >( stream_ );
+   StSetup s;
+   if( int st = st_setup( in, grad_sigmas, tensor_sigmas, bcs, s )) { return st; }
+   if( int st = check_tensor_image( out, s, "out" )) { return st; }
+   size_t const bytes = static_cast< size_t >( s.n ) * ( s.cdouble ? 8 : 4 );
+   Scratch sc{ {}, stream };
+   std::vector< void* > g;
+   for( size_t k = 0; k < s.dims.size(); ++k ) {
+      g.push_back( sc.get( bytes ));
+      if( !g.back() ) { return record_error( DIPCU_ERR_CUDA, "cudaMallocAsync (gradient)" ); }
+   }
+   void* prod = sc.get( bytes );
+   if( !prod ) { return record_error( DIPCU_ERR_CUDA, "cudaMallocAsync (product)" ); }
+   if( int st = gradients( in, s, grad_sigmas, bcs, truncation, g, stream )) { return st; }
+   std::vector< uint32_t > ord( static_cast< size_t >( s.nd ), 0u );
+   dipcu_image_desc pimg = s.plain;
+   pimg.data = prod;
+   std::vector< AxisFilter > f;
+   if( int st = build_filters( &pimg, tensor_sigmas, ord.data(), bcs, truncation, f, nullptr )) { return st; }
+   for( size_t c = 0; c < s.comps.size(); ++c ) {
+      cudaError_t e = elementwise( s.cdouble, prod, g[ static_cast< size_t >( s.comps[ c ].first ) ],
+                                   g[ static_cast< size_t >( s.comps[ c ].second ) ], 1.0, s.n, 0, stream );
+      if( e != cudaSuccess ) { return record_error( DIPCU_ERR_CUDA, cudaGetErrorString( e )); }
+      dipcu_image_desc oc = component( out, static_cast< int >( c ), s.nd );
+      if( int st = run_filters( &pimg, &oc, f, s.cdouble, stream )) { return st; }
+   }
+   return DIPCU_OK;
+}
+
+int dipcu_structure_tensor_backward( dipcu_image_desc const* grad_out, dipcu_image_desc const* in,
+                                     dipcu_image_desc const* grad_in, double const* grad_sigmas,
+                                     double const* tensor_sigmas, int32_t const* bcs, double truncation,
+                                     void* stream_ ) {
+   cudaStream_t stream = static_cast< cudaStream_t >( stream_ );
+   StSetup s;
+   if( int st = st_setup( in, grad_sigmas, tensor_sigmas, bcs, s )) { return st; }
+   if( int st = check_tensor_image( grad_out, s, "grad_out" )) { return st; }
+   if( !grad_in || grad_in->ndims != s.nd || grad_in->dtype != s.cdt ) {
+      return record_error( DIPCU_ERR_INVALID_ARG, "structure tensor: grad_in must be an image of the input's sizes and the computation type" );
+   }
+   size_t const bytes = static_cast< size_t >( s.n ) * ( s.cdouble ? 8 : 4 );
+   Scratch sc{ {}, stream };
+   size_t const m = s.dims.size();
+   std::vector< void* > g, gb;
+   for( size_t k = 0; k < m; ++k ) {
+      g.push_back( sc.get( bytes ));
+      gb.push_back( sc.get( bytes ));
+      if( !g.back() || !gb.back() ) { return record_error( DIPCU_ERR_CUDA, "cudaMallocAsync (gradients)" ); }
+      if( cudaMemsetAsync( gb.back(), 0, bytes, stream ) != cudaSuccess ) {
+         return record_error( DIPCU_ERR_CUDA, "cudaMemsetAsync (gradients)" );
+      }
+   }
+   void* q = sc.get( bytes );
+   void* acc = sc.get( bytes );
+   if( !q || !acc ) { return record_error( DIPCU_ERR_CUDA, "cudaMallocAsync (backward)" ); }
+   // Recompute the gradient images.
+   if( int st = gradients( in, s, grad_sigmas, bcs, truncation, g, stream )) { return st; }
+   std::vector< uint32_t > zero( static_cast< size_t >( s.nd ), 0u );
+   dipcu_image_desc qimg = s.plain;
+   qimg.data = q;
+   for( size_t c = 0; c < s.comps.size(); ++c ) {
+      dipcu_image_desc wc = component( grad_out, static_cast< int >( c ), s.nd );
+      if( int st = dipcu_gauss_fir_backward( &wc, nullptr, &qimg, nullptr, tensor_sigmas, zero.data(), bcs, truncation,
+                                             stream )) {
+         return st;
+      }
+      size_t const i = static_cast< size_t >( s.comps[ c ].first ), j = static_cast< size_t >( s.comps[ c ].second );
+      cudaError_t e;
+      if( i == j ) {
+         e = elementwise( s.cdouble, gb[ i ], q, g[ i ], 2.0, s.n, 1, stream );
+      } else {
+         e = elementwise( s.cdouble, gb[ i ], q, g[ j ], 1.0, s.n, 1, stream );
+         if( e == cudaSuccess ) { e = elementwise( s.cdouble, gb[ j ], q, g[ i ], 1.0, s.n, 1, stream ); }
+      }
+      if( e != cudaSuccess ) { return record_error( DIPCU_ERR_CUDA, cudaGetErrorString( e )); }
+   }
+   // in_bar = sum_k D_k^T g_bar_k, accumulated in `acc`, then converted into grad_in.
+   dipcu_image_desc aimg = s.plain;
+   aimg.data = acc;
+   for( size_t k = 0; k < m; ++k ) {
+      std::vector< uint32_t > ord( static_cast< size_t >( s.nd ), 0u );
+      ord[ static_cast< size_t >( s.dims[ k ] ) ] = 1u;
+      dipcu_image_desc gk = s.plain;
+      gk.data = gb[ k ];
+      dipcu_image_desc target = aimg;
+      if( k > 0 ) { target.data = q; }
+      if( int st = dipcu_gauss_fir_backward( &gk, nullptr, &target, nullptr, grad_sigmas, ord.data(), bcs, truncation,
+                                             stream )) {
+         return st;
+      }
+      if( k > 0 ) {
+         cudaError_t e = elementwise( s.cdouble, acc, q, nullptr, 1.0, s.n, 2, stream );
+         if( e != cudaSuccess ) { return record_error( DIPCU_ERR_CUDA, cudaGetErrorString( e )); }
+      }
+   }
+   ConvertArgs cv{};
+   cv.src = acc;
+   cv.dst = grad_in->data;
+   cv.src_dt = s.cdt;
+   cv.dst_dt = grad_in->dtype;
+   cv.ndims = s.nd;
+   cv.total = s.n;
+   for( int d = 0; d < s.nd; ++d ) {
+      cv.sizes[ d ] = s.plain.sizes[ d ];
+      cv.sst[ d ] = s.plain.strides[ d ];
+      cv.dstst[ d ] = grad_in->strides[ d ];
+   }
+   cudaError_t e = launch_convert( cv, true, stream );
+   if( e != cudaSuccess ) { return record_error( DIPCU_ERR_CUDA, cudaGetErrorString( e )); }
+   return DIPCU_OK;
+}
+
+} // extern "C"

@@ -20,7 +20,7 @@ from . import _abi
 from .filtering import (BoundaryConditionFromString, GaussFIR, ParameterError, _array_use_parameter, check,
                         flex_dtype, image_desc)
 
-__all__ = ["gauss", "gauss_backward"]
+__all__ = ["gauss", "gauss_backward", "structure_tensor", "structure_tensor_backward"]
 
 
 def _params(nd, sigma, order, boundary):
@@ -90,3 +90,48 @@ def gauss(x: torch.Tensor, sigma=1.0, order=0, boundary=(), truncation: float = 
     nd = max(1, x.dim())
     sig, _, _ = _params(nd, sigma, order, boundary)
     return _GaussFIRFunction.apply(x, sigma_t, sig, order, boundary, truncation)
+
+
+def structure_tensor_backward(grad_out: torch.Tensor, x: torch.Tensor, gradient_sigma=1.0, tensor_sigma=5.0,
+                              boundary=(), truncation: float = 3.0) -> torch.Tensor:
+    """dL/dx for T = StructureTensor(x) given dL/dT (planar, as ``structure_tensor`` returns it).
+    The gradient images are recomputed from ``x``."""
+    from .analysis import structure_tensor_params
+    nd = max(1, x.dim())
+    gs, ts, bcs = structure_tensor_params(nd, gradient_sigma, tensor_sigma, "gaussFIR", boundary)
+    cdt = flex_dtype(x.dtype)
+    go = grad_out.to(cdt)
+    gx = torch.empty(x.shape, dtype=cdt, device=x.device)
+    d_go, d_x, d_gx = image_desc(go), image_desc(x), image_desc(gx)
+    with torch.cuda.device(x.device):
+        check(_abi.lib().dipcu_structure_tensor_backward(
+            ctypes.byref(d_go), ctypes.byref(d_x), ctypes.byref(d_gx), (ctypes.c_double * nd)(*gs),
+            (ctypes.c_double * nd)(*ts), (ctypes.c_int32 * nd)(*bcs), float(truncation),
+            ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+    return gx
+
+
+class _StructureTensorFunction(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, x, gradient_sigma, tensor_sigma, boundary, truncation):
+        from .analysis import StructureTensor
+        ctx.save_for_backward(x)
+        ctx.params = (gradient_sigma, tensor_sigma, boundary, truncation)
+        return StructureTensor(x, None, gradient_sigma, tensor_sigma, "gaussFIR", boundary, truncation)
+
+    @staticmethod
+    def backward(ctx, grad_out):
+        (x,) = ctx.saved_tensors
+        gx = structure_tensor_backward(grad_out, x, *ctx.params)
+        if gx.dtype != x.dtype and x.dtype.is_floating_point:
+            gx = gx.to(x.dtype)
+        return gx, None, None, None, None
+
+
+def structure_tensor(x: torch.Tensor, gradient_sigma=1.0, tensor_sigma=5.0, boundary=(),
+                     truncation: float = 3.0) -> torch.Tensor:
+    """Differentiable dip::StructureTensor (Gaussian FIR, no mask) of a CUDA tensor: shape
+    ``(m(m+1)/2,) + x.shape``.  Only ``x`` is saved; the backward recomputes the gradient images."""
+    if not isinstance(x, torch.Tensor) or not x.is_cuda:
+        raise ParameterError("structure_tensor() takes a CUDA tensor")
+    return _StructureTensorFunction.apply(x, gradient_sigma, tensor_sigma, boundary, truncation)

@@ -112,6 +112,30 @@ int dipcu_gauss_fir_backward( dipcu_image_desc const* grad_out, dipcu_image_desc
                               double const* sigmas, uint32_t const* orders, int32_t const* bcs,
                               double truncation, void* stream );
 
+/* ---- Structure tensor ------------------------------------------------------------------------ */
+
+/* dip::StructureTensor with the "gaussFIR" method, no mask (src/analysis/structure_tensor.cpp:33-59
+ * in DIPlib; gradient as dip::Gradient, src/linear/derivative.cpp:142-172).  `in`: a 1D-3D
+ * image of any non-binary type; the gradient runs along every axis of size > 1 and gradient sigma > 0
+ * (dip::FindGradientDimensions, src/linear/derivative.cpp:120-138).  `out`: an image of
+ * ndims + 1 dimensions, the input's sizes followed by the component axis of m(m+1)/2 entries
+ * (m gradient axes) in DIPlib's symmetric-matrix order (diagonal first, then the upper triangle
+ * row by row), of the flex type (sfloat, dfloat for 32/64-bit integer and dfloat input); any
+ * strides, so DIPlib's own layout (component stride 1) and a planar one both work.
+ * `grad_sigmas`, `tensor_sigmas`, `bcs`: one entry per input dimension (already broadcast, as
+ * dip::ArrayUseParameter does).  The gradient images are scratch of the call (stream-ordered
+ * allocations). */
+int dipcu_structure_tensor( dipcu_image_desc const* in, dipcu_image_desc const* out, double const* grad_sigmas,
+                            double const* tensor_sigmas, int32_t const* bcs, double truncation, void* stream );
+
+/* Gradient of L = sum_c <grad_out_c, T_c> with respect to the input (no DIPlib counterpart).
+ * `grad_out` has the layout of dipcu_structure_tensor's `out`; `grad_in` the input's sizes and the
+ * flex type.  The gradient images are recomputed from `in`, never stored by the forward. */
+int dipcu_structure_tensor_backward( dipcu_image_desc const* grad_out, dipcu_image_desc const* in,
+                                     dipcu_image_desc const* grad_in, double const* grad_sigmas,
+                                     double const* tensor_sigmas, int32_t const* bcs, double truncation,
+                                     void* stream );
+
 /* ---- Batched filter ------------------------------------------------------------------------ */
 
 /* Many 2D sfloat images of uneven sizes, each with its own per-axis sigmas, orders (0..3) and

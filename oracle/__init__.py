@@ -87,7 +87,8 @@ def ref_lib():
         _ref.dipref_max_gauss_truncation.restype = ctypes.c_double
         _ref.dipref_structure_tensor.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _i64p, ctypes.c_double,
                                                  ctypes.c_double, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_double,
-                                                 ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.c_char_p,
+                                                 ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
+                                                 ctypes.POINTER(ctypes.c_int), ctypes.c_char_p,
                                                  ctypes.c_int]
     return _ref
 
@@ -197,20 +198,26 @@ def separable_fir(x: np.ndarray, taps, odd, bcs, out_dtype=None) -> np.ndarray:
     return out
 
 
-def structure_tensor(x: np.ndarray, grad_sigma: float, tensor_sigma: float, bc: str = "mirror",
-                     truncation: float = 3.0) -> np.ndarray:
+def structure_tensor(x: np.ndarray, grad_sigma, tensor_sigma, bc="mirror", truncation: float = 3.0) -> np.ndarray:
     """dip::StructureTensor (src/analysis/structure_tensor.cpp:33-59) built from the restated
-    GaussFIR: gradient (order 1 along each axis), products g_i g_j, smoothing of each product.
-    Returns an array of shape (ncomp,) + x.shape with DIPlib's symmetric-matrix component order
-    (diagonal first, then the upper triangle row by row)."""
+    GaussFIR: the gradient along the axes FindGradientDimensions keeps (src/linear/derivative.cpp:120-138:
+    size > 1 and sigma > 0), the products g_i g_j, and the smoothing of each product.  Sigmas and
+    boundary conditions are scalars or per-axis lists in DIPlib order.  Returns an array of shape
+    (ncomp,) + x.shape with DIPlib's symmetric-matrix component order (diagonal first, then the
+    upper triangle row by row)."""
     nd = x.ndim
+    gs = [float(grad_sigma)] * nd if np.isscalar(grad_sigma) else [float(s) for s in grad_sigma]
+    ts = [float(tensor_sigma)] * nd if np.isscalar(tensor_sigma) else [float(s) for s in tensor_sigma]
+    bcs = [bc] if isinstance(bc, str) else list(bc)
+    dims = [d for d in range(nd) if x.shape[nd - 1 - d] > 1 and gs[d] > 0]
     grads = []
-    for d in range(nd):  # d in DIPlib order
+    for d in dims:
         o = [0] * nd
         o[d] = 1
-        grads.append(gauss_fir(x, [grad_sigma] * nd, o, [bc], truncation))
-    pairs = [(i, i) for i in range(nd)] + [(i, j) for i in range(nd) for j in range(i + 1, nd)]
-    comps = [gauss_fir((grads[i] * grads[j]).astype(grads[0].dtype), [tensor_sigma] * nd, [0] * nd, [bc], truncation)
+        grads.append(gauss_fir(x, gs, o, bcs, truncation))
+    m = len(dims)
+    pairs = [(i, i) for i in range(m)] + [(i, j) for i in range(m) for j in range(i + 1, m)]
+    comps = [gauss_fir((grads[i] * grads[j]).astype(grads[0].dtype), ts, [0] * nd, bcs, truncation)
              for i, j in pairs]
     return np.stack(comps)
 
@@ -274,16 +281,18 @@ def ref_structure_tensor(x: np.ndarray, grad_sigma: float, tensor_sigma: float, 
                          truncation: float = 3.0, method: str = "gaussFIR") -> np.ndarray:
     """dip::StructureTensor of the reference; returns (ncomp,) + x.shape."""
     nd = x.ndim
-    ncomp = nd * (nd + 1) // 2
+    maxcomp = nd * (nd + 1) // 2
     sizes, _ = _dip_geometry(x)
     x = np.ascontiguousarray(x)
     res_dt = suggest_flex(x.dtype)
-    out = np.zeros(x.shape + (ncomp,), res_dt)
+    out = np.zeros(x.size * maxcomp, res_dt)
     code = ctypes.c_int(0)
+    ncomp = ctypes.c_int(0)
     errbuf = ctypes.create_string_buffer(512)
     rc = ref_lib().dipref_structure_tensor(x.ctypes.data, DTYPE_CODES[x.dtype], nd, sizes, grad_sigma, tensor_sigma,
                                            method.encode(), bc.encode(), truncation, out.ctypes.data,
-                                           ctypes.byref(code), errbuf, 512)
+                                           ctypes.byref(code), ctypes.byref(ncomp), errbuf, 512)
     if rc != 0:
         raise RuntimeError(errbuf.value.decode() or "StructureTensor failed")
+    out = out[:x.size * ncomp.value].reshape(x.shape + (ncomp.value,))
     return np.moveaxis(out, -1, 0).copy()

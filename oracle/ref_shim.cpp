@@ -132,19 +132,22 @@ int dipref_gauss(
    }
 }
 
-// Output: `ndims*(ndims+1)/2` tensor components per pixel, interleaved (normal strides), in the
-// reference's symmetric-matrix order (diagonal first).  Returns the output data type in *out_dtype.
+// Output: the tensor components per pixel, interleaved (normal strides), in the reference's
+// symmetric-matrix order (diagonal first); `out` has room for ndims*(ndims+1)/2 of them.  Returns the
+// output data type in *out_dtype and the number of components in *ncomp.
 int dipref_structure_tensor(
       void const* in, int in_dtype, int ndims, int64_t const* sizes,
       double grad_sigma, double tensor_sigma, char const* method, char const* bc, double truncation,
-      void* out, int* out_dtype, char* err, int errlen ) {
+      void* out, int* out_dtype, int* ncomp, char* err, int errlen ) {
    try {
       dip::Image img = Wrap( in, in_dtype, ndims, sizes, nullptr );
       dip::Image res;
       dip::StructureTensor( img, {}, res, { grad_sigma }, { tensor_sigma }, method, { bc }, truncation );
       *out_dtype = TypeToCode( res.DataType() );
+      *ncomp = static_cast< int >( res.TensorElements() );
+      if( *ncomp > ndims * ( ndims + 1 ) / 2 ) { return 1; }
       CopyOut( res, out );
-      return static_cast< int >( res.TensorElements() ) == ndims * ( ndims + 1 ) / 2 ? 0 : 1;
+      return 0;
    } catch( dip::Error const& e ) {
       SetErr( err, errlen, e.what() );
       return 1;

@@ -94,3 +94,19 @@ def test_known_answers_from_reference_tests():
 def test_order_gt_3_rejected():
     with pytest.raises(ValueError, match="order > 3"):
         oracle.gauss_fir(np.zeros((8, 8), np.float32), [1.0], [4])
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference library not built here")
+def test_structure_tensor_matches_live_reference():
+    """Size-1 axes drop out of the gradient (FindGradientDimensions); integer inputs go through
+    the flex type; every index-mapping boundary condition."""
+    rng = np.random.default_rng(77)
+    cases = [((9, 11), np.float32, 1.0, 2.0, "mirror"), ((1, 12, 13), np.float32, 1.0, 3.0, "periodic"),
+             ((7, 1, 10), np.uint16, 1.5, 2.0, "add zeros"), ((6, 8, 9), np.int32, 0.9, 1.5, "asym mirror"),
+             ((5, 9, 7), np.float64, 1.0, 2.5, "zero order"), ((17,), np.float32, 1.0, 2.0, "first order")]
+    for shape, dt, gsig, tsig, bc in cases:
+        x = (rng.random(shape) * 1000).astype(dt)
+        ref = oracle.ref_structure_tensor(x, gsig, tsig, bc, 3.0)
+        got = oracle.structure_tensor(x, gsig, tsig, bc, 3.0)
+        assert got.shape == ref.shape and got.dtype == ref.dtype, (shape, got.shape, ref.shape)
+        np.testing.assert_allclose(got, ref, rtol=0, atol=1e-6 * np.abs(ref).max(), err_msg=str((shape, bc)))
