@@ -329,6 +329,435 @@ def run_gpu_arm(args):
     return 0
 
 
+# ------------------------------------------------------------------------------------------------
+# Further workloads (one JSON line each, same keys).  Selected with --workload; the default run
+# above is the headline.  Each one rotates inputs/outputs over more than the 126 MB L2.
+# ------------------------------------------------------------------------------------------------
+
+def _device(args):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    return world, rank, dev
+
+
+def _capture(fn):
+    import torch
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        fn()
+    return g
+
+
+def _timed(graph_lists, steps, dev):
+    """Replays graph_lists[i % len] for `steps` steps between two events (barrier + sync on both
+    sides, max over ranks).  Returns (total ms, per-step ms list, clocks)."""
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    stream = torch.cuda.current_stream(dev)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(dev.index if dev.index is not None else 0) as clk:
+        start.record(stream)
+        for i in range(steps):
+            ev[i][0].record(stream)
+            for g in graph_lists[i % len(graph_lists)]:
+                g.replay()
+            ev[i][1].record(stream)
+        stop.record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    total = start.elapsed_time(stop)
+    if world > 1:
+        t = torch.tensor([total], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total = float(t.item())
+    return total, [a.elapsed_time(b) for a, b in ev], clk.summary()
+
+
+def _finish(line, world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if int(os.environ.get("RANK", "0")) == 0:
+        print(json.dumps(line))
+    return 0
+
+
+def _base_line(args, world, value, ms_step, config, dtype="f32"):
+    return {"metric": METRIC, "value": value, "unit": "Gvox/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": dtype, "data": "synthetic (seeded)",
+            "config": dict(config, parallelism=f"replicas x{world}" if world > 1 else "single GPU")}
+
+
+def _ref_rate(fn, nvox, budget_s=8.0, max_reps=20):
+    """(Gvox/s, cores, reps): the reference's OpenMP CPU path on `fn`, min over reps."""
+    import oracle
+    cores = oracle.ref_set_threads(0)
+    fn()
+    times = []
+    t_end = time.perf_counter() + budget_s
+    while len(times) < max_reps and (time.perf_counter() < t_end or len(times) < 2):
+        t0 = time.perf_counter()
+        fn()
+        times.append(time.perf_counter() - t0)
+    return nvox / min(times) / 1e9, cores, len(times)
+
+
+# ---- plain 2D (1024x1024 sfloat, sigma 2, order 0, mirror) ---------------------------------------
+
+G2_SHAPE = (1024, 1024)
+G2_CONFIG = {"workload": "dip::Gauss FIR 2D 1024^2 sfloat, sigma (2,2), order (0,0), truncation 3, mirror",
+             "l2": "32 rotating input/output sets (268 MB) > 126 MB L2"}
+
+
+def run_gauss2d(args):
+    import torch
+    import diplib_b200 as dipcu
+    world, rank, dev = _device(args)
+    nsets = 32
+    rng = np.random.default_rng(10 + rank)
+    host = rng.random(G2_SHAPE, dtype=np.float32)
+    xs = [torch.from_numpy(host).to(dev).add_(i * 1e-3) for i in range(nsets)]
+    ys = [torch.empty(G2_SHAPE, dtype=torch.float32, device=dev) for _ in range(nsets)]
+
+    def call(i):
+        dipcu.GaussFIR(xs[i], [2.0, 2.0], [0, 0], ["mirror"], 3.0, out=ys[i])
+
+    for i in range(max(args.warmup, nsets)):
+        call(i % nsets)
+    graphs = [[_capture(lambda i=i: call(i))] for i in range(nsets)]
+    for gl in graphs:
+        gl[0].replay()
+    total, per, clk = _timed(graphs, args.steps, dev)
+    npx = int(np.prod(G2_SHAPE))
+    value = world * npx * args.steps / (total * 1e-3) / 1e9
+    avg = sum(per) / len(per)
+    peak, kind = load_peaks()
+    line = _base_line(args, world, value, total / args.steps, G2_CONFIG)
+    ach = 8 * npx / (avg * 1e-3) / 1e9
+    line["roofline"] = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                        "traffic": None, "peak_source": kind, "kernel": "fused2d_kernel", "bytes_per_voxel": 8,
+                        "avg_kernel_ms": avg}
+    line["clocks"] = clk
+    line["gpu_launches"] = args.steps
+    # e2e: pinned host image in, result out.
+    h_in = torch.from_numpy(host).pin_memory()
+    h_out = torch.empty(G2_SHAPE, dtype=torch.float32).pin_memory()
+    d_in, d_out = torch.empty_like(xs[0]), torch.empty_like(ys[0])
+
+    def e2e():
+        d_in.copy_(h_in, non_blocking=True)
+        dipcu.GaussFIR(d_in, [2.0, 2.0], [0, 0], ["mirror"], 3.0, out=d_out)
+        h_out.copy_(d_out, non_blocking=True)
+
+    line["e2e"] = _e2e(e2e, npx, dev, world, 4 * npx, 4 * npx)
+    if rank == 0 and not args.no_cpu_baseline:
+        import oracle
+        if oracle.ref_available():
+            v, cores, reps = _ref_rate(lambda: oracle.ref_gauss(host, [2.0, 2.0], [0, 0], ["mirror"], 3.0), npx)
+            line["cpu_baseline"] = {"value": v, "unit": "Gvox/s", "cores": cores, "kind": "reference",
+                                    "sample": f"full 1024^2 image, min of {reps} reps"}
+    return _finish(line, world)
+
+
+def _e2e(step, nvox, dev, world, h2d, d2h, steps=20):
+    import torch
+    for _ in range(2):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stream = torch.cuda.current_stream(dev)
+    e0.record(stream)
+    for _ in range(steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    return {"value": world * nvox / (ms * 1e-3) / 1e9, "unit": "Gvox/s", "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(d2h), "ms_per_step": ms}
+
+
+# ---- batched uneven 2D (512 images) --------------------------------------------------------------
+
+B_SIGMAS = [0.8, 1.0, 2.0, 4.0, 8.0]
+B_BCS = ["mirror", "periodic", "add zeros"]
+B_CONFIG = {"workload": "batched dip::GaussFIR: 512 2D sfloat images, sides uniform 64..2048, sigma from "
+                        "{0.8,1,2,4,8} per image, order per axis from {0,1,2}, boundary from {mirror, periodic, "
+                        "add zeros}, truncation 3; one persistent launch replayed as a CUDA graph, autotuned tiles",
+            "l2": "the batch holds 2.3 GB of input and 2.3 GB of output (> 126 MB L2)"}
+
+
+def make_batch_params(seed=0, n=512):
+    rng = np.random.default_rng(seed)
+    shapes, params = [], []
+    for _ in range(n):
+        h, w = (int(v) for v in rng.integers(64, 2049, 2))
+        shapes.append((h, w))
+        params.append((float(rng.choice(B_SIGMAS)), [int(rng.integers(0, 3)), int(rng.integers(0, 3))],
+                       str(rng.choice(B_BCS))))
+    return shapes, params
+
+
+def run_batch(args):
+    import torch
+    import diplib_b200 as dipcu
+    from diplib_b200.batch import BatchPlan
+    world, rank, dev = _device(args)
+    shapes, params = make_batch_params(seed=rank)
+    gen = torch.Generator(device=dev).manual_seed(20 + rank)
+    ins = [torch.rand(s, generator=gen, device=dev) for s in shapes]
+    outs = [torch.empty(s, device=dev) for s in shapes]
+    plan = BatchPlan(ins, outs, [p[0] for p in params], [p[1] for p in params], [p[2] for p in params],
+                     graph=True, autotune=True)
+    for _ in range(args.warmup):
+        plan.run()
+    torch.cuda.synchronize()
+
+    class _G:
+        def replay(self):
+            plan.run()
+
+    total, per, clk = _timed([[_G()]], args.steps, dev)
+    npx = sum(h * w for h, w in shapes)
+    value = world * npx * args.steps / (total * 1e-3) / 1e9
+    avg = sum(per) / len(per)
+    peak, kind = load_peaks()
+    line = _base_line(args, world, value, total / args.steps, B_CONFIG)
+    line["config"]["plan"] = plan.info()
+    ach = 8 * npx / (avg * 1e-3) / 1e9
+    line["roofline"] = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                        "traffic": None, "peak_source": kind, "kernel": "batch_kernel (persistent work queue)",
+                        "bytes_per_voxel": 8, "avg_kernel_ms": avg}
+    line["clocks"] = clk
+    line["gpu_launches"] = 2 * args.steps   # weights + persistent kernel per graph
+    # The same per-pixel work as single large images: per (sigma, orders) combination of the
+    # batch, the plain path's rate on one 4096x4096 image; the batch's pixel shares weight them.
+    share = {}
+    for (h, w), (sg, o, _) in zip(shapes, params):
+        key = (sg, o[0], o[1])
+        share[key] = share.get(key, 0) + h * w
+    big = torch.rand((4096, 4096), generator=gen, device=dev)
+    bigs = [big, big.clone().add_(1e-3)]
+    bigo = [torch.empty_like(big) for _ in range(2)]
+    t_single = 0.0
+    rates = {}
+    for key, px in sorted(share.items()):
+        sg, ox, oy = key
+        gl = [[_capture(lambda i=i: dipcu.GaussFIR(bigs[i], [sg, sg], [ox, oy], ["mirror"], 3.0, out=bigo[i]))]
+              for i in range(2)]
+        for g in gl:
+            g[0].replay()
+        tt, _, _ = _timed(gl, 10, dev)
+        r = 4096 * 4096 * 10 / (tt * 1e-3) / 1e9
+        rates[f"s{sg}_o{ox}{oy}"] = round(r, 2)
+        t_single += px / (r * 1e9)
+    single_rate = npx / t_single / 1e9
+    line["vs_single_image"] = {"single_image_gvox_s": single_rate, "ratio": value / world / single_rate,
+                               "how": "plain dipcu_gauss_fir on one 4096^2 image per (sigma, orders) combination, "
+                                      "weighted by the batch's pixel shares", "rates": rates}
+    # e2e: every image in from pinned host memory, every result back.
+    h_in = [t.cpu().pin_memory() for t in ins]
+    h_out = [torch.empty(s).pin_memory() for s in shapes]
+
+    def e2e():
+        for a, b in zip(h_in, ins):
+            b.copy_(a, non_blocking=True)
+        plan.run()
+        for a, b in zip(h_out, outs):
+            a.copy_(b, non_blocking=True)
+
+    line["e2e"] = _e2e(e2e, npx, dev, world, 4 * npx, 4 * npx, steps=5)
+    if rank == 0 and not args.no_cpu_baseline:
+        import oracle
+        if oracle.ref_available():
+            hs = [t.cpu().numpy() for t in ins[:24]]
+            sample_px = sum(a.size for a in hs)
+
+            def ref():
+                for a, (sg, o, bc) in zip(hs, params[:24]):
+                    oracle.ref_gauss(a, [sg, sg], o, [bc], 3.0)
+
+            v, cores, reps = _ref_rate(ref, sample_px)
+            line["cpu_baseline"] = {"value": v, "unit": "Gvox/s", "cores": cores, "kind": "reference",
+                                    "sample": f"the first 24 images of the batch ({sample_px / 1e6:.1f} Mpx), "
+                                              f"min of {reps} reps"}
+    plan.close()
+    return _finish(line, world)
+
+
+# ---- differentiable 2D Gaussian (2048x2048, sigma 3, four orders, forward + backward) -------------
+
+D_SHAPE = (2048, 2048)
+D_ORDERS = [(0, 0), (1, 0), (0, 1), (2, 0)]
+D_CONFIG = {"workload": "differentiable dip::GaussFIR 2D 2048^2 sfloat, sigma 3, orders (0,0),(1,0),(0,1),(2,0), "
+                        "mirror; step = forward + backward (input and sigma gradients) of all four",
+            "l2": "4 rotating sets of input, upstream gradient, output and gradients (268 MB) > 126 MB L2"}
+
+
+def run_fwdbwd(args):
+    import torch
+    import diplib_b200 as dipcu
+    from diplib_b200 import torch_ops
+    world, rank, dev = _device(args)
+    nsets = 4
+    gen = torch.Generator(device=dev).manual_seed(30 + rank)
+    xs = [torch.rand(D_SHAPE, generator=gen, device=dev) for _ in range(nsets)]
+    gys = [torch.randn(D_SHAPE, generator=gen, device=dev) for _ in range(nsets)]
+    ys = [torch.empty(D_SHAPE, device=dev) for _ in range(nsets)]
+    gxs = [torch.empty(D_SHAPE, device=dev) for _ in range(nsets)]
+    gss = [torch.empty(2, dtype=torch.float64, device=dev) for _ in range(nsets)]
+
+    def fwd(i, o):
+        dipcu.GaussFIR(xs[i], [3.0, 3.0], list(o), ["mirror"], 3.0, out=ys[i])
+
+    def bwd(i, o):
+        gx, gs = torch_ops.gauss_backward(gys[i], xs[i], [3.0, 3.0], list(o), ["mirror"], 3.0, True, True)
+        gxs[i].copy_(gx)
+        gss[i].copy_(gs)
+
+    def bwd_raw(i, o):
+        import ctypes
+        from diplib_b200 import _abi
+        d_go, d_x, d_gx = dipcu.image_desc(gys[i]), dipcu.image_desc(xs[i]), dipcu.image_desc(gxs[i])
+        dipcu.filtering.check(_abi.lib().dipcu_gauss_fir_backward(
+            ctypes.byref(d_go), ctypes.byref(d_x), ctypes.byref(d_gx), ctypes.c_void_p(gss[i].data_ptr()),
+            (ctypes.c_double * 2)(3.0, 3.0), (ctypes.c_uint32 * 2)(*o), (ctypes.c_int32 * 2)(0, 0), 3.0,
+            ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+
+    for i in range(nsets):
+        for o in D_ORDERS:
+            fwd(i, o)
+            bwd(i, o)
+    torch.cuda.synchronize()
+    g_f = [[_capture(lambda i=i, o=o: fwd(i, o)) for o in D_ORDERS] for i in range(nsets)]
+    g_fb = [[_capture(lambda i=i, o=o: (fwd(i, o), bwd_raw(i, o))) for o in D_ORDERS] for i in range(nsets)]
+    for gl in g_f + g_fb:
+        for g in gl:
+            g.replay()
+    t_f, per_f, _ = _timed(g_f, args.steps, dev)
+    t_fb, per_fb, clk = _timed(g_fb, args.steps, dev)
+    npx = int(np.prod(D_SHAPE)) * len(D_ORDERS)
+    value = world * npx * args.steps / (t_fb * 1e-3) / 1e9
+    peak, kind = load_peaks()
+    line = _base_line(args, world, value, t_fb / args.steps, D_CONFIG)
+    ach = 20 * npx / (t_fb / args.steps * 1e-3) / 1e9
+    line["roofline"] = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                        "traffic": None, "peak_source": kind, "kernel": "whole step (forward 8 B + backward 12 B "
+                        "per pixel and order)", "bytes_per_voxel": 20, "avg_kernel_ms": t_fb / args.steps}
+    line["forward_only"] = {"ms_per_step": t_f / args.steps, "gvox_s": world * npx * args.steps / (t_f * 1e-3) / 1e9,
+                            "fwd_plus_bwd_over_fwd": t_fb / t_f}
+    line["clocks"] = clk
+    line["gpu_launches"] = None
+    if rank == 0 and not args.no_cpu_baseline:
+        import oracle
+        if oracle.ref_available():
+            hx = xs[0].cpu().numpy()
+
+            def ref():
+                for o in D_ORDERS:
+                    oracle.ref_gauss(hx, [3.0, 3.0], list(o), ["mirror"], 3.0)
+
+            v, cores, reps = _ref_rate(ref, npx)
+            line["cpu_baseline"] = {"value": v, "unit": "Gvox/s", "cores": cores, "kind": "reference",
+                                    "sample": f"forward only (DIPlib has no backward): the four orders on one "
+                                              f"2048^2 image, min of {reps} reps"}
+    return _finish(line, world)
+
+
+# ---- differentiable structure tensor (8 x 192^3, forward + backward) ------------------------------
+
+S_SHAPE = (192, 192, 192)
+S_BATCH = 8
+S_CONFIG = {"workload": "differentiable dip::StructureTensor, 8 sfloat volumes of 192^3 (Gauss sigma 2 of N(0,1)), "
+                        "gradient sigma 1, tensor sigma 4, mirror; loss = sum of the 6 components times N(0,1) "
+                        "weights; step = forward + backward w.r.t. the input of all 8 (gradient images recomputed)",
+            "l2": "8 volumes with 6-component tensors and weights (2.9 GB) > 126 MB L2"}
+
+
+def run_structure_tensor(args):
+    import torch
+    from diplib_b200 import torch_ops
+    world, rank, dev = _device(args)
+    gen = torch.Generator(device=dev).manual_seed(40 + rank)
+    import diplib_b200 as dipcu
+    xs = []
+    for _ in range(S_BATCH):
+        n = torch.randn(S_SHAPE, generator=gen, device=dev)
+        xs.append(dipcu.GaussFIR(n, 2.0, 0, "mirror", 3.0))
+    ws = [torch.randn((6,) + S_SHAPE, generator=gen, device=dev) for _ in range(S_BATCH)]
+    ts = [None] * S_BATCH
+    gxs = [None] * S_BATCH
+
+    def fwd(i):
+        ts[i] = torch_ops.structure_tensor(xs[i], 1.0, 4.0, "mirror", 3.0)
+
+    def fb(i):
+        ts[i] = torch_ops.structure_tensor(xs[i], 1.0, 4.0, "mirror", 3.0)
+        gxs[i] = torch_ops.structure_tensor_backward(ws[i], xs[i], 1.0, 4.0, "mirror", 3.0)
+
+    for i in range(S_BATCH):
+        fb(i)
+    torch.cuda.synchronize()
+    g_f = [[_capture(lambda i=i: fwd(i)) for i in range(S_BATCH)]]
+    g_fb = [[_capture(lambda i=i: fb(i)) for i in range(S_BATCH)]]
+    for gl in g_f + g_fb:
+        for g in gl:
+            g.replay()
+    t_f, _, _ = _timed(g_f, max(3, args.steps // 10), dev)
+    steps = max(3, args.steps // 10)
+    t_fb, _, clk = _timed(g_fb, steps, dev)
+    nvox = S_BATCH * int(np.prod(S_SHAPE))
+    value = world * nvox * steps / (t_fb * 1e-3) / 1e9
+    peak, kind = load_peaks()
+    args_steps = args.steps
+    args.steps = steps
+    line = _base_line(args, world, value, t_fb / steps, S_CONFIG)
+    args.steps = args_steps
+    ach = 60 * nvox / (t_fb / steps * 1e-3) / 1e9
+    line["roofline"] = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                        "traffic": None, "peak_source": kind, "kernel": "whole step (forward 28 B + backward 32 B "
+                        "per voxel)", "bytes_per_voxel": 60, "avg_kernel_ms": t_fb / steps}
+    line["forward_only"] = {"ms_per_step": t_f / steps, "gvox_s": world * nvox * steps / (t_f * 1e-3) / 1e9,
+                            "fwd_plus_bwd_over_fwd": t_fb / t_f}
+    line["clocks"] = clk
+    line["gpu_launches"] = None
+    if rank == 0 and not args.no_cpu_baseline:
+        import oracle
+        if oracle.ref_available():
+            hx = xs[0].cpu().numpy()
+            v, cores, reps = _ref_rate(lambda: oracle.ref_structure_tensor(hx, 1.0, 4.0, "mirror", 3.0),
+                                       hx.size, budget_s=10.0, max_reps=5)
+            line["cpu_baseline"] = {"value": v, "unit": "Gvox/s", "cores": cores, "kind": "reference",
+                                    "sample": f"forward only (DIPlib has no backward): one 192^3 volume, "
+                                              f"min of {reps} reps"}
+    return _finish(line, world)
+
+
+WORKLOADS = {"gauss2d": run_gauss2d, "batch": run_batch, "fwdbwd": run_fwdbwd,
+             "structure_tensor": run_structure_tensor}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -336,11 +765,16 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="dipcu", choices=["dipcu", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="gauss3d", choices=["gauss3d"] + sorted(WORKLOADS),
+                    help="gauss3d: the headline 256^3 uint16 volume (default); the others are the further "
+                         "configurations (plain 2D, batched uneven 2D, differentiable 2D, structure tensor)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.workload != "gauss3d":
+        return WORKLOADS[args.workload](args)
     return run_gpu_arm(args)
 
 
