@@ -9,10 +9,12 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <type_traits>
 #include <utility>
 
 #include "fused.cuh"
 #include "fused3d_tma.cuh"
+#include "fused3d_ws.cuh"
 
 namespace dipcu {
 
@@ -189,6 +191,69 @@ cudaError_t run3d_tma( FusedArgs& a, cudaStream_t s ) {
    return cudaGetLastError();
 }
 
+// Warp-specialised 3D kernel; cudaErrorNotSupported when its conditions do not hold (TMA layout,
+// x-y boundary conditions whose halo sources leave the box), so that the caller falls back.
+template< typename TIn, int HX, int HY, int HZ, bool OX, bool OY, bool OZ >
+cudaError_t run3d_ws( FusedArgs& a, cudaStream_t s ) {
+   using G = W5Geom< TIn, HX, HY, HZ >;
+   if constexpr( !G::fits ) {
+      return cudaErrorNotSupported;
+   } else {
+      constexpr int esz = sizeof( TIn );
+      if( a.ss[ 1 ] <= 0 || a.ss[ 2 ] <= 0 || ( a.nb > 1 && a.sb <= 0 )) { return cudaErrorNotSupported; }
+      if(( reinterpret_cast< uintptr_t >( a.src ) & 15 ) != 0 ) { return cudaErrorNotSupported; }
+      if(( a.ss[ 1 ] * esz ) % 16 || ( a.ss[ 2 ] * esz ) % 16 || ( a.nb > 1 && ( a.sb * esz ) % 16 )) { return cudaErrorNotSupported; }
+      if( a.n[ 0 ] > 0x3fffffff || a.n[ 1 ] > 0x3fffffff || a.n[ 2 ] > 0x3fffffff || a.nb > 0x3fffffff ) { return cudaErrorNotSupported; }
+      bool const flt = std::is_same< TIn, float >::value;
+      for( int d = 0; d < 2; ++d ) {
+         int32_t const bc = a.bc[ d ];
+         bool ok = bc == BC_SYMMETRIC_MIRROR || bc == BC_ZERO_ORDER_EXTRAPOLATE || bc == BC_ADD_ZEROS ||
+                   ( flt && bc == BC_ASYMMETRIC_MIRROR );
+         int64_t const h = d == 0 ? HX : HY;
+         if( !ok || a.n[ d ] <= h ) { return cudaErrorNotSupported; }   // single reflection: sources in the box
+      }
+      if( !bc_is_index_map( a.bc[ 2 ] )) { return cudaErrorNotSupported; }
+      W5Args z{};
+      CUtensorMapDataType dt = sizeof( TIn ) == 2 ? CU_TENSOR_MAP_DATA_TYPE_UINT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+      cuuint64_t dims[ 4 ] = { static_cast< cuuint64_t >( a.n[ 0 ] ), static_cast< cuuint64_t >( a.n[ 1 ] ),
+                               static_cast< cuuint64_t >( a.n[ 2 ] ), static_cast< cuuint64_t >( a.nb ) };
+      cuuint64_t strides[ 3 ] = { static_cast< cuuint64_t >( a.ss[ 1 ] * esz ), static_cast< cuuint64_t >( a.ss[ 2 ] * esz ),
+                                  static_cast< cuuint64_t >(( a.nb > 1 ? a.sb : a.ss[ 2 ] * a.n[ 2 ] ) * esz ) };
+      if( strides[ 2 ] % 16 ) { strides[ 2 ] = ( strides[ 2 ] + 15 ) / 16 * 16; }
+      cuuint32_t box[ 4 ] = { static_cast< cuuint32_t >( G::BW ), static_cast< cuuint32_t >( G::BH ), 1, 1 };
+      if( encode_tmap( &z.tmap, dt, a.src, dims, strides, box ) != CUDA_SUCCESS ) { return cudaErrorNotSupported; }
+      z.dst = a.dst;
+      for( int i = 0; i < 3; ++i ) {
+         z.n[ i ] = static_cast< int32_t >( a.n[ i ] );
+         z.ds[ i ] = a.ds[ i ];
+         z.bc[ i ] = a.bc[ i ];
+         for( int k = 0; k < kFusedMaxTaps; ++k ) { z.w[ i ][ k ] = make_float2( a.w[ i ][ k ], a.w[ i ][ k ] ); }
+      }
+      z.nb = static_cast< int32_t >( a.nb );
+      z.db = a.db;
+      z.vec_store = (( reinterpret_cast< uintptr_t >( a.dst ) & 7 ) == 0 && a.ds[ 1 ] % 2 == 0 && a.ds[ 2 ] % 2 == 0 &&
+                     ( a.nb <= 1 || a.db % 2 == 0 )) ? 1 : 0;
+      z.tiles_x = static_cast< int32_t >(( a.n[ 0 ] + G::OFF + G::TX - 1 ) / G::TX );
+      z.tiles_y = static_cast< int32_t >(( a.n[ 1 ] + G::TY - 1 ) / G::TY );
+      z.units = static_cast< int64_t >( z.tiles_x ) * z.tiles_y * a.nb * a.n[ 2 ];
+      z.status = device_status_ptr();
+      if( !z.status ) { return cudaErrorUnknown; }
+      auto kern = fused3d_ws_kernel< TIn, HX, HY, HZ, OX, OY, OZ >;
+      size_t smem = G::BYTES;
+      int per_sm = prepare_kernel( kern, G::NT, smem );
+      if( per_sm < 1 ) { return cudaErrorInvalidConfiguration; }
+      static int const want = getenv( "DIPCU_W5_CTAS_PER_SM" ) ? atoi( getenv( "DIPCU_W5_CTAS_PER_SM" )) : 4;
+      if( per_sm > want ) { per_sm = want; }
+      if( per_sm < 1 ) { per_sm = 1; }
+      int64_t nctas = static_cast< int64_t >( sm_count() ) * per_sm;
+      int64_t max_ctas = z.units / ( 4 * HZ + 4 );   // keep chunks long against the 2*HZ halo planes
+      if( nctas > max_ctas ) { nctas = max_ctas; }
+      if( nctas < 1 ) { nctas = 1; }
+      kern<<< static_cast< unsigned >( nctas ), G::NT, smem, s >>>( z );
+      return cudaGetLastError();
+   }
+}
+
 template< typename TIn, int HX, int HY, bool OX, bool OY >
 cudaError_t run2d( FusedArgs& a, cudaStream_t s ) {
    constexpr int TX = 64, TY = 32, RX = 4, RY = 8;
@@ -209,6 +274,12 @@ cudaError_t run2d( FusedArgs& a, cudaStream_t s ) {
 template< typename TIn, int HX, int HY, int HZ, bool OX, bool OY, bool OZ >
 cudaError_t run3d( FusedArgs& a, cudaStream_t s ) {
    if( !getenv( "DIPCU_NO_TMA" )) {
+      if constexpr( sizeof( TIn ) == 2 || std::is_same< TIn, float >::value ) {
+         if( !getenv( "DIPCU_NO_WS" )) {
+            cudaError_t e = run3d_ws< TIn, HX, HY, HZ, OX, OY, OZ >( a, s );
+            if( e != cudaErrorNotSupported ) { return e; }
+         }
+      }
       cudaError_t e = run3d_tma< TIn, HX, HY, HZ, OX, OY, OZ >( a, s );
       if( e != cudaErrorNotSupported ) { return e; }
    }

@@ -31,6 +31,20 @@ __device__ __forceinline__ void mbar_arrive_expect_tx( uint64_t* bar, uint32_t b
    asm volatile( "mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"( smem_u32( bar )), "r"( bytes ) : "memory" );
 }
 
+__device__ __forceinline__ void mbar_arrive( uint64_t* bar ) {
+   asm volatile( "mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"( smem_u32( bar )) : "memory" );
+}
+
+// Named barrier over the first `threads` threads of the block (id 1..15; 0 is __syncthreads).
+__device__ __forceinline__ void named_bar_sync( int id, int threads ) {
+   asm volatile( "bar.sync %0, %1;" :: "r"( id ), "r"( threads ) : "memory" );
+}
+
+// Arrives at named barrier `id` without waiting (producer side of a producer/consumer pair).
+__device__ __forceinline__ void named_bar_arrive( int id, int threads ) {
+   asm volatile( "bar.arrive %0, %1;" :: "r"( id ), "r"( threads ) : "memory" );
+}
+
 // Bounded wait for the phase with parity `parity` to complete.  Returns false on timeout.
 __device__ __forceinline__ bool mbar_wait( uint64_t* bar, uint32_t parity ) {
    uint32_t addr = smem_u32( bar );
