@@ -220,8 +220,12 @@ cudaError_t run3d_ws( FusedArgs& a, cudaStream_t s ) {
       cuuint64_t strides[ 3 ] = { static_cast< cuuint64_t >( a.ss[ 1 ] * esz ), static_cast< cuuint64_t >( a.ss[ 2 ] * esz ),
                                   static_cast< cuuint64_t >(( a.nb > 1 ? a.sb : a.ss[ 2 ] * a.n[ 2 ] ) * esz ) };
       if( strides[ 2 ] % 16 ) { strides[ 2 ] = ( strides[ 2 ] + 15 ) / 16 * 16; }
-      cuuint32_t box[ 4 ] = { static_cast< cuuint32_t >( G::BW ), static_cast< cuuint32_t >( G::BH ), 1, 1 };
-      if( encode_tmap( &z.tmap, dt, a.src, dims, strides, box ) != CUDA_SUCCESS ) { return cudaErrorNotSupported; }
+      cuuint32_t box1[ 4 ] = { static_cast< cuuint32_t >( G::BW ), static_cast< cuuint32_t >( G::BH ), 1, 1 };
+      cuuint32_t box2[ 4 ] = { static_cast< cuuint32_t >( G::BW ), static_cast< cuuint32_t >( G::BH ), a.n[ 2 ] >= 2 ? 2u : 1u, 1 };
+      if( encode_tmap( &z.tmap1, dt, a.src, dims, strides, box1 ) != CUDA_SUCCESS ||
+          encode_tmap( &z.tmap2, dt, a.src, dims, strides, box2 ) != CUDA_SUCCESS ) {
+         return cudaErrorNotSupported;
+      }
       z.dst = a.dst;
       for( int i = 0; i < 3; ++i ) {
          z.n[ i ] = static_cast< int32_t >( a.n[ i ] );
