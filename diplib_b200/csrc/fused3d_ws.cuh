@@ -80,7 +80,7 @@ struct W5Geom {
    static constexpr int NS = w5_pow2( 2 * HZ + 8 );
    static constexpr int RZ = ( NS - 2 * HZ ) / 2 / 2 * 2;
    static constexpr int NWZ = ( ZITEMS + 63 ) / 64;                    // z-pass warps (~2 items per thread)
-   static constexpr int NWI = 5;                                       // in-plane warps
+   static constexpr int NWI = 6;                                       // in-plane warps
    static constexpr int NWC = NWI + NWZ;
    static constexpr int NT = NWC * 32;
    static constexpr int PLANE_BYTES = BW * BH * static_cast< int >( sizeof( TIn ));
@@ -108,6 +108,7 @@ struct W5Geom {
    static_assert( PLANE_BYTES % 16 == 0 && OFF_B2 % 16 == 0 && OFF_RING % 16 == 0 && OFF_TAB % 16 == 0 &&
                   OFF_BAR % 16 == 0, "16-byte aligned sections" );
    static constexpr bool fits = BYTES <= 227 * 1024;
+   static constexpr int MINB = BYTES <= 113 * 1024 ? 2 : 1;            // CTAs per SM the registers must allow
 };
 
 // Column pair (box columns 2p, 2p+1) of stage row r, as float.
@@ -182,7 +183,7 @@ __device__ __forceinline__ void w5_issue_pair( W5Args const& a, unsigned char* s
 }
 
 template< typename TIn, int HX, int HY, int HZ, bool OX, bool OY, bool OZ >
-__global__ void __launch_bounds__( W5Geom< TIn, HX, HY, HZ >::NT ) fused3d_ws_kernel( W5Args const __grid_constant__ a ) {
+__global__ void __launch_bounds__( W5Geom< TIn, HX, HY, HZ >::NT, W5Geom< TIn, HX, HY, HZ >::MINB ) fused3d_ws_kernel( W5Args const __grid_constant__ a ) {
    using G = W5Geom< TIn, HX, HY, HZ >;
    constexpr int TX = G::TX, TY = G::TY, BW = G::BW, BH = G::BH, NS = G::NS, RZ = G::RZ, SPW = G::SPW;
    constexpr int NWI = G::NWI, NWZ = G::NWZ, NWC = G::NWC, XQ = G::XQ, E = G::E;
@@ -365,6 +366,7 @@ __global__ void __launch_bounds__( W5Geom< TIn, HX, HY, HZ >::NT ) fused3d_ws_ke
                   }
                   // x pass: 2x2 output points -> ring plane
                   float* const rs = ring + ( q & ( NS - 1 )) * G::RING_PLANE;
+#pragma unroll
                   for( int it = lane; it < G::XITEMS; it += 32 ) {
                      int const cp = it % ( TX / 2 ), rp = it / ( TX / 2 );
                      float4 const* row = b2 + rp * ( BW / 2 ) + cp;
@@ -405,6 +407,7 @@ __global__ void __launch_bounds__( W5Geom< TIn, HX, HY, HZ >::NT ) fused3d_ws_ke
             named_bar_sync( kBarReady + ( blk & 1u ), NWC * 32 );
             int const ob = j * RZ;
             int const nout = nout_total - ob < RZ ? nout_total - ob : RZ;
+#pragma unroll
             for( int it = zt; it < G::ZITEMS; it += NWZ * 32 ) {
                int const cp = it % ( TX / 2 ), y = it / ( TX / 2 );
                float2 acc[ RZ ];
