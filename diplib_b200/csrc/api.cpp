@@ -102,7 +102,6 @@ bool try_fused( dipcu_image_desc const* in, dipcu_image_desc const* out, std::ve
       key.h[ i ] = static_cast< int32_t >( f[ axes[ i ] ].h );
       key.odd[ i ] = f[ axes[ i ] ].odd;
    }
-   if( !fused_available( key )) { return false; }
    FusedArgs a{};
    a.src = in->data;
    a.dst = static_cast< float* >( out->data );
@@ -130,6 +129,11 @@ bool try_fused( dipcu_image_desc const* in, dipcu_image_desc const* out, std::ve
       a.sb = 0;
       a.db = 0;
    }
+   if( np == 2 ) {
+      *err = launch_fused2d_ws( key, a, stream );
+      if( *err != cudaErrorNotSupported ) { return true; }
+   }
+   if( !fused_available( key )) { return false; }
    *err = launch_fused( key, a, stream );
    return *err != cudaErrorNotSupported;
 }

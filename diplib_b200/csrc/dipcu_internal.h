@@ -74,6 +74,10 @@ cudaError_t launch_fused( FusedKey const& key, FusedArgs& args, cudaStream_t str
 
 bool fused_available( FusedKey const& key );
 
+// Warp-per-tile 2D kernel (any half-widths up to 12, float or uint16 input, the x-y boundary
+// conditions it handles); cudaErrorNotSupported when it does not apply.
+cudaError_t launch_fused2d_ws( FusedKey const& key, FusedArgs& args, cudaStream_t stream );
+
 // Adjoint halo fold along one axis (k_backward.cu).
 struct FoldPass {
    void const* g;            // gradient w.r.t. the forward pass output (compute type)

@@ -15,6 +15,7 @@
 #include "fused.cuh"
 #include "fused3d_tma.cuh"
 #include "fused3d_ws.cuh"
+#include "fused2d_ws.cuh"
 
 namespace dipcu {
 
@@ -258,6 +259,74 @@ cudaError_t run3d_ws( FusedArgs& a, cudaStream_t s ) {
    }
 }
 
+// Warp-per-tile 2D kernel for half-widths up to B on both axes (taps zero beyond each axis' h);
+// cudaErrorNotSupported when its conditions do not hold, so that the caller falls back.
+template< typename TIn, int B >
+cudaError_t run2d_ws( FusedArgs& a, int32_t const* odd, cudaStream_t s ) {
+   using G = W2Geom< TIn, B >;
+   static_assert( G::fits, "shared memory" );
+   constexpr int esz = sizeof( TIn );
+   if( a.ss[ 0 ] != 1 || a.ss[ 1 ] <= 0 || ( a.nb > 1 && a.sb <= 0 )) { return cudaErrorNotSupported; }
+   if(( reinterpret_cast< uintptr_t >( a.src ) & 15 ) != 0 ) { return cudaErrorNotSupported; }
+   if(( a.ss[ 1 ] * esz ) % 16 || ( a.nb > 1 && ( a.sb * esz ) % 16 )) { return cudaErrorNotSupported; }
+   if( a.n[ 0 ] > 0x3fffffff || a.n[ 1 ] > 0x3fffffff || a.nb > 0x3fffffff ) { return cudaErrorNotSupported; }
+   bool const flt = std::is_same< TIn, float >::value;
+   for( int d = 0; d < 2; ++d ) {
+      int32_t const bc = a.bc[ d ];
+      bool ok = bc == BC_SYMMETRIC_MIRROR || bc == BC_ZERO_ORDER_EXTRAPOLATE || bc == BC_ADD_ZEROS ||
+                ( flt && bc == BC_ASYMMETRIC_MIRROR );
+      if( !ok || a.n[ d ] <= B ) { return cudaErrorNotSupported; }
+   }
+   W2Args z{};
+   CUtensorMapDataType dt = sizeof( TIn ) == 2 ? CU_TENSOR_MAP_DATA_TYPE_UINT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+   cuuint64_t dims[ 4 ] = { static_cast< cuuint64_t >( a.n[ 0 ] ), static_cast< cuuint64_t >( a.n[ 1 ] ), 1,
+                            static_cast< cuuint64_t >( a.nb ) };
+   cuuint64_t strides[ 3 ] = { static_cast< cuuint64_t >( a.ss[ 1 ] * esz ),
+                               static_cast< cuuint64_t >( a.ss[ 1 ] * a.n[ 1 ] * esz ),
+                               static_cast< cuuint64_t >(( a.nb > 1 ? a.sb : a.ss[ 1 ] * a.n[ 1 ] ) * esz ) };
+   for( auto& v : strides ) { if( v % 16 ) { v = ( v + 15 ) / 16 * 16; } }
+   cuuint32_t box[ 4 ] = { static_cast< cuuint32_t >( G::BW ), static_cast< cuuint32_t >( G::BH ), 1, 1 };
+   if( encode_tmap( &z.tmap, dt, a.src, dims, strides, box ) != CUDA_SUCCESS ) { return cudaErrorNotSupported; }
+   z.dst = a.dst;
+   for( int i = 0; i < 2; ++i ) {
+      z.n[ i ] = static_cast< int32_t >( a.n[ i ] );
+      z.ds[ i ] = a.ds[ i ];
+      z.bc[ i ] = a.bc[ i ];
+      float const sg = odd[ i ] ? -1.f : 1.f;
+      z.sgn[ i ] = make_float2( sg, sg );
+      for( int k = 0; k < kFusedMaxTaps; ++k ) { z.w[ i ][ k ] = make_float2( a.w[ i ][ k ], a.w[ i ][ k ] ); }
+   }
+   z.nb = static_cast< int32_t >( a.nb );
+   z.db = a.db;
+   z.vec_store = (( reinterpret_cast< uintptr_t >( a.dst ) & 7 ) == 0 && a.ds[ 1 ] % 2 == 0 &&
+                  ( a.nb <= 1 || a.db % 2 == 0 )) ? 1 : 0;
+   z.tiles_x = static_cast< int32_t >(( a.n[ 0 ] + G::OFF + G::TX - 1 ) / G::TX );
+   z.tiles_y = static_cast< int32_t >(( a.n[ 1 ] + G::TY - 1 ) / G::TY );
+   z.ntiles = static_cast< int64_t >( z.tiles_x ) * z.tiles_y * a.nb;
+   z.status = device_status_ptr();
+   if( !z.status ) { return cudaErrorUnknown; }
+   auto kern = fused2d_ws_kernel< TIn, B >;
+   size_t smem = G::BYTES;
+   int per_sm = prepare_kernel( kern, G::NT, smem );
+   if( per_sm < 1 ) { return cudaErrorInvalidConfiguration; }
+   int64_t nctas = static_cast< int64_t >( sm_count() ) * per_sm;
+   int64_t const need = ( z.ntiles + G::NW - 1 ) / G::NW;
+   if( nctas > need ) { nctas = need; }
+   if( nctas < 1 ) { nctas = 1; }
+   kern<<< static_cast< unsigned >( nctas ), G::NT, smem, s >>>( z );
+   return cudaGetLastError();
+}
+
+template< typename TIn >
+cudaError_t run2d_ws_bucket( FusedArgs& a, int32_t const* h, int32_t const* odd, cudaStream_t s ) {
+   int const hm = h[ 0 ] > h[ 1 ] ? h[ 0 ] : h[ 1 ];
+   if( hm <= 4 ) { return run2d_ws< TIn, 4 >( a, odd, s ); }
+   if( hm <= 6 ) { return run2d_ws< TIn, 6 >( a, odd, s ); }
+   if( hm <= 9 ) { return run2d_ws< TIn, 9 >( a, odd, s ); }
+   if( hm <= 12 ) { return run2d_ws< TIn, 12 >( a, odd, s ); }
+   return cudaErrorNotSupported;
+}
+
 template< typename TIn, int HX, int HY, bool OX, bool OY >
 cudaError_t run2d( FusedArgs& a, cudaStream_t s ) {
    constexpr int TX = 64, TY = 32, RX = 4, RY = 8;
@@ -367,6 +436,13 @@ Entry const* find( FusedKey const& k ) {
 }
 
 } // namespace
+
+cudaError_t launch_fused2d_ws( FusedKey const& key, FusedArgs& args, cudaStream_t stream ) {
+   if( key.ndims != 2 || getenv( "DIPCU_NO_WS" )) { return cudaErrorNotSupported; }
+   if( key.in_dt == DT_SFLOAT ) { return run2d_ws_bucket< float >( args, key.h, key.odd, stream ); }
+   if( key.in_dt == DT_UINT16 ) { return run2d_ws_bucket< uint16_t >( args, key.h, key.odd, stream ); }
+   return cudaErrorNotSupported;
+}
 
 bool fused_available( FusedKey const& key ) {
    return find( key ) != nullptr;
