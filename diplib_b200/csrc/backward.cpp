@@ -62,6 +62,64 @@ int fail_cuda( cudaError_t e, char const* where ) {
    return record_error( DIPCU_ERR_CUDA, msg.c_str() );
 }
 
+// The whole 2D backward in one kernel (input gradient and both sigma gradients) when the layout
+// allows it: both processed axes filtered in float, x the axis of unit stride in grad_out,
+// grad_in and in, at most one other axis of size > 1 (a batch).  Returns -1 when it does not
+// apply, else the status.
+int try_fused_adjoint( dipcu_image_desc const* grad_out, dipcu_image_desc const* in, dipcu_image_desc const* grad_in,
+                       double* grad_sigma, std::vector< AxisFilter > const& f, std::vector< std::vector< double >> const& df,
+                       std::vector< int > const& order, cudaStream_t stream ) {
+   int const nd = grad_out->ndims;
+   int ax = -1, ay = -1;
+   for( int d : order ) {
+      bool unit = grad_out->strides[ d ] == 1 && ( !grad_in || grad_in->strides[ d ] == 1 ) &&
+                  ( !grad_sigma || ( in && in->strides[ d ] == 1 ));
+      if( unit && ax < 0 ) { ax = d; }
+   }
+   if( ax < 0 ) { return -1; }
+   for( int d : order ) { if( d != ax ) { ay = d; } }
+   int batch = -1;
+   for( int d = 0; d < nd; ++d ) {
+      if( d == ax || d == ay || grad_out->sizes[ d ] == 1 ) { continue; }
+      if( batch >= 0 ) { return -1; }
+      batch = d;
+   }
+   if( grad_sigma && ( !in || !( in->dtype == DT_SFLOAT || in->dtype == DT_UINT16 ))) { return -1; }
+   Adj2Params p{};
+   p.gy = static_cast< float const* >( grad_out->data );
+   p.gys1 = grad_out->strides[ ay ];
+   p.gyb = batch >= 0 ? grad_out->strides[ batch ] : 0;
+   p.x = grad_sigma ? in->data : nullptr;
+   p.x_dt = grad_sigma ? in->dtype : DT_SFLOAT;
+   p.xs1 = grad_sigma ? in->strides[ ay ] : 0;
+   p.xb = ( grad_sigma && batch >= 0 ) ? in->strides[ batch ] : 0;
+   p.gx = grad_in ? static_cast< float* >( grad_in->data ) : nullptr;
+   p.gxs1 = grad_in ? grad_in->strides[ ay ] : 0;
+   p.gxb = ( grad_in && batch >= 0 ) ? grad_in->strides[ batch ] : 0;
+   p.n[ 0 ] = grad_out->sizes[ ax ];
+   p.n[ 1 ] = grad_out->sizes[ ay ];
+   p.nb = batch >= 0 ? grad_out->sizes[ batch ] : 1;
+   int const axes[ 2 ] = { ax, ay };
+   for( int i = 0; i < 2; ++i ) {
+      AxisFilter const& af = f[ static_cast< size_t >( axes[ i ] ) ];
+      p.bc[ i ] = af.bc;
+      p.h[ i ] = static_cast< int32_t >( af.h );
+      p.odd[ i ] = af.odd;
+      p.taps[ i ] = af.taps.data();
+      p.dtaps[ i ] = df[ static_cast< size_t >( axes[ i ] ) ].data();
+   }
+   if( grad_sigma ) {
+      cudaError_t e = cudaMemsetAsync( grad_sigma, 0, sizeof( double ) * static_cast< size_t >( nd ), stream );
+      if( e != cudaSuccess ) { return fail_cuda( e, "cudaMemsetAsync" ); }
+      p.dsig[ 0 ] = grad_sigma + ax;
+      p.dsig[ 1 ] = grad_sigma + ay;
+   }
+   cudaError_t e = launch_fused_adjoint2d( p, stream );
+   if( e == cudaErrorNotSupported ) { return -1; }
+   if( e != cudaSuccess ) { return fail_cuda( e, "fused2d_adj_kernel" ); }
+   return DIPCU_OK;
+}
+
 } // namespace
 
 } // namespace dipcu
@@ -104,6 +162,10 @@ extern "C" int dipcu_gauss_fir_backward( dipcu_image_desc const* grad_out, dipcu
    {
       int64_t s = 1;
       for( int d = 0; d < nd; ++d ) { normal[ d ] = s; s *= ref->sizes[ d ]; }
+   }
+   if( P == 2 && !cdouble && ( grad_in || grad_sigma )) {
+      int st = try_fused_adjoint( grad_out, in, grad_in, grad_sigma, f, df, order, stream );
+      if( st != -1 ) { return st; }
    }
    size_t const esz = cdouble ? 8 : 4;
    int const nscratch = ( grad_sigma && P > 0 ) ? 2 : ( P > 2 ? 2 : ( P > 1 ? 1 : 0 ));

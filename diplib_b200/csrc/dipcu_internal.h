@@ -74,6 +74,25 @@ cudaError_t launch_fused( FusedKey const& key, FusedArgs& args, cudaStream_t str
 
 bool fused_available( FusedKey const& key );
 
+// Fused 2D adjoint (input gradient and both sigma gradients) of the Gaussian FIR.
+struct Adj2Params {
+   float const* gy;                   // dL/d(out), float, x stride 1
+   int64_t gys1, gyb;                 // row and batch strides
+   void const* x;                     // the forward input (nullptr: no sigma gradients)
+   int32_t x_dt;
+   int64_t xs1, xb;
+   float* gx;                         // dL/d(in), float, x stride 1 (nullptr: not wanted)
+   int64_t gxs1, gxb;
+   double* dsig[ 2 ];                 // dL/dsigma of the x and y axes (device; accumulated)
+   int64_t n[ 2 ], nb;
+   int32_t bc[ 2 ], h[ 2 ], odd[ 2 ];
+   double const* taps[ 2 ];           // h + 1 taps, centre first
+   double const* dtaps[ 2 ];          // their sigma derivatives (may be nullptr without sigma)
+};
+// cudaErrorNotSupported when the fused kernel does not apply (the caller runs the pass-by-pass
+// adjoint instead).
+cudaError_t launch_fused_adjoint2d( Adj2Params const& p, cudaStream_t stream );
+
 // Warp-per-tile 2D kernel (any half-widths up to 12, float or uint16 input, the x-y boundary
 // conditions it handles); cudaErrorNotSupported when it does not apply.
 cudaError_t launch_fused2d_ws( FusedKey const& key, FusedArgs& args, cudaStream_t stream );

@@ -16,6 +16,7 @@
 #include "fused3d_tma.cuh"
 #include "fused3d_ws.cuh"
 #include "fused2d_ws.cuh"
+#include "fused2d_adj.cuh"
 
 namespace dipcu {
 
@@ -317,6 +318,96 @@ cudaError_t run2d_ws( FusedArgs& a, int32_t const* odd, cudaStream_t s ) {
    return cudaGetLastError();
 }
 
+template< typename TIn, int B >
+cudaError_t run_adj2d( Adj2Params const& p, cudaStream_t s ) {
+   using G = A2Geom< TIn, B >;
+   static_assert( G::fits, "shared memory" );
+   bool const sig = p.x != nullptr && p.dsig[ 0 ] && p.dsig[ 1 ];
+   if( p.gys1 <= 0 || ( p.nb > 1 && p.gyb <= 0 )) { return cudaErrorNotSupported; }
+   if(( reinterpret_cast< uintptr_t >( p.gy ) & 15 ) || ( p.gys1 * 4 ) % 16 || ( p.nb > 1 && ( p.gyb * 4 ) % 16 )) {
+      return cudaErrorNotSupported;
+   }
+   constexpr int esz = sizeof( TIn );
+   if( sig && (( reinterpret_cast< uintptr_t >( p.x ) & 15 ) || p.xs1 <= 0 || ( p.xs1 * esz ) % 16 ||
+               ( p.nb > 1 && ( p.xb <= 0 || ( p.xb * esz ) % 16 )))) {
+      return cudaErrorNotSupported;
+   }
+   if( p.n[ 0 ] > 0x3fffffff || p.n[ 1 ] > 0x3fffffff || p.nb > 0x3fffffff ) { return cudaErrorNotSupported; }
+   for( int d = 0; d < 2; ++d ) {
+      int32_t const bc = p.bc[ d ];
+      bool ok = bc == BC_SYMMETRIC_MIRROR || bc == BC_ZERO_ORDER_EXTRAPOLATE || bc == BC_ADD_ZEROS || bc == BC_ASYMMETRIC_MIRROR;
+      if( !ok || p.n[ d ] <= B || p.h[ d ] > B || p.h[ d ] < 1 ) { return cudaErrorNotSupported; }
+   }
+   A2Args z{};
+   {
+      cuuint64_t dims[ 4 ] = { static_cast< cuuint64_t >( p.n[ 0 ] ), static_cast< cuuint64_t >( p.n[ 1 ] ), 1,
+                               static_cast< cuuint64_t >( p.nb ) };
+      cuuint64_t st[ 3 ] = { static_cast< cuuint64_t >( p.gys1 * 4 ), static_cast< cuuint64_t >( p.gys1 * p.n[ 1 ] * 4 ),
+                             static_cast< cuuint64_t >(( p.nb > 1 ? p.gyb : p.gys1 * p.n[ 1 ] ) * 4 ) };
+      for( auto& v : st ) { if( v % 16 ) { v = ( v + 15 ) / 16 * 16; } }
+      cuuint32_t box[ 4 ] = { static_cast< cuuint32_t >( G::BW ), static_cast< cuuint32_t >( G::BH ), 1, 1 };
+      if( encode_tmap( &z.tg, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, p.gy, dims, st, box ) != CUDA_SUCCESS ) { return cudaErrorNotSupported; }
+   }
+   if( sig ) {
+      cuuint64_t dims[ 4 ] = { static_cast< cuuint64_t >( p.n[ 0 ] ), static_cast< cuuint64_t >( p.n[ 1 ] ), 1,
+                               static_cast< cuuint64_t >( p.nb ) };
+      cuuint64_t st[ 3 ] = { static_cast< cuuint64_t >( p.xs1 * esz ), static_cast< cuuint64_t >( p.xs1 * p.n[ 1 ] * esz ),
+                             static_cast< cuuint64_t >(( p.nb > 1 ? p.xb : p.xs1 * p.n[ 1 ] ) * esz ) };
+      for( auto& v : st ) { if( v % 16 ) { v = ( v + 15 ) / 16 * 16; } }
+      cuuint32_t box[ 4 ] = { static_cast< cuuint32_t >( G::TX ), static_cast< cuuint32_t >( G::TY ), 1, 1 };
+      CUtensorMapDataType dt = esz == 2 ? CU_TENSOR_MAP_DATA_TYPE_UINT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+      if( encode_tmap( &z.tx, dt, p.x, dims, st, box ) != CUDA_SUCCESS ) { return cudaErrorNotSupported; }
+   }
+   z.gx = p.gx;
+   z.dsig[ 0 ] = sig ? p.dsig[ 0 ] : nullptr;
+   z.dsig[ 1 ] = sig ? p.dsig[ 1 ] : nullptr;
+   z.nb = static_cast< int32_t >( p.nb );
+   z.gs1 = p.gxs1;
+   z.gb = p.gxb;
+   for( int d = 0; d < 2; ++d ) {
+      z.n[ d ] = static_cast< int32_t >( p.n[ d ] );
+      z.bc[ d ] = p.bc[ d ];
+      z.h[ d ] = p.h[ d ];
+      float const sg = p.odd[ d ] ? -1.f : 1.f;
+      z.s[ d ] = make_float2( sg, sg );
+      for( int k = 0; k <= p.h[ d ]; ++k ) {
+         // C^T in the forward's pair form: the flipped taps of an odd kernel are its negation.
+         float const w = static_cast< float >( p.taps[ d ][ k ] ) * ( k > 0 ? sg : 1.f );
+         z.w[ d ][ k ] = make_float2( w, w );
+         if( sig ) {
+            float const wd = static_cast< float >( p.dtaps[ d ][ k ] ) * ( k > 0 ? sg : 1.f );
+            z.wd[ d ][ k ] = make_float2( wd, wd );
+         }
+      }
+   }
+   z.vec_store = p.gx && (( reinterpret_cast< uintptr_t >( p.gx ) & 7 ) == 0 && p.gxs1 % 2 == 0 && ( p.nb <= 1 || p.gxb % 2 == 0 )) ? 1 : 0;
+   z.tiles_x = static_cast< int32_t >(( p.n[ 0 ] + G::TX - 1 ) / G::TX );
+   z.tiles_y = static_cast< int32_t >(( p.n[ 1 ] + G::TY - 1 ) / G::TY );
+   z.ntiles = static_cast< int64_t >( z.tiles_x ) * z.tiles_y * p.nb;
+   z.status = device_status_ptr();
+   if( !z.status ) { return cudaErrorUnknown; }
+   auto kern = fused2d_adj_kernel< TIn, B >;
+   size_t smem = G::BYTES;
+   int per_sm = prepare_kernel( kern, G::NT, smem );
+   if( per_sm < 1 ) { return cudaErrorInvalidConfiguration; }
+   int64_t nctas = static_cast< int64_t >( sm_count() ) * per_sm;
+   int64_t const need = ( z.ntiles + G::NW - 1 ) / G::NW;
+   if( nctas > need ) { nctas = need; }
+   if( nctas < 1 ) { nctas = 1; }
+   kern<<< static_cast< unsigned >( nctas ), G::NT, smem, s >>>( z );
+   return cudaGetLastError();
+}
+
+template< typename TIn >
+cudaError_t run_adj2d_bucket( Adj2Params const& p, cudaStream_t s ) {
+   int const hm = p.h[ 0 ] > p.h[ 1 ] ? p.h[ 0 ] : p.h[ 1 ];
+   if( hm <= 4 ) { return run_adj2d< TIn, 4 >( p, s ); }
+   if( hm <= 6 ) { return run_adj2d< TIn, 6 >( p, s ); }
+   if( hm <= 9 ) { return run_adj2d< TIn, 9 >( p, s ); }
+   if( hm <= 12 ) { return run_adj2d< TIn, 12 >( p, s ); }
+   return cudaErrorNotSupported;
+}
+
 template< typename TIn >
 cudaError_t run2d_ws_bucket( FusedArgs& a, int32_t const* h, int32_t const* odd, cudaStream_t s ) {
    int const hm = h[ 0 ] > h[ 1 ] ? h[ 0 ] : h[ 1 ];
@@ -441,6 +532,13 @@ cudaError_t launch_fused2d_ws( FusedKey const& key, FusedArgs& args, cudaStream_
    if( key.ndims != 2 || getenv( "DIPCU_NO_WS" )) { return cudaErrorNotSupported; }
    if( key.in_dt == DT_SFLOAT ) { return run2d_ws_bucket< float >( args, key.h, key.odd, stream ); }
    if( key.in_dt == DT_UINT16 ) { return run2d_ws_bucket< uint16_t >( args, key.h, key.odd, stream ); }
+   return cudaErrorNotSupported;
+}
+
+cudaError_t launch_fused_adjoint2d( Adj2Params const& p, cudaStream_t stream ) {
+   if( getenv( "DIPCU_NO_WS" )) { return cudaErrorNotSupported; }
+   if( !p.x || p.x_dt == DT_SFLOAT ) { return run_adj2d_bucket< float >( p, stream ); }
+   if( p.x_dt == DT_UINT16 ) { return run_adj2d_bucket< uint16_t >( p, stream ); }
    return cudaErrorNotSupported;
 }
 

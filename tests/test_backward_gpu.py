@@ -180,3 +180,36 @@ def test_autograd_gradcheck(cuda):
     s1 = torch.tensor(1.7, dtype=torch.float64).cuda().requires_grad_()
     assert torch.autograd.gradcheck(lambda xx, ss: tops().gauss(xx, ss, [1, 0], ["periodic"], 3.0), (x, s1),
                                     eps=1e-6, atol=1e-7, rtol=1e-5)
+
+
+@pytest.mark.parametrize("case", [
+    ((48, 50), np.float32, [3.0, 3.0], [2, 1], "mirror"),
+    ((3, 40, 52), np.float32, [2.0, 1.5, 0.0], [1, 0, 0], "asym mirror"),      # batch axis
+    ((45, 60), np.uint16, [1.5, 2.5], [0, 1], "zero order"),
+    ((33, 70), np.float32, [4.0, 1.0], [0, 2], "add zeros"),
+])
+def test_fused_adjoint_matches_pass_by_pass_adjoint(cuda, case, monkeypatch):
+    """The one-kernel 2D backward against the pass-by-pass adjoint (line passes + halo folds) on
+    the same inputs: input gradient, sigma gradients, a batch axis, integer input."""
+    shape, dt, sig, ords, bc = case
+    rng = np.random.default_rng(sum(shape))
+    x = (rng.random(shape) * 1000).astype(dt) if dt == np.uint16 else rng.random(shape).astype(dt)
+    gy = rng.standard_normal(shape).astype(np.float32)
+    xt = torch.from_numpy(x.view(np.int16) if dt == np.uint16 else x).cuda()
+    if dt == np.uint16:
+        xt = xt.view(torch.uint16)
+    gt = torch.from_numpy(gy).cuda()
+    bcs = [bc] * len(shape)
+    gx1, gs1 = tops().gauss_backward(gt, xt, sig, ords, bcs, 3.0, True, True)
+    gx_only, _ = tops().gauss_backward(gt, xt, sig, ords, bcs, 3.0, True, False)
+    _, gs_only = tops().gauss_backward(gt, xt, sig, ords, bcs, 3.0, False, True)
+    torch.cuda.synchronize()
+    monkeypatch.setenv("DIPCU_NO_WS", "1")
+    gx2, gs2 = tops().gauss_backward(gt, xt, sig, ords, bcs, 3.0, True, True)
+    torch.cuda.synchronize()
+    g1, g2 = gx1.cpu().numpy(), gx2.cpu().numpy()
+    assert np.abs(g1 - g2).max() <= 1e-5 * np.abs(g2).max()
+    assert np.array_equal(gx_only.cpu().numpy(), g1)
+    s1, s2 = gs1.cpu().numpy(), gs2.cpu().numpy()
+    assert np.allclose(s1, s2, rtol=1e-4, atol=1e-4 * np.abs(s2).max()), (s1, s2)
+    assert np.allclose(gs_only.cpu().numpy(), s1, rtol=1e-6, atol=1e-9)
