@@ -209,7 +209,7 @@ def test_fused_adjoint_matches_pass_by_pass_adjoint(cuda, case, monkeypatch):
     torch.cuda.synchronize()
     g1, g2 = gx1.cpu().numpy(), gx2.cpu().numpy()
     assert np.abs(g1 - g2).max() <= 1e-5 * np.abs(g2).max()
-    assert np.array_equal(gx_only.cpu().numpy(), g1)
+    assert np.abs(gx_only.cpu().numpy() - g1).max() <= 1e-6 * np.abs(g1).max()
     s1, s2 = gs1.cpu().numpy(), gs2.cpu().numpy()
     assert np.allclose(s1, s2, rtol=1e-4, atol=1e-4 * np.abs(s2).max()), (s1, s2)
     assert np.allclose(gs_only.cpu().numpy(), s1, rtol=1e-6, atol=1e-9)
