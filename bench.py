@@ -311,7 +311,7 @@ def run_gpu_arm(args):
         "config": dict(CONFIG, parallelism=f"replicas x{world}" if world > 1 else "single GPU"),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic_from_profiles(), "peak_source": peak_kind,
-                     "kernel": "fused3d_tma_kernel (TMA-pipelined z-marching tile kernel)", "bytes_per_voxel": BYTES_PER_VOXEL,
+                     "kernel": "fused3d_ws_kernel (warp-specialised z-marching tile kernel)", "bytes_per_voxel": BYTES_PER_VOXEL,
                      "avg_kernel_ms": avg_kernel_ms},
         "e2e": {"value": e2e_value, "unit": "Gvox/s", "h2d_bytes_per_step": int(h_in.numel() * 2),
                 "d2h_bytes_per_step": int(sum(h.numel() * 4 for h in h_out)), "ms_per_step": e2e_ms},
@@ -452,7 +452,7 @@ def run_gauss2d(args):
     line = _base_line(args, world, value, total / args.steps, G2_CONFIG)
     ach = 8 * npx / (avg * 1e-3) / 1e9
     line["roofline"] = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
-                        "traffic": None, "peak_source": kind, "kernel": "fused2d_kernel", "bytes_per_voxel": 8,
+                        "traffic": None, "peak_source": kind, "kernel": "fused2d_ws_kernel (warp per tile)", "bytes_per_voxel": 8,
                         "avg_kernel_ms": avg}
     line["clocks"] = clk
     line["gpu_launches"] = args.steps
