@@ -19,9 +19,9 @@
 // is written once.  Many loaders per CTA and 2-plane boxes keep enough TMA traffic in flight: a
 // single loader thread issuing 1-plane boxes was limited to about one box per 150 ns per CTA.
 //
-// Tile geometry: the TMA box starts at a 16-byte boundary, which fixes the tile origin offset
-// OFF and rounds TX to the TMA granule; E = HX % 2 adds one leading box column for odd HX, so
-// that the y pass works on aligned column pairs.
+// Tile geometry: the TMA box starts LEAD >= HX columns before the tile, LEAD a multiple of the
+// TMA granule (16 bytes), so tiles start at multiples of TX and output rows are sector-aligned;
+// the y pass works on aligned column pairs.
 //
 // Boundary conditions: z uses the mapped plane index as the TMA coordinate (an out-of-range
 // coordinate gives TMA zero fill for "add zeros"), with the plane negated for the asymmetric
@@ -65,13 +65,15 @@ template< typename TIn, int HX, int HY, int HZ >
 struct W5Geom {
    static constexpr int A = 16 / static_cast< int >( sizeof( TIn ));  // TMA x granule (samples)
    static constexpr int E = HX % 2;
-   static constexpr int OFF = ( A - ( HX + E ) % A ) % A;              // tile origin offset (even)
-   static constexpr int PPL = ( E + 2 * HX + 48 <= 64 ) ? 1 : 2;       // y-pass column pairs per lane
+   static constexpr int LEAD = ( HX + E + A - 1 ) / A * A;             // box columns before the tile (TMA granule)
+   static constexpr int OFF = 0;                                       // tiles start at multiples of TX
+   static constexpr int PPL = ( LEAD + HX + 48 <= 64 ) ? 1 : 2;        // y-pass column pairs per lane
    static constexpr int BW = 64 * PPL;                                 // box width
-   static constexpr int TX = ( BW - E - 2 * HX ) / A * A;              // outputs per tile row
+   static constexpr int TX = ( BW - LEAD - HX ) / A * A;               // outputs per tile row
    static constexpr int TY = 8;
    static constexpr int BH = TY + 2 * HY;                              // box height
-   static constexpr int NPAIR = ( E + TX + 2 * HX + 1 ) / 2;          // y-pass column pairs
+   static constexpr int P0 = ( LEAD - HX ) / 2;                        // first y-pass column pair
+   static constexpr int NPAIR = ( LEAD + TX + HX - 1 ) / 2 - P0 + 1;   // y-pass column pairs
    static constexpr int XQ = HX + 1 + E;                               // float4 reads per x-pass point group
    static constexpr int XITEMS = ( TX / 2 ) * ( TY / 2 );
    static constexpr int ZITEMS = ( TX / 2 ) * TY;
@@ -88,7 +90,7 @@ struct W5Geom {
    static constexpr int STAGE_STRIDE = ( STAGE_BYTES + 127 ) / 128 * 128;
    static constexpr int B2_BYTES = ( BW / 2 ) * ( TY / 2 ) * 16;      // per in-plane warp
    static constexpr int RING_PLANE = TX * TY;                          // floats
-   static constexpr int XFIX_MAX = 2 * ( HX + E + 1 );                 // halo columns patched after the y pass
+   static constexpr int XFIX_MAX = 2 * ( HX + 1 );                     // halo columns patched after the y pass
    static constexpr int FIXED = NWI * B2_BYTES + NS * RING_PLANE * 4 + 512;
    static constexpr int BUDGET = FIXED <= 80 * 1024 ? 110 * 1024 : 225 * 1024;
    // Stages per in-plane warp (each warp streams its own plane pairs).
@@ -100,7 +102,8 @@ struct W5Geom {
    static constexpr int OFF_BAR = ( OFF_TAB + BH * 8 + XFIX_MAX * 4 + 16 + 15 ) / 16 * 16;
    static constexpr int BYTES = OFF_BAR + D * 8 + 16;
    static_assert( TX >= 8 && TX % 2 == 0 && TX % A == 0, "tile width" );
-   static_assert( E + TX + 2 * HX <= BW && TX + 2 * HX + 2 * E <= BW, "box width" );
+   static_assert( LEAD >= HX && LEAD + TX + HX <= BW && 2 * ( P0 + NPAIR ) <= BW, "box width" );
+   static_assert(( LEAD + TX - 2 - HX ) / 2 + XQ <= P0 + NPAIR, "x pass reads only y-pass columns" );
    static_assert( NPAIR <= 32 * PPL, "y-pass pairs per lane" );
    static_assert( RZ >= 2 && RZ % 2 == 0 && NS >= 2 * RZ + 2 * HZ, "z ring" );
    static_assert( NT <= 1024, "block size" );
@@ -222,8 +225,8 @@ __global__ void __launch_bounds__( W5Geom< TIn, HX, HY, HZ >::NT, W5Geom< TIn, H
       int64_t const tr = tc / a.tiles_x;
       int const tyi = static_cast< int >( tr % a.tiles_y );
       int const b = static_cast< int >( tr / a.tiles_y );
-      int const x0 = txi * TX - G::OFF, y0 = tyi * TY;
-      int const bx = x0 - HX - E, by = y0 - HY;
+      int const x0 = txi * TX, y0 = tyi * TY;
+      int const bx = x0 - G::LEAD, by = y0 - HY;
       int const nout_total = ze - zs;
       int const nplanes = nout_total + 2 * HZ;
       int const npairs = ( nplanes + 1 ) / 2;
@@ -263,17 +266,17 @@ __global__ void __launch_bounds__( W5Geom< TIn, HX, HY, HZ >::NT, W5Geom< TIn, H
       }
       if( xedge && warp == NWC - 1 ) {
          // One warp: each lane tests one used box column; ballot-compacted list.
-         constexpr int UC = E + TX + 2 * HX;
+         constexpr int C_LO = G::LEAD - HX, C_HI = G::LEAD + TX + HX;
          int n = 0;
-         for( int c0 = 0; c0 < UC; c0 += 32 ) {
-            int const c = c0 + lane;
+         for( int cc = C_LO; cc < C_HI; cc += 32 ) {
+            int const c = cc + lane;
             int const xx = bx + c;
             uint32_t ent = 0;
-            bool want = c < UC && !( xx >= 0 && xx < nx ) && xx >= -HX && xx < nx + HX && a.bc[ 0 ] != BC_ADD_ZEROS;
+            bool want = c < C_HI && !( xx >= 0 && xx < nx ) && xx >= -HX && xx < nx + HX && a.bc[ 0 ] != BC_ADD_ZEROS;
             if( want ) {
                bool neg;
                int const sc = static_cast< int >( bc_map_index( xx, nx, a.bc[ 0 ], &neg )) - bx;
-               want = sc >= 0 && sc < UC;
+               want = sc >= C_LO && sc < C_HI;
                ent = static_cast< uint32_t >( c ) | ( static_cast< uint32_t >( sc < 0 ? 0 : sc ) << 8 ) | ( neg ? 1u << 16 : 0u );
             }
             uint32_t const m = __ballot_sync( 0xffffffffu, want );
@@ -306,8 +309,8 @@ __global__ void __launch_bounds__( W5Geom< TIn, HX, HY, HZ >::NT, W5Geom< TIn, H
                   // y pass: lane -> column pair(s), all TY rows
 #pragma unroll
                   for( int pp = 0; pp < G::PPL; ++pp ) {
-                     int const p = lane + 32 * pp;
-                     if( p < G::NPAIR ) {
+                     int const p = G::P0 + lane + 32 * pp;
+                     if( lane + 32 * pp < G::NPAIR ) {
                         float2 v[ BH ];
                         if( !yedge ) {
 #pragma unroll
@@ -369,7 +372,7 @@ __global__ void __launch_bounds__( W5Geom< TIn, HX, HY, HZ >::NT, W5Geom< TIn, H
 #pragma unroll
                   for( int it = lane; it < G::XITEMS; it += 32 ) {
                      int const cp = it % ( TX / 2 ), rp = it / ( TX / 2 );
-                     float4 const* row = b2 + rp * ( BW / 2 ) + cp;
+                     float4 const* row = b2 + rp * ( BW / 2 ) + (( G::LEAD + 2 * cp - HX ) >> 1 );
                      float2 vx[ 2 * XQ ];
 #pragma unroll
                      for( int m = 0; m < XQ; ++m ) {
