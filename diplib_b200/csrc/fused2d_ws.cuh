@@ -7,7 +7,8 @@
 // tile, warp-locally: the y pass (one column pair per lane, row blocks of RB outputs, packed f32x2
 // arithmetic; y-edge tiles read through a row map) into the warp's buffer, the x-edge fix of the
 // halo columns, and the x pass (a sliding register window over a strip of columns per lane) into
-// a staging tile that the warp then stores row by row, coalesced.
+// a staging tile that one TMA store writes out (row-by-row coalesced stores where the destination
+// layout does not allow TMA).
 // No block barrier at all; each input pixel crosses HBM once and each output pixel is written
 // once.
 //
@@ -32,6 +33,8 @@ namespace dipcu {
 
 struct W2Args {
    CUtensorMap tmap;        // 4D (x, y, 1, batch) tiled map of the source
+   CUtensorMap tout;        // the same for the destination, box = one tile (TMA stores)
+   int32_t tma_store;       // destination layout allows TMA stores
    float* dst;
    int32_t n[ 2 ];
    int32_t nb;
@@ -46,7 +49,7 @@ struct W2Args {
    float2 w[ 2 ][ kFusedMaxTaps ];  // per axis (x, y), centre first, zero beyond h
 };
 
-template< typename TIn, int B >
+template< typename TIn, int B, int TYP = 16 >
 struct W2Geom {
    static constexpr int A = 16 / static_cast< int >( sizeof( TIn ));  // TMA x granule (samples)
    static constexpr int E = B % 2;
@@ -54,42 +57,49 @@ struct W2Geom {
    static constexpr int OFF = 0;                                       // tiles start at multiples of TX
    static constexpr int BW = 64;                                       // box width: one column pair per lane
    static constexpr int TX = ( BW - LEAD - B ) / 8 * 8;                // outputs per tile row (4 strips of SW)
-   static constexpr int TY = 16;
+   static constexpr int TY = TYP;                                      // rows per tile (16 or 32)
    static constexpr int RB = B >= 9 ? 16 : 8;                          // y-pass rows per register block
    static constexpr int BH = TY + 2 * B;                               // box height
    static constexpr int P0 = ( LEAD - B ) / 2;                         // first y-pass column pair
    static constexpr int NPAIR = ( LEAD + TX + B - 1 ) / 2 - P0 + 1;    // y-pass column pairs (one per lane)
    static constexpr int SW = TX / 4;                                   // x-pass strip width (one lane: row pair x strip)
    static constexpr int NPX = SW / 2 + B + E;                          // column pairs a strip reads
-   static constexpr int OTS = TX + 4;                                  // row stride of the output staging tile
-   static constexpr int NW = 4;                                        // warps per CTA
-   static constexpr int NT = NW * 32;
+   static constexpr int OTS = TX;                                      // row stride of the output staging tile (dense: TMA store)
    static constexpr int STAGE_BYTES = BW * BH * static_cast< int >( sizeof( TIn ));
    static constexpr int STAGE_STRIDE = ( STAGE_BYTES + 127 ) / 128 * 128;
    static constexpr int B2_BYTES = ( BW / 2 ) * ( TY / 2 ) * 16;
    static constexpr int XFIX_MAX = 2 * ( B + 1 );
    static constexpr int TAB_BYTES = ( BH * 8 + XFIX_MAX * 4 + 16 + 15 ) / 16 * 16;   // per warp
-   static constexpr int OT_BYTES = TY * OTS * 4;                       // per warp
+   static constexpr int OT_BYTES = ( TY * OTS * 4 + 127 ) / 128 * 128; // per warp
    static constexpr int PER_WARP = B2_BYTES + TAB_BYTES + OT_BYTES;
-   static constexpr int SPW = NW * ( 3 * STAGE_STRIDE + PER_WARP ) + 256 <= 112 * 1024 ? 3 : 2;   // stages per warp
-   static constexpr int OFF_B2 = NW * SPW * STAGE_STRIDE;
+   // Warps per CTA and stages per warp: two CTAs per SM, as many warps as fit with 2 stages each
+   // (3 when there is room), else 4 warps of 1 stage.
+   static constexpr int FIT4_3 = 4 * ( 3 * STAGE_STRIDE + PER_WARP ) + 512 <= 112 * 1024;
+   static constexpr int FIT4_2 = 4 * ( 2 * STAGE_STRIDE + PER_WARP ) + 512 <= 112 * 1024;
+   static constexpr int FIT3_2 = 3 * ( 2 * STAGE_STRIDE + PER_WARP ) + 512 <= 112 * 1024;
+   static constexpr int NW = ( FIT4_3 || FIT4_2 ) ? 4 : ( FIT3_2 ? 3 : 4 );
+   static constexpr int SPW = FIT4_3 ? 3 : (( FIT4_2 || FIT3_2 ) ? 2 : 1 );
+   static constexpr int NT = NW * 32;
+   static constexpr int OFF_OT = 0;                                    // 128-byte aligned staging tiles first
+   static constexpr int OFF_STAGE = NW * OT_BYTES;
+   static constexpr int OFF_B2 = OFF_STAGE + NW * SPW * STAGE_STRIDE;
    static constexpr int OFF_TAB = OFF_B2 + NW * B2_BYTES;
-   static constexpr int OFF_OT = OFF_TAB + NW * TAB_BYTES;
-   static constexpr int OFF_BAR = OFF_OT + NW * OT_BYTES;
+   static constexpr int OFF_BAR = OFF_TAB + NW * TAB_BYTES;
    static constexpr int BYTES = OFF_BAR + NW * SPW * 8 + 16;
    static_assert( TX >= 8 && TX % 8 == 0 && TX % A == 0 && SW % 2 == 0, "tile width" );
-   static_assert( TY == 16, "x-pass lanes: 8 row pairs x 4 strips" );
+   static_assert( TY % 16 == 0, "x-pass lanes: 8 row pairs x 4 strips per group of 16 rows" );
    static_assert(( LEAD + 3 * SW - B ) / 2 + NPX <= P0 + NPAIR, "x-pass reads only y-pass columns" );
    static_assert( LEAD >= B && LEAD + TX + B <= BW && 2 * ( P0 + NPAIR ) <= BW, "box width" );
    static_assert( NPAIR <= 32, "one column pair per lane" );
    static_assert( TY % RB == 0 && RB % 2 == 0, "row blocks" );
-   static_assert( STAGE_BYTES % 128 == 0, "TMA destinations 128-byte aligned" );
+   static_assert( STAGE_BYTES % 128 == 0 && OFF_STAGE % 128 == 0 && STAGE_STRIDE % 128 == 0, "TMA destinations 128-byte aligned" );
+   static_assert(( TX * 4 ) % 16 == 0, "TMA store rows of 16-byte multiples" );
    static constexpr bool fits = BYTES <= 113 * 1024;
 };
 
-template< typename TIn, int B >
-__global__ void __launch_bounds__( W2Geom< TIn, B >::NT, 2 ) fused2d_ws_kernel( W2Args const __grid_constant__ a ) {
-   using G = W2Geom< TIn, B >;
+template< typename TIn, int B, int TYP >
+__global__ void __launch_bounds__( W2Geom< TIn, B, TYP >::NT, 2 ) fused2d_ws_kernel( W2Args const __grid_constant__ a ) {
+   using G = W2Geom< TIn, B, TYP >;
    constexpr int TX = G::TX, TY = G::TY, BW = G::BW, BH = G::BH, SPW = G::SPW, RB = G::RB, E = G::E;
    constexpr int NW = G::NW;
    constexpr bool kFloat = std::is_same< TIn, float >::value;
@@ -98,13 +108,13 @@ __global__ void __launch_bounds__( W2Geom< TIn, B >::NT, 2 ) fused2d_ws_kernel( 
    int const warp = tid >> 5, lane = tid & 31;
    uint64_t* const full = reinterpret_cast< uint64_t* >( smem + G::OFF_BAR ) + warp * SPW;
    int volatile* abort = reinterpret_cast< int* >( smem + G::OFF_BAR + NW * SPW * 8 );
-   unsigned char* const stages = smem + warp * SPW * G::STAGE_STRIDE;
+   unsigned char* const stages = smem + G::OFF_STAGE + warp * SPW * G::STAGE_STRIDE;
    float4* const b2 = reinterpret_cast< float4* >( smem + G::OFF_B2 + warp * G::B2_BYTES );   // [TY/2][BW/2]
    unsigned char* const tab = smem + G::OFF_TAB + warp * G::TAB_BYTES;
    int32_t* const rmap = reinterpret_cast< int32_t* >( tab );                    // [BH]
    float* const rsgn = reinterpret_cast< float* >( rmap + BH );                   // [BH]
    uint32_t* const xfix = reinterpret_cast< uint32_t* >( rsgn + BH );            // [XFIX_MAX]
-   float* const ot = reinterpret_cast< float* >( smem + G::OFF_OT + warp * G::OT_BYTES );   // [TY][OTS]
+   float* const ot = reinterpret_cast< float* >( smem + G::OFF_OT + warp * G::OT_BYTES );   // [TY][TX]
 
    if( tid == 0 ) { *abort = 0; }
    if( lane == 0 ) {
@@ -240,8 +250,14 @@ __global__ void __launch_bounds__( W2Geom< TIn, B >::NT, 2 ) fused2d_ws_kernel( 
       }
       // x pass: lane -> (row pair, strip of SW columns); a sliding register window over the
       // strip's NPX column pairs, SW independent accumulators, results staged in `ot`.
-      {
-         int const rp = lane >> 2, c0 = ( lane & 3 ) * G::SW;
+      if( a.tma_store ) {
+         // The previous tile's TMA store has finished reading `ot`.
+         if( lane == 0 ) { asm volatile( "cp.async.bulk.wait_group.read 0;" ::: "memory" ); }
+         __syncwarp();
+      }
+#pragma unroll 1
+      for( int grp = 0; grp < TY / 16; ++grp ) {
+         int const rp = ( lane >> 2 ) + 8 * grp, c0 = ( lane & 3 ) * G::SW;
          float4 const* row = b2 + rp * ( BW / 2 ) + (( G::LEAD + c0 - B ) >> 1 );
          float2 vx[ 2 * G::NPX ];
 #pragma unroll
@@ -268,9 +284,19 @@ __global__ void __launch_bounds__( W2Geom< TIn, B >::NT, 2 ) fused2d_ws_kernel( 
             *reinterpret_cast< float2* >( ot + ( 2 * rp + 1 ) * G::OTS + c0 + c ) = make_float2( out[ c ].y, out[ c + 1 ].y );
          }
       }
-      __syncwarp();
-      // coalesced stores of the staged tile: lanes sweep rows in column pairs
-      {
+      if( a.tma_store ) {
+         // One TMA store of the staged tile (clipped at the image edges by the tensor map).
+         fence_proxy_async();
+         __syncwarp();
+         if( lane == 0 ) {
+            asm volatile( "cp.async.bulk.tensor.4d.global.shared::cta.bulk_group [%0, {%1, %2, %3, %4}], [%5];"
+                          :: "l"( reinterpret_cast< uint64_t >( &a.tout )), "r"( x0 ), "r"( y0 ), "r"( 0 ), "r"( b ),
+                             "r"( smem_u32( ot )) : "memory" );
+            asm volatile( "cp.async.bulk.commit_group;" ::: "memory" );
+         }
+      } else {
+         __syncwarp();
+         // coalesced stores of the staged tile: lanes sweep rows in column pairs
          float* const dst_b = a.dst + static_cast< int64_t >( b ) * a.db;
 #pragma unroll 4
          for( int e = lane; e < TY * ( TX / 2 ); e += 32 ) {
@@ -290,6 +316,7 @@ __global__ void __launch_bounds__( W2Geom< TIn, B >::NT, 2 ) fused2d_ws_kernel( 
       }
       __syncwarp();   // b2 and table reads done before the next tile
    }
+   if( a.tma_store && lane == 0 ) { asm volatile( "cp.async.bulk.wait_group 0;" ::: "memory" ); }
 }
 
 } // namespace dipcu

@@ -264,7 +264,8 @@ cudaError_t run3d_ws( FusedArgs& a, cudaStream_t s ) {
 // cudaErrorNotSupported when its conditions do not hold, so that the caller falls back.
 template< typename TIn, int B >
 cudaError_t run2d_ws( FusedArgs& a, int32_t const* odd, cudaStream_t s ) {
-   using G = W2Geom< TIn, B >;
+   constexpr int TYP = 32;
+   using G = W2Geom< TIn, B, TYP >;
    static_assert( G::fits, "shared memory" );
    constexpr int esz = sizeof( TIn );
    if( a.ss[ 0 ] != 1 || a.ss[ 1 ] <= 0 || ( a.nb > 1 && a.sb <= 0 )) { return cudaErrorNotSupported; }
@@ -289,6 +290,18 @@ cudaError_t run2d_ws( FusedArgs& a, int32_t const* odd, cudaStream_t s ) {
    cuuint32_t box[ 4 ] = { static_cast< cuuint32_t >( G::BW ), static_cast< cuuint32_t >( G::BH ), 1, 1 };
    if( encode_tmap( &z.tmap, dt, a.src, dims, strides, box ) != CUDA_SUCCESS ) { return cudaErrorNotSupported; }
    z.dst = a.dst;
+   // TMA stores of whole tiles when the destination layout allows them.
+   z.tma_store = 0;
+   if( a.ds[ 0 ] == 1 && a.ds[ 1 ] > 0 && ( reinterpret_cast< uintptr_t >( a.dst ) & 15 ) == 0 && ( a.ds[ 1 ] * 4 ) % 16 == 0 &&
+       ( a.nb <= 1 || ( a.db > 0 && ( a.db * 4 ) % 16 == 0 )) && !getenv( "DIPCU_NO_TMA_STORE" )) {
+      cuuint64_t od[ 4 ] = { static_cast< cuuint64_t >( a.n[ 0 ] ), static_cast< cuuint64_t >( a.n[ 1 ] ), 1,
+                             static_cast< cuuint64_t >( a.nb ) };
+      cuuint64_t os[ 3 ] = { static_cast< cuuint64_t >( a.ds[ 1 ] * 4 ), static_cast< cuuint64_t >( a.ds[ 1 ] * a.n[ 1 ] * 4 ),
+                             static_cast< cuuint64_t >(( a.nb > 1 ? a.db : a.ds[ 1 ] * a.n[ 1 ] ) * 4 ) };
+      for( auto& v : os ) { if( v % 16 ) { v = ( v + 15 ) / 16 * 16; } }
+      cuuint32_t ob[ 4 ] = { static_cast< cuuint32_t >( G::TX ), static_cast< cuuint32_t >( G::TY ), 1, 1 };
+      if( encode_tmap( &z.tout, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, a.dst, od, os, ob ) == CUDA_SUCCESS ) { z.tma_store = 1; }
+   }
    for( int i = 0; i < 2; ++i ) {
       z.n[ i ] = static_cast< int32_t >( a.n[ i ] );
       z.ds[ i ] = a.ds[ i ];
@@ -306,7 +319,7 @@ cudaError_t run2d_ws( FusedArgs& a, int32_t const* odd, cudaStream_t s ) {
    z.ntiles = static_cast< int64_t >( z.tiles_x ) * z.tiles_y * a.nb;
    z.status = device_status_ptr();
    if( !z.status ) { return cudaErrorUnknown; }
-   auto kern = fused2d_ws_kernel< TIn, B >;
+   auto kern = fused2d_ws_kernel< TIn, B, TYP >;
    size_t smem = G::BYTES;
    int per_sm = prepare_kernel( kern, G::NT, smem );
    if( per_sm < 1 ) { return cudaErrorInvalidConfiguration; }
