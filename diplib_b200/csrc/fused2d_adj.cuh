@@ -15,7 +15,7 @@
 // from the same loads; y-edge tiles add the y fold (the tile that owns the fold's target row
 // computes the halo value z(j) from its own staged rows); the x pass computes x_bar = C_x^T v,
 // a = C'_x^T v and c = C_x^T v', x-edge tiles add the x fold, and a, c are dotted with x.  x_bar
-// goes out through a staging tile with coalesced stores; the dots are reduced per warp and added
+// goes out through a staging tile (one TMA store, or coalesced stores); the dots are reduced per warp and added
 // to the two sigma gradients (double) once per warp.  One kernel reads y_bar and x once and writes
 // x_bar once.
 //
@@ -34,6 +34,8 @@ namespace dipcu {
 struct A2Args {
    CUtensorMap tg;          // y_bar: 4D (x, y, 1, batch) float map, box (64, BH)
    CUtensorMap tx;          // x: the same layout in the input type, box (TX, 16)
+   CUtensorMap tgx;         // x_bar, box = one tile (TMA stores)
+   int32_t tma_store;       // x_bar layout allows TMA stores
    float* gx;               // x_bar (nullptr: not wanted)
    double* dsig[ 2 ];       // dL/dsigma_x, dL/dsigma_y accumulators (nullptr: not wanted)
    int32_t n[ 2 ];
@@ -66,12 +68,13 @@ struct A2Geom {
    static constexpr int SPW = 2;
    static constexpr int NW = ( 110 * 1024 ) / ( SPW * STAGE_STRIDE + PER_WARP ) >= 4 ? 4 : 3;
    static constexpr int NT = NW * 32;
-   static constexpr int OFF_B2 = NW * SPW * STAGE_STRIDE;
+   static constexpr int OFF_OT = 0;                                    // 128-byte aligned staging tiles first
+   static constexpr int OFF_STAGE = NW * OT_BYTES;
+   static constexpr int OFF_B2 = OFF_STAGE + NW * SPW * STAGE_STRIDE;
    static constexpr int OFF_TAB = OFF_B2 + NW * 2 * B2_BYTES;
-   static constexpr int OFF_OT = OFF_TAB + NW * TAB_BYTES;
-   static constexpr int OFF_BAR = OFF_OT + NW * OT_BYTES;
+   static constexpr int OFF_BAR = OFF_TAB + NW * TAB_BYTES;
    static constexpr int BYTES = OFF_BAR + NW * SPW * 8 + 16;
-   static_assert( GBYTES % 128 == 0 && ( XBYTES % 16 ) == 0, "TMA destinations" );
+   static_assert( GBYTES % 128 == 0 && ( XBYTES % 16 ) == 0 && OT_BYTES % 128 == 0, "TMA destinations and sources" );
    static_assert(( TX * static_cast< int >( sizeof( TIn ))) % 16 == 0, "x box rows of 16-byte multiples" );
    static constexpr bool fits = BYTES <= 113 * 1024;
 };
@@ -91,7 +94,7 @@ __global__ void __launch_bounds__( A2Geom< TIn, B >::NT, 2 ) fused2d_adj_kernel(
    int const warp = tid >> 5, lane = tid & 31;
    uint64_t* const full = reinterpret_cast< uint64_t* >( smem + G::OFF_BAR ) + warp * SPW;
    int volatile* abort = reinterpret_cast< int* >( smem + G::OFF_BAR + NW * SPW * 8 );
-   unsigned char* const stages = smem + warp * SPW * G::STAGE_STRIDE;
+   unsigned char* const stages = smem + G::OFF_STAGE + warp * SPW * G::STAGE_STRIDE;
    float4* const b2 = reinterpret_cast< float4* >( smem + G::OFF_B2 + warp * 2 * G::B2_BYTES );    // v
    float4* const b2d = reinterpret_cast< float4* >( smem + G::OFF_B2 + warp * 2 * G::B2_BYTES + G::B2_BYTES );   // v'
    uint32_t* const yfold = reinterpret_cast< uint32_t* >( smem + G::OFF_TAB + warp * G::TAB_BYTES );   // tr | jb << 8 | neg << 16
@@ -247,6 +250,11 @@ __global__ void __launch_bounds__( A2Geom< TIn, B >::NT, 2 ) fused2d_adj_kernel(
       }
       __syncwarp();
 
+      if( want_gx && a.tma_store ) {
+         // The previous tile's TMA store has finished reading `ot`.
+         if( lane == 0 ) { asm volatile( "cp.async.bulk.wait_group.read 0;" ::: "memory" ); }
+         __syncwarp();
+      }
       // ---- x pass: lane -> (row pair, strip of SW columns)
       int const rp = lane >> 2, c0 = ( lane & 3 ) * SW;
       constexpr int C0 = B + E;
@@ -348,7 +356,16 @@ __global__ void __launch_bounds__( A2Geom< TIn, B >::NT, 2 ) fused2d_adj_kernel(
          int64_t const tn = t + SPW * nwarps;
          if( tn < a.ntiles ) { issue( tn, st ); }
       }
-      if( want_gx ) {
+      if( want_gx && a.tma_store ) {
+         fence_proxy_async();
+         __syncwarp();
+         if( lane == 0 ) {
+            asm volatile( "cp.async.bulk.tensor.4d.global.shared::cta.bulk_group [%0, {%1, %2, %3, %4}], [%5];"
+                          :: "l"( reinterpret_cast< uint64_t >( &a.tgx )), "r"( x0 ), "r"( y0 ), "r"( 0 ), "r"( b ),
+                             "r"( smem_u32( ot )) : "memory" );
+            asm volatile( "cp.async.bulk.commit_group;" ::: "memory" );
+         }
+      } else if( want_gx ) {
          float* const dst_b = a.gx + static_cast< int64_t >( b ) * a.gb;
 #pragma unroll 4
          for( int e = lane; e < TY * ( TX / 2 ); e += 32 ) {
@@ -368,6 +385,7 @@ __global__ void __launch_bounds__( A2Geom< TIn, B >::NT, 2 ) fused2d_adj_kernel(
       }
       __syncwarp();   // ot reads done before the next tile
    }
+   if( want_gx && a.tma_store && lane == 0 ) { asm volatile( "cp.async.bulk.wait_group 0;" ::: "memory" ); }
    if( want_sig ) {
       double dx = dsx, dy = dsy;
 #pragma unroll

@@ -372,6 +372,17 @@ cudaError_t run_adj2d( Adj2Params const& p, cudaStream_t s ) {
       if( encode_tmap( &z.tx, dt, p.x, dims, st, box ) != CUDA_SUCCESS ) { return cudaErrorNotSupported; }
    }
    z.gx = p.gx;
+   z.tma_store = 0;
+   if( p.gx && p.gxs1 > 0 && ( reinterpret_cast< uintptr_t >( p.gx ) & 15 ) == 0 && ( p.gxs1 * 4 ) % 16 == 0 &&
+       ( p.nb <= 1 || ( p.gxb > 0 && ( p.gxb * 4 ) % 16 == 0 )) && !getenv( "DIPCU_NO_TMA_STORE" )) {
+      cuuint64_t od[ 4 ] = { static_cast< cuuint64_t >( p.n[ 0 ] ), static_cast< cuuint64_t >( p.n[ 1 ] ), 1,
+                             static_cast< cuuint64_t >( p.nb ) };
+      cuuint64_t os[ 3 ] = { static_cast< cuuint64_t >( p.gxs1 * 4 ), static_cast< cuuint64_t >( p.gxs1 * p.n[ 1 ] * 4 ),
+                             static_cast< cuuint64_t >(( p.nb > 1 ? p.gxb : p.gxs1 * p.n[ 1 ] ) * 4 ) };
+      for( auto& v : os ) { if( v % 16 ) { v = ( v + 15 ) / 16 * 16; } }
+      cuuint32_t ob[ 4 ] = { static_cast< cuuint32_t >( G::TX ), static_cast< cuuint32_t >( G::TY ), 1, 1 };
+      if( encode_tmap( &z.tgx, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, p.gx, od, os, ob ) == CUDA_SUCCESS ) { z.tma_store = 1; }
+   }
    z.dsig[ 0 ] = sig ? p.dsig[ 0 ] : nullptr;
    z.dsig[ 1 ] = sig ? p.dsig[ 1 ] : nullptr;
    z.nb = static_cast< int32_t >( p.nb );
