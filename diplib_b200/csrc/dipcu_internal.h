@@ -1,6 +1,7 @@
 // Internal interfaces between the C-ABI layer (api.cpp) and the kernel launchers.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -61,6 +62,11 @@ struct FusedArgs {
    int32_t tiles_x, tiles_y, zchunks, lz;
    float w[ 3 ][ kFusedMaxTaps ];  // per axis, centre tap first
 };
+
+// 4D tiled TMA map (no swizzle, no interleave, zero fill) of a device buffer; cached per
+// (pointer, layout, box).
+CUresult encode_source_map( CUtensorMap* out, CUtensorMapDataType dt, void const* ptr, cuuint64_t const* dims,
+                            cuuint64_t const* strides, cuuint32_t const* box );
 
 struct FusedKey {
    int32_t ndims;          // 2 or 3

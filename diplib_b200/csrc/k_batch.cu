@@ -28,6 +28,7 @@
 #include "dipcu_common.cuh"
 #include "dipcu_internal.h"
 #include "fused.cuh"
+#include "fused2d_ws.cuh"
 
 namespace dipcu {
 
@@ -227,6 +228,344 @@ __global__ void __launch_bounds__( 256 ) batch_kernel( BatchArgs const __grid_co
    }
 }
 
+// ---- grouped warp-per-tile path: images with half-widths up to 12 and x-y boundary conditions
+// the 2D tile kernel takes (fused2d_ws.cuh) run through a variant of that kernel with per-image
+// tables: a TMA map per image in device memory and a work list of (image, tile) items, dealt
+// round-robin over the warps of a persistent grid.  Taps come from the plan's weight bank per
+// tile (zero beyond each axis' half-width), so a sigma-table update replays correctly.
+
+struct alignas( 128 ) G2Image {
+   CUtensorMap tmap;        // 4D (x, y, 1, 1) tiled map of the source, box = tile + halo
+   float* dst;
+   int64_t ds1;             // destination row stride (x stride 1)
+   int32_t n[ 2 ];
+   int32_t bc[ 2 ];
+   int32_t h[ 2 ];
+   int32_t wofs[ 2 ];       // weight-bank offsets of the x and y kernels
+   int32_t odd[ 2 ];
+   int32_t tiles_x, tiles_y;
+   int32_t vec_store;       // float2 stores are 8-byte aligned
+};
+
+struct G2Args {
+   G2Image const* images;
+   BatchItem const* items;
+   float const* wbank;
+   int32_t* status;
+   int32_t nimages;
+   int32_t nitems;
+};
+
+constexpr int kG2Buckets[ 4 ] = { 4, 6, 9, 12 };
+
+template< int B >
+struct G2Geom {
+   using G = W2Geom< float, B, 32 >;
+   static constexpr int WT = 2 * ( B + 1 );                            // taps per warp: x then y, float2
+   static constexpr int OFF_WT = ( G::BYTES + 15 ) / 16 * 16;
+   static constexpr int BYTES = OFF_WT + G::NW * WT * 8;
+   static_assert( WT <= 32, "one tap per lane" );
+   static_assert( BYTES <= 113 * 1024, "two CTAs per SM" );
+};
+
+template< int B >
+__global__ void __launch_bounds__( W2Geom< float, B, 32 >::NT, 2 ) batch_ws_kernel( G2Args const __grid_constant__ a ) {
+   using G = W2Geom< float, B, 32 >;
+   using GG = G2Geom< B >;
+   constexpr int TX = G::TX, TY = G::TY, BW = G::BW, BH = G::BH, SPW = G::SPW, RB = G::RB, E = G::E;
+   constexpr int NW = G::NW;
+   extern __shared__ __align__( 128 ) unsigned char smem[];
+   int const tid = static_cast< int >( threadIdx.x );
+   int const warp = tid >> 5, lane = tid & 31;
+   uint64_t* const full = reinterpret_cast< uint64_t* >( smem + G::OFF_BAR ) + warp * SPW;
+   int volatile* abort = reinterpret_cast< int* >( smem + G::OFF_BAR + NW * SPW * 8 );
+   unsigned char* const stages = smem + G::OFF_STAGE + warp * SPW * G::STAGE_STRIDE;
+   float4* const b2 = reinterpret_cast< float4* >( smem + G::OFF_B2 + warp * G::B2_BYTES );   // [TY/2][BW/2]
+   unsigned char* const tab = smem + G::OFF_TAB + warp * G::TAB_BYTES;
+   int32_t* const rmap = reinterpret_cast< int32_t* >( tab );                    // [BH]
+   float* const rsgn = reinterpret_cast< float* >( rmap + BH );                   // [BH]
+   uint32_t* const xfix = reinterpret_cast< uint32_t* >( rsgn + BH );            // [XFIX_MAX]
+   float* const ot = reinterpret_cast< float* >( smem + G::OFF_OT + warp * G::OT_BYTES );   // [TY][TX]
+   float2* const wt = reinterpret_cast< float2* >( smem + GG::OFF_WT ) + warp * GG::WT;    // x taps, then y taps
+   float2 const* const wtx = wt;
+   float2 const* const wty = wt + ( B + 1 );
+
+   if( tid == 0 ) { *abort = 0; }
+   if( lane == 0 ) {
+      for( int d = 0; d < SPW; ++d ) { mbar_init( &full[ d ], 1 ); }
+      fence_mbar_init();
+   }
+   __syncthreads();
+
+   int64_t const gw = static_cast< int64_t >( blockIdx.x ) * NW + warp;
+   int64_t const nwarps = static_cast< int64_t >( gridDim.x ) * NW;
+   // Item t's image and tile, or false for an item that names no image or tile (skipped and
+   // reported; its stage phase is completed without a copy so the stage sequence stays aligned).
+   auto lookup = [ & ]( int64_t t, G2Image const*& im, int& x0, int& y0 ) -> bool {
+      BatchItem const it = a.items[ t ];
+      if( it.image < 0 || it.image >= a.nimages ) { return false; }
+      im = a.images + it.image;
+      if( it.tile < 0 || it.tile >= im->tiles_x * im->tiles_y ) { return false; }
+      x0 = ( it.tile % im->tiles_x ) * TX;
+      y0 = ( it.tile / im->tiles_x ) * TY;
+      return true;
+   };
+   auto issue = [ & ]( int64_t t, int st ) {
+      G2Image const* im;
+      int x0, y0;
+      if( lookup( t, im, x0, y0 )) {
+         mbar_arrive_expect_tx( &full[ st ], G::STAGE_BYTES );
+         tma_load_4d( stages + st * G::STAGE_STRIDE, &im->tmap, &full[ st ], x0 - G::LEAD, y0 - B, 0, 0 );
+      } else {
+         mbar_arrive( &full[ st ] );
+      }
+   };
+   if( lane == 0 ) {
+      for( int k = 0; k < SPW; ++k ) {
+         int64_t const t = gw + k * nwarps;
+         if( t < a.nitems ) { issue( t, k ); }
+      }
+   }
+   uint32_t kdone = 0;
+   for( int64_t t = gw; t < a.nitems; t += nwarps, ++kdone ) {
+      int const st = static_cast< int >( kdone % SPW );
+      unsigned char* const sp = stages + st * G::STAGE_STRIDE;
+      G2Image const* im = nullptr;
+      int x0 = 0, y0 = 0;
+      bool const valid = lookup( t, im, x0, y0 );
+      if( !valid ) {
+         w5_wait( &full[ st ], ( kdone / SPW ) & 1u, abort, a.status );
+         __syncwarp();
+         if( lane == 0 ) {
+            atomicExch( a.status, DIPCU_ERR_INVALID_ARG );
+            int64_t const tn = t + SPW * nwarps;
+            if( tn < a.nitems ) { issue( tn, st ); }
+         }
+         __syncwarp();
+         continue;
+      }
+      int const nx = im->n[ 0 ], ny = im->n[ 1 ];
+      int const bcx = im->bc[ 0 ], bcy = im->bc[ 1 ];
+      int const bx = x0 - G::LEAD, by = y0 - B;
+      bool const yedge = by < 0 || y0 + TY + B > ny;
+      bool const xedge = x0 - B < 0 || x0 + TX + B > nx;
+      // Taps of this image (the previous tile's reads of `wt` are done).
+      if( lane < GG::WT ) {
+         int const ax = lane / ( B + 1 ), k = lane - ax * ( B + 1 );
+         float const w = k <= im->h[ ax ] ? __ldg( a.wbank + im->wofs[ ax ] + k ) : 0.f;
+         wt[ lane ] = make_float2( w, w );
+      }
+      float2 const sx = im->odd[ 0 ] ? make_float2( -1.f, -1.f ) : make_float2( 1.f, 1.f );
+      float2 const sy = im->odd[ 1 ] ? make_float2( -1.f, -1.f ) : make_float2( 1.f, 1.f );
+      // Boundary tables of an edge tile.
+      if( yedge ) {
+         for( int r = lane; r < BH; r += 32 ) {
+            int const yy = by + r;
+            int src = r;
+            float sg = 1.f;
+            if(( yy < 0 || yy >= ny ) && yy >= -B && yy < ny + B && bcy != BC_ADD_ZEROS ) {
+               bool neg;
+               int const si = static_cast< int >( bc_map_index( yy, ny, bcy, &neg )) - by;
+               if( si >= 0 && si < BH ) { src = si; sg = neg ? -1.f : 1.f; }
+            }
+            rmap[ r ] = src;
+            rsgn[ r ] = sg;
+         }
+      }
+      int nfx = 0;
+      if( xedge ) {
+         constexpr int C_LO = G::LEAD - B, C_HI = G::LEAD + TX + B;
+         for( int cc = C_LO; cc < C_HI; cc += 32 ) {
+            int const c = cc + lane;
+            int const xx = bx + c;
+            uint32_t ent = 0;
+            bool want = c < C_HI && !( xx >= 0 && xx < nx ) && xx >= -B && xx < nx + B && bcx != BC_ADD_ZEROS;
+            if( want ) {
+               bool neg;
+               int const sc = static_cast< int >( bc_map_index( xx, nx, bcx, &neg )) - bx;
+               want = sc >= C_LO && sc < C_HI;
+               ent = static_cast< uint32_t >( c ) | ( static_cast< uint32_t >( sc < 0 ? 0 : sc ) << 8 ) | ( neg ? 1u << 16 : 0u );
+            }
+            uint32_t const m = __ballot_sync( 0xffffffffu, want );
+            int const slot = nfx + __popc( m & (( 1u << lane ) - 1u ));
+            if( want && slot < G::XFIX_MAX ) { xfix[ slot ] = ent; }
+            nfx += __popc( m );
+         }
+         nfx = nfx < G::XFIX_MAX ? nfx : G::XFIX_MAX;
+      }
+      __syncwarp();
+      w5_wait( &full[ st ], ( kdone / SPW ) & 1u, abort, a.status );
+      // y pass: lane -> column pair, row blocks of RB outputs
+      if( lane < G::NPAIR ) {
+         int const pc = G::P0 + lane;
+#pragma unroll
+         for( int r0 = 0; r0 < TY; r0 += RB ) {
+            float2 v[ RB + 2 * B ];
+            if( !yedge ) {
+#pragma unroll
+               for( int r = 0; r < RB + 2 * B; ++r ) { v[ r ] = w5_pair< float, BW >( sp, r0 + r, pc ); }
+            } else {
+#pragma unroll
+               for( int r = 0; r < RB + 2 * B; ++r ) {
+                  v[ r ] = w5_pair< float, BW >( sp, rmap[ r0 + r ], pc );
+                  v[ r ] = fmul2( make_float2( rsgn[ r0 + r ], rsgn[ r0 + r ] ), v[ r ] );
+               }
+            }
+            float2 o[ RB ];
+#pragma unroll
+            for( int t2 = 0; t2 < RB; ++t2 ) {
+               float2 acc = fmul2( wty[ 0 ], v[ t2 + B ] );
+#pragma unroll
+               for( int k = 1; k <= B; ++k ) {
+                  float2 const ps = ffma2( sy, v[ t2 + B - k ], v[ t2 + B + k ] );
+                  acc = ffma2( wty[ k ], ps, acc );
+               }
+               o[ t2 ] = acc;
+            }
+#pragma unroll
+            for( int rp = 0; rp < RB / 2; ++rp ) {
+               b2[ ( r0 / 2 + rp ) * ( BW / 2 ) + pc ] =
+                     make_float4( o[ 2 * rp ].x, o[ 2 * rp + 1 ].x, o[ 2 * rp ].y, o[ 2 * rp + 1 ].y );
+            }
+         }
+      }
+      __syncwarp();
+      if( lane == 0 ) {
+         // The stage is read: stream this warp's item SPW ahead into it.
+         int64_t const tn = t + SPW * nwarps;
+         if( tn < a.nitems ) { issue( tn, st ); }
+      }
+      if( nfx > 0 ) {
+         float2* const b2f = reinterpret_cast< float2* >( b2 );
+         for( int f = lane; f < nfx * ( TY / 2 ); f += 32 ) {
+            uint32_t const fe = xfix[ f / ( TY / 2 ) ];
+            int const rp = f % ( TY / 2 );
+            int const dc = static_cast< int >( fe & 0xffu ), sc = static_cast< int >(( fe >> 8 ) & 0xffu );
+            float2 val = b2f[ ( rp * ( BW / 2 ) + ( sc >> 1 )) * 2 + ( sc & 1 ) ];
+            if( fe & ( 1u << 16 )) { val = make_float2( -val.x, -val.y ); }
+            b2f[ ( rp * ( BW / 2 ) + ( dc >> 1 )) * 2 + ( dc & 1 ) ] = val;
+         }
+         __syncwarp();
+      }
+      // x pass: lane -> (row pair, strip of SW columns), results staged in `ot`
+#pragma unroll 1
+      for( int grp = 0; grp < TY / 16; ++grp ) {
+         int const rp = ( lane >> 2 ) + 8 * grp, c0 = ( lane & 3 ) * G::SW;
+         float4 const* row = b2 + rp * ( BW / 2 ) + (( G::LEAD + c0 - B ) >> 1 );
+         float2 vx[ 2 * G::NPX ];
+#pragma unroll
+         for( int m = 0; m < G::NPX; ++m ) {
+            float4 const f = row[ m ];
+            vx[ 2 * m ] = make_float2( f.x, f.y );
+            vx[ 2 * m + 1 ] = make_float2( f.z, f.w );
+         }
+         float2 out[ G::SW ];
+#pragma unroll
+         for( int c = 0; c < G::SW; ++c ) {
+            constexpr int C0 = B + E;
+            float2 acc = fmul2( wtx[ 0 ], vx[ C0 + c ] );
+#pragma unroll
+            for( int k = 1; k <= B; ++k ) {
+               float2 const ps = ffma2( sx, vx[ C0 + c - k ], vx[ C0 + c + k ] );
+               acc = ffma2( wtx[ k ], ps, acc );
+            }
+            out[ c ] = acc;
+         }
+#pragma unroll
+         for( int c = 0; c < G::SW; c += 2 ) {
+            *reinterpret_cast< float2* >( ot + ( 2 * rp ) * G::OTS + c0 + c ) = make_float2( out[ c ].x, out[ c + 1 ].x );
+            *reinterpret_cast< float2* >( ot + ( 2 * rp + 1 ) * G::OTS + c0 + c ) = make_float2( out[ c ].y, out[ c + 1 ].y );
+         }
+      }
+      __syncwarp();
+      // coalesced stores of the staged tile: lanes sweep rows in column pairs
+      float* const dst = im->dst;
+      int64_t const ds1 = im->ds1;
+      bool const vec = im->vec_store != 0;
+#pragma unroll 4
+      for( int e = lane; e < TY * ( TX / 2 ); e += 32 ) {
+         int const r = e / ( TX / 2 ), cp = e - r * ( TX / 2 );
+         int const xo = x0 + 2 * cp, yo = y0 + r;
+         if( xo < nx && yo < ny ) {
+            float2 const val = *reinterpret_cast< float2 const* >( ot + r * G::OTS + 2 * cp );
+            float* const p = dst + static_cast< int64_t >( yo ) * ds1 + xo;
+            if( xo + 1 < nx && vec ) {
+               *reinterpret_cast< float2* >( p ) = val;
+            } else {
+               p[ 0 ] = val.x;
+               if( xo + 1 < nx ) { p[ 1 ] = val.y; }
+            }
+         }
+      }
+      __syncwarp();   // b2, tables, taps and staging reads done before the next tile
+   }
+}
+
+template< int B >
+cudaError_t launch_batch_ws( G2Args const& a, int grid, cudaStream_t st ) {
+   batch_ws_kernel< B ><<< grid, W2Geom< float, B, 32 >::NT, G2Geom< B >::BYTES, st >>>( a );
+   return cudaGetLastError();
+}
+
+template< int B >
+int batch_ws_grid() {
+   static std::mutex mu;
+   static std::map< int, int > cache;
+   int dev = 0;
+   cudaGetDevice( &dev );
+   std::lock_guard< std::mutex > lock( mu );
+   auto it = cache.find( dev );
+   if( it != cache.end() ) { return it->second; }
+   auto kern = batch_ws_kernel< B >;
+   size_t const smem = G2Geom< B >::BYTES;
+   if( cudaFuncSetAttribute( kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast< int >( smem )) != cudaSuccess ) {
+      return -1;
+   }
+   int per_sm = 0, sms = 148;
+   if( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &per_sm, kern, W2Geom< float, B, 32 >::NT, smem ) != cudaSuccess || per_sm < 1 ) {
+      return -1;
+   }
+   cudaDeviceGetAttribute( &sms, cudaDevAttrMultiProcessorCount, dev );
+   cache[ dev ] = std::min( per_sm, 2 ) * sms;
+   return cache[ dev ];
+}
+
+int g2_tile_x( int b ) {
+   switch( b ) {
+      case 0: return W2Geom< float, 4, 32 >::TX;
+      case 1: return W2Geom< float, 6, 32 >::TX;
+      case 2: return W2Geom< float, 9, 32 >::TX;
+      default: return W2Geom< float, 12, 32 >::TX;
+   }
+}
+
+int g2_box_h( int b ) {
+   switch( b ) {
+      case 0: return W2Geom< float, 4, 32 >::BH;
+      case 1: return W2Geom< float, 6, 32 >::BH;
+      case 2: return W2Geom< float, 9, 32 >::BH;
+      default: return W2Geom< float, 12, 32 >::BH;
+   }
+}
+
+int g2_grid( int b ) {
+   switch( b ) {
+      case 0: return batch_ws_grid< 4 >();
+      case 1: return batch_ws_grid< 6 >();
+      case 2: return batch_ws_grid< 9 >();
+      default: return batch_ws_grid< 12 >();
+   }
+}
+
+cudaError_t g2_launch( int b, G2Args const& a, int grid, cudaStream_t st ) {
+   switch( b ) {
+      case 0: return launch_batch_ws< 4 >( a, grid, st );
+      case 1: return launch_batch_ws< 6 >( a, grid, st );
+      case 2: return launch_batch_ws< 9 >( a, grid, st );
+      default: return launch_batch_ws< 12 >( a, grid, st );
+   }
+}
+
 // Candidate tile shapes (the autotuner's search space).
 struct TileShape { int tx, ty; };
 constexpr TileShape kShapes[ 3 ] = { { 64, 32 }, { 64, 16 }, { 128, 32 } };
@@ -308,6 +647,11 @@ struct dipcu_batch_plan {
    float* d_bank = nullptr;
    int32_t* d_counter = nullptr;
    int nitems = 0;
+   // Grouped warp-per-tile path, per half-width bucket (4, 6, 9, 12).
+   std::vector< int > gbucket;             // per image: bucket index, or -1 (persistent tile kernel)
+   G2Image* d_gimg[ 4 ] = {};
+   BatchItem* d_gitems[ 4 ] = {};
+   int g_nimg[ 4 ] = {}, g_nitems[ 4 ] = {}, g_grid[ 4 ] = {};
    cudaStream_t cap_stream = nullptr;
    cudaGraph_t graph = nullptr;
    cudaGraphExec_t exec = nullptr;
@@ -317,12 +661,86 @@ namespace {
 
 int plan_fail( int code, std::string const& msg ) { return record_error( code, msg.c_str() ); }
 
+// Images the grouped warp-per-tile path takes: both half-widths up to 12, x-y boundary
+// conditions with every halo source inside the staged box ("mirror", "zero order", "add zeros",
+// "asym mirror"; sizes above the bucket), and a TMA-compatible layout.  Their tables and work
+// items are uploaded once per plan; `inject` plants one impossible item when the persistent tile
+// kernel gets no items of its own.
+int plan_groups( dipcu_batch_plan* p, int inject ) {
+   p->gbucket.assign( static_cast< size_t >( p->count ), -1 );
+   if( getenv( "DIPCU_BATCH_NO_WS" )) { return DIPCU_OK; }
+   std::vector< G2Image > gimg[ 4 ];
+   std::vector< BatchItem > gitems[ 4 ];
+   int rest = 0;
+   for( int i = 0; i < p->count; ++i ) {
+      BatchImage const& im = p->images[ static_cast< size_t >( i ) ];
+      int const hm = std::max( im.h[ 0 ], im.h[ 1 ] );
+      int const b = hm <= 4 ? 0 : hm <= 6 ? 1 : hm <= 9 ? 2 : hm <= 12 ? 3 : -1;
+      bool ok = b >= 0 && ( reinterpret_cast< uintptr_t >( im.src ) & 15 ) == 0 && im.ss[ 1 ] > 0 && ( im.ss[ 1 ] * 4 ) % 16 == 0 &&
+                im.ds[ 1 ] > 0 && im.n[ 0 ] < ( 1 << 30 ) && im.n[ 1 ] < ( 1 << 30 );
+      for( int d = 0; d < 2 && ok; ++d ) {
+         int32_t const bc = im.bc[ d ];
+         ok = ( bc == BC_SYMMETRIC_MIRROR || bc == BC_ZERO_ORDER_EXTRAPOLATE || bc == BC_ADD_ZEROS || bc == BC_ASYMMETRIC_MIRROR ) &&
+              im.n[ d ] > kG2Buckets[ b ];
+      }
+      G2Image g{};
+      if( ok ) {
+         cuuint64_t dims[ 4 ] = { static_cast< cuuint64_t >( im.n[ 0 ] ), static_cast< cuuint64_t >( im.n[ 1 ] ), 1, 1 };
+         cuuint64_t plane = static_cast< cuuint64_t >( im.ss[ 1 ] * im.n[ 1 ] * 4 );
+         plane = ( plane + 15 ) / 16 * 16;
+         cuuint64_t strides[ 3 ] = { static_cast< cuuint64_t >( im.ss[ 1 ] * 4 ), plane, plane };
+         cuuint32_t box[ 4 ] = { 64, static_cast< cuuint32_t >( g2_box_h( b )), 1, 1 };
+         ok = encode_source_map( &g.tmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, im.src, dims, strides, box ) == CUDA_SUCCESS;
+      }
+      if( !ok ) { ++rest; continue; }
+      g.dst = im.dst;
+      g.ds1 = im.ds[ 1 ];
+      for( int d = 0; d < 2; ++d ) {
+         g.n[ d ] = static_cast< int32_t >( im.n[ d ] );
+         g.bc[ d ] = im.bc[ d ];
+         g.h[ d ] = im.h[ d ];
+         g.wofs[ d ] = im.wofs[ d ];
+         g.odd[ d ] = im.odd[ d ];
+      }
+      int const tx = g2_tile_x( b );
+      g.tiles_x = static_cast< int32_t >(( im.n[ 0 ] + tx - 1 ) / tx );
+      g.tiles_y = static_cast< int32_t >(( im.n[ 1 ] + 31 ) / 32 );
+      g.vec_store = (( reinterpret_cast< uintptr_t >( im.dst ) & 7 ) == 0 && im.ds[ 1 ] % 2 == 0 ) ? 1 : 0;
+      int const gi = static_cast< int >( gimg[ b ].size());
+      for( int t = 0; t < g.tiles_x * g.tiles_y; ++t ) { gitems[ b ].push_back( BatchItem{ gi, t } ); }
+      gimg[ b ].push_back( g );
+      p->gbucket[ static_cast< size_t >( i ) ] = b;
+   }
+   if( inject && rest == 0 ) {
+      for( auto& v : gitems ) {
+         if( v.empty()) { continue; }
+         if( inject == 1 ) { v[ v.size() / 2 ].image = 1 << 20; } else { v[ v.size() / 2 ].tile = 1 << 30; }
+         break;
+      }
+   }
+   for( int b = 0; b < 4; ++b ) {
+      p->g_nimg[ b ] = static_cast< int >( gimg[ b ].size());
+      p->g_nitems[ b ] = static_cast< int >( gitems[ b ].size());
+      if( gitems[ b ].empty()) { continue; }
+      p->g_grid[ b ] = g2_grid( b );
+      if( p->g_grid[ b ] < 1 ||
+          cudaMalloc( &p->d_gimg[ b ], sizeof( G2Image ) * gimg[ b ].size()) != cudaSuccess ||
+          cudaMalloc( &p->d_gitems[ b ], sizeof( BatchItem ) * gitems[ b ].size()) != cudaSuccess ||
+          cudaMemcpy( p->d_gimg[ b ], gimg[ b ].data(), sizeof( G2Image ) * gimg[ b ].size(), cudaMemcpyHostToDevice ) != cudaSuccess ||
+          cudaMemcpy( p->d_gitems[ b ], gitems[ b ].data(), sizeof( BatchItem ) * gitems[ b ].size(), cudaMemcpyHostToDevice ) != cudaSuccess ) {
+         return plan_fail( DIPCU_ERR_CUDA, "batch plan: grouped tables" );
+      }
+   }
+   return DIPCU_OK;
+}
+
 // Tile the images for shape `s` and upload the work items, most expensive first.
 int plan_items( dipcu_batch_plan* p, int s, int inject ) {
    TileShape const ts = kShapes[ s ];
    std::vector< BatchItem > items;
    for( int i = 0; i < p->count; ++i ) {
       BatchImage& im = p->images[ static_cast< size_t >( i ) ];
+      if( p->gbucket[ static_cast< size_t >( i ) ] >= 0 ) { continue; }   // grouped warp-per-tile path
       im.tiles_x = static_cast< int32_t >(( im.n[ 0 ] + ts.tx - 1 ) / ts.tx );
       im.tiles_y = static_cast< int32_t >(( im.n[ 1 ] + ts.ty - 1 ) / ts.ty );
       for( int t = 0; t < im.tiles_x * im.tiles_y; ++t ) { items.push_back( BatchItem{ i, t } ); }
@@ -355,16 +773,30 @@ int enqueue_run( dipcu_batch_plan* p, cudaStream_t st ) {
    cudaError_t e = launch_gauss_weights( p->d_sigmas, p->d_orders, 2 * p->count, p->truncation, p->d_bank, nullptr,
                                          nullptr, kBankStride, st );
    if( e != cudaSuccess ) { return plan_fail( DIPCU_ERR_CUDA, "gauss_weights_kernel" ); }
-   BatchArgs a{};
-   a.images = p->d_images;
-   a.items = p->d_items;
-   a.wbank = p->d_bank;
-   a.counter = p->d_counter;
-   a.status = device_status_ptr();
-   a.nimages = p->count;
-   a.nitems = p->nitems;
-   e = launch_shape( p->shape, p->grid, a, st );
-   if( e != cudaSuccess ) { return plan_fail( DIPCU_ERR_CUDA, std::string( "batch_kernel: " ) + cudaGetErrorString( e )); }
+   if( p->nitems > 0 ) {
+      BatchArgs a{};
+      a.images = p->d_images;
+      a.items = p->d_items;
+      a.wbank = p->d_bank;
+      a.counter = p->d_counter;
+      a.status = device_status_ptr();
+      a.nimages = p->count;
+      a.nitems = p->nitems;
+      e = launch_shape( p->shape, p->grid, a, st );
+      if( e != cudaSuccess ) { return plan_fail( DIPCU_ERR_CUDA, std::string( "batch_kernel: " ) + cudaGetErrorString( e )); }
+   }
+   for( int b = 0; b < 4; ++b ) {
+      if( p->g_nitems[ b ] == 0 ) { continue; }
+      G2Args g{};
+      g.images = p->d_gimg[ b ];
+      g.items = p->d_gitems[ b ];
+      g.wbank = p->d_bank;
+      g.status = device_status_ptr();
+      g.nimages = p->g_nimg[ b ];
+      g.nitems = p->g_nitems[ b ];
+      e = g2_launch( b, g, std::min( p->g_grid[ b ], std::max( 1, p->g_nitems[ b ] / 4 )), st );
+      if( e != cudaSuccess ) { return plan_fail( DIPCU_ERR_CUDA, std::string( "batch_ws_kernel: " ) + cudaGetErrorString( e )); }
+   }
    return DIPCU_OK;
 }
 
@@ -448,6 +880,7 @@ int dipcu_batch_plan_create( dipcu_image_desc const* ins, dipcu_image_desc const
       dipcu_batch_plan_destroy( p );
       return plan_fail( DIPCU_ERR_CUDA, "device status word" );
    }
+   if( int st = plan_groups( p, inject )) { dipcu_batch_plan_destroy( p ); return st; }
    // Tile shape: the autotuner times every candidate on this batch (the filter outputs are
    // overwritten by the final runs), remembering the winner per batch signature.
    int shape = 0;
@@ -509,7 +942,10 @@ int dipcu_batch_plan_run( dipcu_batch_plan* plan, void* stream ) {
 
 int dipcu_batch_plan_info( dipcu_batch_plan const* plan, int* nitems, int* tile_x, int* tile_y, int* grid ) {
    if( !plan ) { return plan_fail( DIPCU_ERR_INVALID_ARG, "null plan" ); }
-   if( nitems ) { *nitems = plan->nitems; }
+   if( nitems ) {
+      *nitems = plan->nitems;
+      for( int b = 0; b < 4; ++b ) { *nitems += plan->g_nitems[ b ]; }
+   }
    if( tile_x ) { *tile_x = kShapes[ plan->shape ].tx; }
    if( tile_y ) { *tile_y = kShapes[ plan->shape ].ty; }
    if( grid ) { *grid = plan->grid; }
@@ -530,6 +966,10 @@ int dipcu_batch_plan_destroy( dipcu_batch_plan* plan ) {
    cudaFree( plan->d_orders );
    cudaFree( plan->d_bank );
    cudaFree( plan->d_counter );
+   for( int b = 0; b < 4; ++b ) {
+      cudaFree( plan->d_gimg[ b ] );
+      cudaFree( plan->d_gitems[ b ] );
+   }
    delete plan;
    return DIPCU_OK;
 }

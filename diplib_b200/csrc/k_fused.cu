@@ -552,6 +552,11 @@ Entry const* find( FusedKey const& k ) {
 
 } // namespace
 
+CUresult encode_source_map( CUtensorMap* out, CUtensorMapDataType dt, void const* ptr, cuuint64_t const* dims,
+                            cuuint64_t const* strides, cuuint32_t const* box ) {
+   return encode_tmap( out, dt, ptr, dims, strides, box );
+}
+
 cudaError_t launch_fused2d_ws( FusedKey const& key, FusedArgs& args, cudaStream_t stream ) {
    if( key.ndims != 2 || getenv( "DIPCU_NO_WS" )) { return cudaErrorNotSupported; }
    if( key.in_dt == DT_SFLOAT ) { return run2d_ws_bucket< float >( args, key.h, key.odd, stream ); }
