@@ -551,11 +551,12 @@ def run_batch(args):
                         "bytes_per_voxel": 8, "avg_kernel_ms": avg}
     line["clocks"] = clk
     line["gpu_launches"] = 2 * args.steps   # weights + persistent kernel per graph
-    # The same per-pixel work as single large images: per (sigma, orders) combination of the
-    # batch, the plain path's rate on one 4096x4096 image; the batch's pixel shares weight them.
+    # The same per-pixel work as single large images: per (sigma, orders, boundary condition)
+    # combination of the batch, the plain path's rate on one 4096x4096 image; the batch's pixel
+    # shares weight them.
     share = {}
-    for (h, w), (sg, o, _) in zip(shapes, params):
-        key = (sg, o[0], o[1])
+    for (h, w), (sg, o, bc) in zip(shapes, params):
+        key = (sg, o[0], o[1], bc)
         share[key] = share.get(key, 0) + h * w
     big = torch.rand((4096, 4096), generator=gen, device=dev)
     bigs = [big, big.clone().add_(1e-3)]
@@ -563,19 +564,19 @@ def run_batch(args):
     t_single = 0.0
     rates = {}
     for key, px in sorted(share.items()):
-        sg, ox, oy = key
-        gl = [[_capture(lambda i=i: dipcu.GaussFIR(bigs[i], [sg, sg], [ox, oy], ["mirror"], 3.0, out=bigo[i]))]
+        sg, ox, oy, bc = key
+        gl = [[_capture(lambda i=i: dipcu.GaussFIR(bigs[i], [sg, sg], [ox, oy], [bc], 3.0, out=bigo[i]))]
               for i in range(2)]
         for g in gl:
             g[0].replay()
         tt, _, _ = _timed(gl, 10, dev)
         r = 4096 * 4096 * 10 / (tt * 1e-3) / 1e9
-        rates[f"s{sg}_o{ox}{oy}"] = round(r, 2)
+        rates[f"s{sg}_o{ox}{oy}_{bc.replace(' ', '')}"] = round(r, 2)
         t_single += px / (r * 1e9)
     single_rate = npx / t_single / 1e9
     line["vs_single_image"] = {"single_image_gvox_s": single_rate, "ratio": value / world / single_rate,
-                               "how": "plain dipcu_gauss_fir on one 4096^2 image per (sigma, orders) combination, "
-                                      "weighted by the batch's pixel shares", "rates": rates}
+                               "how": "plain dipcu_gauss_fir on one 4096^2 image per (sigma, orders, boundary "
+                                      "condition) combination, weighted by the batch's pixel shares", "rates": rates}
     # e2e: every image in from pinned host memory, every result back.
     h_in = [t.cpu().pin_memory() for t in ins]
     h_out = [torch.empty(s).pin_memory() for s in shapes]

@@ -232,10 +232,17 @@ __global__ void __launch_bounds__( 256 ) batch_kernel( BatchArgs const __grid_co
 // the 2D tile kernel takes (fused2d_ws.cuh) run through a variant of that kernel with per-image
 // tables: a TMA map per image in device memory and a work list of (image, tile) items, dealt
 // round-robin over the warps of a persistent grid.  Taps come from the plan's weight bank per
-// tile (zero beyond each axis' half-width), so a sigma-table update replays correctly.
+// tile (zero beyond each axis' half-width), so a sigma-table update replays correctly.  Images
+// whose row stride is not a multiple of 16 bytes (TMA global strides are) get the same boxes
+// from per-lane 4-byte cp.async copies with zero fill; every stage fill commits one copy group
+// (empty for TMA boxes), so waiting until SPW - 1 groups are pending finds the current stage's
+// copies done.
 
 struct alignas( 128 ) G2Image {
-   CUtensorMap tmap;        // 4D (x, y, 1, 1) tiled map of the source, box = tile + halo
+   CUtensorMap tmap;        // 4D (x, y, 1, 1) tiled map of the source, box = tile + halo (if tma)
+   float const* src;        // the source, for images whose layout TMA cannot take
+   int64_t ss1;             // source row stride (x stride 1)
+   int32_t tma;             // 1: boxes by TMA; 0: by per-lane asynchronous copies
    float* dst;
    int64_t ds1;             // destination row stride (x stride 1)
    int32_t n[ 2 ];
@@ -310,22 +317,44 @@ __global__ void __launch_bounds__( W2Geom< float, B, 32 >::NT, 2 ) batch_ws_kern
       y0 = ( it.tile / im->tiles_x ) * TY;
       return true;
    };
+   // Warp-wide: fills stage `st` with item t's box (nothing for t past the end) and commits
+   // one copy group.
    auto issue = [ & ]( int64_t t, int st ) {
-      G2Image const* im;
-      int x0, y0;
-      if( lookup( t, im, x0, y0 )) {
-         mbar_arrive_expect_tx( &full[ st ], G::STAGE_BYTES );
-         tma_load_4d( stages + st * G::STAGE_STRIDE, &im->tmap, &full[ st ], x0 - G::LEAD, y0 - B, 0, 0 );
-      } else {
-         mbar_arrive( &full[ st ] );
+      if( t < a.nitems ) {
+         G2Image const* im;
+         int x0, y0;
+         bool const ok = lookup( t, im, x0, y0 );
+         if( ok && im->tma ) {
+            if( lane == 0 ) {
+               mbar_arrive_expect_tx( &full[ st ], G::STAGE_BYTES );
+               tma_load_4d( stages + st * G::STAGE_STRIDE, &im->tmap, &full[ st ], x0 - G::LEAD, y0 - B, 0, 0 );
+            }
+         } else {
+            if( lane == 0 ) { mbar_arrive( &full[ st ] ); }
+            if( ok ) {
+               // Box rows of BW floats, two columns per lane; outside the image: zero fill.
+               int const nx = im->n[ 0 ], ny = im->n[ 1 ];
+               int const bx = x0 - G::LEAD, by = y0 - B;
+               float* const dst = reinterpret_cast< float* >( stages + st * G::STAGE_STRIDE );
+               for( int r = 0; r < BH; ++r ) {
+                  int const y = by + r;
+                  bool const yin = y >= 0 && y < ny;
+#pragma unroll
+                  for( int h = 0; h < 2; ++h ) {
+                     int const c = 2 * lane + h;
+                     int const x = bx + c;
+                     bool const in = yin && x >= 0 && x < nx;
+                     float const* src = in ? im->src + static_cast< int64_t >( y ) * im->ss1 + x : im->src;
+                     asm volatile( "cp.async.ca.shared.global [%0], [%1], 4, %2;"
+                                   :: "r"( smem_u32( dst + r * BW + c )), "l"( src ), "r"( in ? 4 : 0 ) : "memory" );
+                  }
+               }
+            }
+         }
       }
+      asm volatile( "cp.async.commit_group;" ::: "memory" );
    };
-   if( lane == 0 ) {
-      for( int k = 0; k < SPW; ++k ) {
-         int64_t const t = gw + k * nwarps;
-         if( t < a.nitems ) { issue( t, k ); }
-      }
-   }
+   for( int k = 0; k < SPW; ++k ) { issue( gw + k * nwarps, k ); }
    uint32_t kdone = 0;
    for( int64_t t = gw; t < a.nitems; t += nwarps, ++kdone ) {
       int const st = static_cast< int >( kdone % SPW );
@@ -335,12 +364,10 @@ __global__ void __launch_bounds__( W2Geom< float, B, 32 >::NT, 2 ) batch_ws_kern
       bool const valid = lookup( t, im, x0, y0 );
       if( !valid ) {
          w5_wait( &full[ st ], ( kdone / SPW ) & 1u, abort, a.status );
+         asm volatile( "cp.async.wait_group %0;" :: "n"( SPW - 1 ) : "memory" );
          __syncwarp();
-         if( lane == 0 ) {
-            atomicExch( a.status, DIPCU_ERR_INVALID_ARG );
-            int64_t const tn = t + SPW * nwarps;
-            if( tn < a.nitems ) { issue( tn, st ); }
-         }
+         if( lane == 0 ) { atomicExch( a.status, DIPCU_ERR_INVALID_ARG ); }
+         issue( t + SPW * nwarps, st );
          __syncwarp();
          continue;
       }
@@ -395,6 +422,8 @@ __global__ void __launch_bounds__( W2Geom< float, B, 32 >::NT, 2 ) batch_ws_kern
       }
       __syncwarp();
       w5_wait( &full[ st ], ( kdone / SPW ) & 1u, abort, a.status );
+      asm volatile( "cp.async.wait_group %0;" :: "n"( SPW - 1 ) : "memory" );
+      __syncwarp();
       // y pass: lane -> column pair, row blocks of RB outputs
       if( lane < G::NPAIR ) {
          int const pc = G::P0 + lane;
@@ -430,11 +459,8 @@ __global__ void __launch_bounds__( W2Geom< float, B, 32 >::NT, 2 ) batch_ws_kern
          }
       }
       __syncwarp();
-      if( lane == 0 ) {
-         // The stage is read: stream this warp's item SPW ahead into it.
-         int64_t const tn = t + SPW * nwarps;
-         if( tn < a.nitems ) { issue( tn, st ); }
-      }
+      // The stage is read: stream this warp's item SPW ahead into it.
+      issue( t + SPW * nwarps, st );
       if( nfx > 0 ) {
          float2* const b2f = reinterpret_cast< float2* >( b2 );
          for( int f = lane; f < nfx * ( TY / 2 ); f += 32 ) {
@@ -663,7 +689,8 @@ int plan_fail( int code, std::string const& msg ) { return record_error( code, m
 
 // Images the grouped warp-per-tile path takes: both half-widths up to 12, x-y boundary
 // conditions with every halo source inside the staged box ("mirror", "zero order", "add zeros",
-// "asym mirror"; sizes above the bucket), and a TMA-compatible layout.  Their tables and work
+// "asym mirror"; sizes above the bucket), 4-byte aligned rows (TMA boxes where the layout allows,
+// per-lane copies otherwise).  Their tables and work
 // items are uploaded once per plan; `inject` plants one impossible item when the persistent tile
 // kernel gets no items of its own.
 int plan_groups( dipcu_batch_plan* p, int inject ) {
@@ -676,23 +703,26 @@ int plan_groups( dipcu_batch_plan* p, int inject ) {
       BatchImage const& im = p->images[ static_cast< size_t >( i ) ];
       int const hm = std::max( im.h[ 0 ], im.h[ 1 ] );
       int const b = hm <= 4 ? 0 : hm <= 6 ? 1 : hm <= 9 ? 2 : hm <= 12 ? 3 : -1;
-      bool ok = b >= 0 && ( reinterpret_cast< uintptr_t >( im.src ) & 15 ) == 0 && im.ss[ 1 ] > 0 && ( im.ss[ 1 ] * 4 ) % 16 == 0 &&
-                im.ds[ 1 ] > 0 && im.n[ 0 ] < ( 1 << 30 ) && im.n[ 1 ] < ( 1 << 30 );
+      bool ok = b >= 0 && ( reinterpret_cast< uintptr_t >( im.src ) & 3 ) == 0 && im.ss[ 1 ] > 0 && im.ds[ 1 ] > 0 &&
+                im.n[ 0 ] < ( 1 << 30 ) && im.n[ 1 ] < ( 1 << 30 );
       for( int d = 0; d < 2 && ok; ++d ) {
          int32_t const bc = im.bc[ d ];
          ok = ( bc == BC_SYMMETRIC_MIRROR || bc == BC_ZERO_ORDER_EXTRAPOLATE || bc == BC_ADD_ZEROS || bc == BC_ASYMMETRIC_MIRROR ) &&
               im.n[ d ] > kG2Buckets[ b ];
       }
       G2Image g{};
-      if( ok ) {
+      if( !ok ) { ++rest; continue; }
+      g.src = im.src;
+      g.ss1 = im.ss[ 1 ];
+      g.tma = 0;
+      if(( reinterpret_cast< uintptr_t >( im.src ) & 15 ) == 0 && ( im.ss[ 1 ] * 4 ) % 16 == 0 && !getenv( "DIPCU_BATCH_NO_TMA" )) {
          cuuint64_t dims[ 4 ] = { static_cast< cuuint64_t >( im.n[ 0 ] ), static_cast< cuuint64_t >( im.n[ 1 ] ), 1, 1 };
          cuuint64_t plane = static_cast< cuuint64_t >( im.ss[ 1 ] * im.n[ 1 ] * 4 );
          plane = ( plane + 15 ) / 16 * 16;
          cuuint64_t strides[ 3 ] = { static_cast< cuuint64_t >( im.ss[ 1 ] * 4 ), plane, plane };
          cuuint32_t box[ 4 ] = { 64, static_cast< cuuint32_t >( g2_box_h( b )), 1, 1 };
-         ok = encode_source_map( &g.tmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, im.src, dims, strides, box ) == CUDA_SUCCESS;
+         g.tma = encode_source_map( &g.tmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, im.src, dims, strides, box ) == CUDA_SUCCESS ? 1 : 0;
       }
-      if( !ok ) { ++rest; continue; }
       g.dst = im.dst;
       g.ds1 = im.ds[ 1 ];
       for( int d = 0; d < 2; ++d ) {

@@ -97,3 +97,16 @@ def test_batch_planted_invalid_item_is_skipped_and_reported(cuda, flag):
     nan_count = sum(int(torch.isnan(o).sum()) for o in outs)
     assert 0 < nan_count <= 128 * 32
     plan.close()
+
+
+def test_batch_tile_path_aligned_and_unaligned_rows(cuda):
+    """Images the grouped tile path takes, with row strides that TMA can and cannot address
+    (widths multiple of 4 and not), every bucket of half-widths, even and odd orders."""
+    rng = np.random.default_rng(9)
+    imgs, params = [], []
+    for i, (w, s) in enumerate([(64, 0.8), (67, 1.0), (130, 2.0), (131, 2.0), (200, 3.0), (203, 3.0), (96, 4.0), (97, 4.0)]):
+        imgs.append(rng.random((45 + 7 * i, w), dtype=np.float32))
+        params.append((s, [i % 3, (i + 1) % 3] if s < 3 else [0, i % 2], ["mirror", "add zeros"][i % 2]))
+    plan, ins, outs = run_plan(imgs, params, graph=False, autotune=False)
+    check_all(imgs, params, outs)
+    plan.close()
