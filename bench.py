@@ -504,7 +504,8 @@ B_SIGMAS = [0.8, 1.0, 2.0, 4.0, 8.0]
 B_BCS = ["mirror", "periodic", "add zeros"]
 B_CONFIG = {"workload": "batched dip::GaussFIR: 512 2D sfloat images, sides uniform 64..2048, sigma from "
                         "{0.8,1,2,4,8} per image, order per axis from {0,1,2}, boundary from {mirror, periodic, "
-                        "add zeros}, truncation 3; one persistent launch replayed as a CUDA graph, autotuned tiles",
+                        "add zeros}, truncation 3; weights, the persistent tile kernel and the grouped "
+                        "warp-per-tile launches replayed as one CUDA graph, autotuned tiles",
             "l2": "the batch holds 2.3 GB of input and 2.3 GB of output (> 126 MB L2)"}
 
 
@@ -550,7 +551,7 @@ def run_batch(args):
                         "traffic": None, "peak_source": kind, "kernel": "batch_kernel (persistent work queue)",
                         "bytes_per_voxel": 8, "avg_kernel_ms": avg}
     line["clocks"] = clk
-    line["gpu_launches"] = 2 * args.steps   # weights + persistent kernel per graph
+    line["gpu_launches"] = plan.info()["kernels_per_run"] * args.steps   # all kernels of the captured graph
     # The same per-pixel work as single large images: per (sigma, orders, boundary condition)
     # combination of the batch, the plain path's rate on one 4096x4096 image; the batch's pixel
     # shares weight them.

@@ -63,6 +63,7 @@ SIGNATURES = {
     "dipcu_batch_plan_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "dipcu_batch_plan_info": (ctypes.c_int, [ctypes.c_void_p, _P(ctypes.c_int), _P(ctypes.c_int), _P(ctypes.c_int),
                                              _P(ctypes.c_int)]),
+    "dipcu_batch_plan_launches": (ctypes.c_int, [ctypes.c_void_p, _P(ctypes.c_int), _P(ctypes.c_int)]),
     "dipcu_batch_plan_sigmas": (ctypes.c_void_p, [ctypes.c_void_p]),
     "dipcu_batch_plan_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "dipcu_device_status": (ctypes.c_int, [_P(ctypes.c_int), ctypes.c_int]),

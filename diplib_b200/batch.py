@@ -66,7 +66,10 @@ class BatchPlan:
         ni, tx, ty, g = (ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int())
         check(_abi.lib().dipcu_batch_plan_info(self._plan, ctypes.byref(ni), ctypes.byref(tx), ctypes.byref(ty),
                                                ctypes.byref(g)))
-        return {"items": ni.value, "tile": (tx.value, ty.value), "grid": g.value}
+        nk, ng = ctypes.c_int(), ctypes.c_int()
+        check(_abi.lib().dipcu_batch_plan_launches(self._plan, ctypes.byref(nk), ctypes.byref(ng)))
+        return {"items": ni.value, "tile": (tx.value, ty.value), "grid": g.value, "kernels_per_run": nk.value,
+                "grouped_items": ng.value}
 
     def sigma_table(self) -> torch.Tensor:
         """The plan's device sigma table (2 * count float64, x then y per image), as a tensor view

@@ -982,6 +982,18 @@ int dipcu_batch_plan_info( dipcu_batch_plan const* plan, int* nitems, int* tile_
    return DIPCU_OK;
 }
 
+int dipcu_batch_plan_launches( dipcu_batch_plan const* plan, int* kernels, int* grouped_items ) {
+   if( !plan ) { return plan_fail( DIPCU_ERR_INVALID_ARG, "null plan" ); }
+   int k = 1 + ( plan->nitems > 0 ? 1 : 0 ), g = 0;
+   for( int b = 0; b < 4; ++b ) {
+      k += plan->g_nitems[ b ] > 0 ? 1 : 0;
+      g += plan->g_nitems[ b ];
+   }
+   if( kernels ) { *kernels = k; }
+   if( grouped_items ) { *grouped_items = g; }
+   return DIPCU_OK;
+}
+
 double* dipcu_batch_plan_sigmas( dipcu_batch_plan* plan ) {
    return plan ? plan->d_sigmas : nullptr;
 }

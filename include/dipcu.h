@@ -139,15 +139,18 @@ int dipcu_structure_tensor_backward( dipcu_image_desc const* grad_out, dipcu_ima
 /* ---- Batched filter ------------------------------------------------------------------------ */
 
 /* Many 2D sfloat images of uneven sizes, each with its own per-axis sigmas, orders (0..3) and
- * boundary conditions (the index-mapping ones and "add zeros"; half-widths up to 32), filtered by
- * one persistent launch that pulls (image, tile) work items from a device queue.  No DIPlib
- * counterpart (DIPlib filters one image per call; this is dip::GaussFIR per image).
+ * boundary conditions (the index-mapping ones and "add zeros"; half-widths up to 32).  Images
+ * with both half-widths up to 12 and "mirror", "zero order", "add zeros" or "asym mirror" along
+ * both axes run through grouped warp-per-tile launches (one per half-width bucket, per-image work
+ * lists); the others through one persistent launch that pulls (image, tile) work items from a
+ * device queue.  No DIPlib counterpart (DIPlib filters one image per call; this is
+ * dip::GaussFIR per image).
  * `sigmas`, `orders`, `bcs`: host arrays of 2 * count entries (x then y of each image).
- * Flags: DIPCU_BATCH_GRAPH captures the run (queue reset, on-device weights, persistent kernel)
+ * Flags: DIPCU_BATCH_GRAPH captures the run (queue reset, on-device weights, all launches)
  * into a CUDA graph so that dipcu_batch_plan_run is one graph launch; DIPCU_BATCH_AUTOTUNE times
  * the candidate tile shapes on this batch at creation (overwriting the outputs) and keeps the
  * fastest, remembered per batch signature.  The two INJECT flags are test hooks that plant one
- * impossible work item, which the kernel skips and reports through dipcu_device_status.
+ * impossible work item, which the kernels skip and report through dipcu_device_status.
  * The plan allocates its tables at creation; runs allocate nothing.  The images must stay alive
  * while the plan is used.  The sigma table (dipcu_batch_plan_sigmas, device, 2 * count doubles)
  * may be rewritten between runs, as long as no kernel length changes. */
@@ -160,8 +163,12 @@ int dipcu_batch_plan_create( dipcu_image_desc const* ins, dipcu_image_desc const
                              double const* sigmas, uint32_t const* orders, int32_t const* bcs, double truncation,
                              int flags, dipcu_batch_plan** plan );
 int dipcu_batch_plan_run( dipcu_batch_plan* plan, void* stream );
-/* Work items, chosen tile shape and persistent grid size of a plan. */
+/* Work items (all paths), chosen tile shape and persistent grid size of a plan. */
 int dipcu_batch_plan_info( dipcu_batch_plan const* plan, int* nitems, int* tile_x, int* tile_y, int* grid );
+/* Kernels one run launches (the weights kernel, the persistent tile kernel when it has items,
+ * one grouped warp-per-tile launch per half-width bucket in use) and the work items the grouped
+ * path takes.  No counterpart in the reference (plan introspection). */
+int dipcu_batch_plan_launches( dipcu_batch_plan const* plan, int* kernels, int* grouped_items );
 double* dipcu_batch_plan_sigmas( dipcu_batch_plan* plan );
 int dipcu_batch_plan_destroy( dipcu_batch_plan* plan );
 
