@@ -68,7 +68,7 @@ bool try_fused( dipcu_image_desc const* in, dipcu_image_desc const* out, std::ve
                 std::vector< int > const& order, bool compute_double, cudaStream_t stream, cudaError_t* err ) {
    int const nd = in->ndims;
    int const np = static_cast< int >( order.size() );
-   if( compute_double || out->dtype != DT_SFLOAT ) { return false; }
+   if( compute_double || out->dtype != DT_SFLOAT || getenv( "DIPCU_NO_FUSED" )) { return false; }   // switch for A/B timing
    if( !( in->dtype == DT_SFLOAT || in->dtype == DT_UINT16 || in->dtype == DT_UINT8 || in->dtype == DT_SINT16 )) { return false; }
    if( np != 2 && np != 3 ) { return false; }
    for( int d : order ) {

@@ -14,6 +14,8 @@
 // smallest-stride axis share a CTA so that global accesses stay coalesced.
 #include <cuda_runtime.h>
 
+#include <cstdlib>
+
 #include "dipcu_common.cuh"
 #include "dipcu_internal.h"
 
@@ -106,6 +108,191 @@ __global__ void __launch_bounds__( 256 ) line_pass_kernel( LineArgs< T, MAXH1 > 
    }
 }
 
+// ---- fast float path ------------------------------------------------------------------------
+// Float input and output, half-widths up to 32, the index-mapping boundary conditions and "add
+// zeros", and a unit-stride axis in both images: the same pass with the taps unrolled over a
+// compile-time bucket HB >= h (zero beyond h) and register windows.
+//   * Along the unit-stride axis (line_x_kernel): a CTA stages one line segment of 128 R_X outputs
+//     plus the halo in shared memory (coalesced loads, boundary extension at the line ends); each
+//     thread evaluates R_X consecutive outputs from a float4 window of R_X + 2 HB samples.
+//   * Along any other axis (line_y_kernel): threads run along the unit-stride axis (coalesced),
+//     each owns one column and evaluates R_Y consecutive outputs along the processed axis from a
+//     register window of R_Y + 2 HB samples read straight from global memory (the window overlap
+//     of neighbouring blocks is served by L1/L2).
+
+constexpr int kFastMaxH = 32;
+constexpr int kRX = 4;    // outputs per thread, line_x_kernel
+constexpr int kRY = 16;   // outputs per thread, line_y_kernel
+
+struct LineFastArgs {
+   float const* src;
+   float* dst;
+   int32_t ndims, axis, comp;   // comp: the unit-stride axis the threads of line_y_kernel run along
+   int32_t h, odd, bc;
+   int64_t n, ncomp, nouter;    // length along axis, size along comp, lines (x) / column groups (y)
+   int64_t sizes[ DIPCU_MAX_DIMS ];
+   int64_t sst[ DIPCU_MAX_DIMS ], dstst[ DIPCU_MAX_DIMS ];
+   float taps[ kFastMaxH + 1 ];  // centre first, zero beyond h
+};
+
+// Source sample at index j of a line (base offset `base`, stride `st`), extended past [0, n) with
+// the boundary condition (index maps; zero for "add zeros").
+__device__ __forceinline__ float fast_load( LineFastArgs const& a, int64_t base, int64_t st, int64_t j ) {
+   if( j >= 0 && j < a.n ) { return __ldg( a.src + base + j * st ); }
+   if( a.bc == BC_ADD_ZEROS ) { return 0.f; }
+   bool neg;
+   int64_t const i = bc_map_index( j, a.n, a.bc, &neg );
+   float const v = __ldg( a.src + base + i * st );
+   return neg ? -v : v;
+}
+
+// Offsets of the line / column group u over all axes but `axis` (and `comp`).
+__device__ __forceinline__ void fast_decode( LineFastArgs const& a, int64_t u, int64_t& sb, int64_t& db ) {
+   sb = 0;
+   db = 0;
+   for( int d = 0; d < a.ndims; ++d ) {
+      if( d == a.axis || d == a.comp ) { continue; }
+      int64_t const c = u % a.sizes[ d ];
+      u /= a.sizes[ d ];
+      sb += c * a.sst[ d ];
+      db += c * a.dstst[ d ];
+   }
+}
+
+template< int HB, bool ODD >
+__device__ __forceinline__ float fast_tap_sum( LineFastArgs const& a, float const* v ) {   // v[0] is the centre
+   float s0 = ODD ? 0.f : a.taps[ 0 ] * v[ 0 ], s1 = 0.f;
+#pragma unroll
+   for( int k = 1; k <= HB; ++k ) {
+      float const p = ODD ? v[ k ] - v[ -k ] : v[ k ] + v[ -k ];
+      if( k & 1 ) { s1 = fmaf( a.taps[ k ], p, s1 ); } else { s0 = fmaf( a.taps[ k ], p, s0 ); }
+   }
+   return s0 + s1;
+}
+
+template< int HB, bool ODD >
+__global__ void __launch_bounds__( 128 ) line_x_kernel( LineFastArgs const __grid_constant__ a ) {
+   constexpr int T = 128 * kRX, W = T + 2 * HB;
+   __shared__ __align__( 16 ) float tile[ ( W + 3 ) / 4 * 4 ];
+   int const tid = static_cast< int >( threadIdx.x );
+   int64_t const a0 = static_cast< int64_t >( blockIdx.x ) * T;
+   int64_t const sa = a.sst[ a.axis ], da = a.dstst[ a.axis ];
+   for( int64_t u = blockIdx.y; u < a.nouter; u += gridDim.y ) {
+      int64_t sb, db;
+      fast_decode( a, u, sb, db );
+      for( int e = tid; e < W; e += 128 ) { tile[ e ] = fast_load( a, sb, sa, a0 - HB + e ); }
+      __syncthreads();
+      float v[ kRX + 2 * HB + 4 ];
+      float4 const* w4 = reinterpret_cast< float4 const* >( tile + tid * kRX );
+#pragma unroll
+      for( int q = 0; q < ( kRX + 2 * HB + 3 ) / 4; ++q ) {
+         float4 const f = w4[ q ];
+         v[ 4 * q ] = f.x; v[ 4 * q + 1 ] = f.y; v[ 4 * q + 2 ] = f.z; v[ 4 * q + 3 ] = f.w;
+      }
+#pragma unroll
+      for( int r = 0; r < kRX; ++r ) {
+         int64_t const i = a0 + tid * kRX + r;
+         if( i < a.n ) { a.dst[ db + i * da ] = fast_tap_sum< HB, ODD >( a, v + HB + r ); }
+      }
+      __syncthreads();
+   }
+}
+
+template< int HB, bool ODD >
+__global__ void __launch_bounds__( 128 ) line_y_kernel( LineFastArgs const __grid_constant__ a ) {
+   int64_t const c = static_cast< int64_t >( blockIdx.x ) * 128 + threadIdx.x;
+   if( c >= a.ncomp ) { return; }
+   int64_t const sa = a.sst[ a.axis ], da = a.dstst[ a.axis ];
+   int64_t const nblk = ( a.n + kRY - 1 ) / kRY;
+   for( int64_t u = blockIdx.y; u < a.nouter * nblk; u += gridDim.y ) {
+      int64_t const blk = u % nblk;
+      int64_t sb, db;
+      fast_decode( a, u / nblk, sb, db );
+      sb += c * a.sst[ a.comp ];
+      db += c * a.dstst[ a.comp ];
+      int64_t const i0 = blk * kRY;
+      float v[ kRY + 2 * HB ];
+      if( i0 - HB >= 0 && i0 + kRY + HB <= a.n ) {
+         float const* p = a.src + sb + ( i0 - HB ) * sa;
+#pragma unroll
+         for( int j = 0; j < kRY + 2 * HB; ++j ) { v[ j ] = __ldg( p + j * sa ); }
+      } else {
+#pragma unroll
+         for( int j = 0; j < kRY + 2 * HB; ++j ) { v[ j ] = fast_load( a, sb, sa, i0 - HB + j ); }
+      }
+#pragma unroll
+      for( int r = 0; r < kRY; ++r ) {
+         int64_t const i = i0 + r;
+         if( i < a.n ) { a.dst[ db + i * da ] = fast_tap_sum< HB, ODD >( a, v + HB + r ); }
+      }
+   }
+}
+
+template< int HB >
+cudaError_t launch_fast_bucket( LineFastArgs const& a, bool along, cudaStream_t stream ) {
+   if( along ) {
+      int64_t const gx = ( a.n + 128 * kRX - 1 ) / ( 128 * kRX );
+      int64_t const gy = a.nouter < 65535 ? a.nouter : 65535;
+      if( gx > 0x7fffffff ) { return cudaErrorInvalidValue; }
+      dim3 const grid( static_cast< unsigned >( gx ), static_cast< unsigned >( gy ));
+      if( a.odd ) { line_x_kernel< HB, true ><<< grid, 128, 0, stream >>>( a ); }
+      else { line_x_kernel< HB, false ><<< grid, 128, 0, stream >>>( a ); }
+   } else {
+      int64_t const gx = ( a.ncomp + 127 ) / 128;
+      int64_t const work = a.nouter * (( a.n + kRY - 1 ) / kRY );
+      int64_t const gy = work < 65535 ? work : 65535;
+      if( gx > 0x7fffffff ) { return cudaErrorInvalidValue; }
+      dim3 const grid( static_cast< unsigned >( gx ), static_cast< unsigned >( gy ));
+      if( a.odd ) { line_y_kernel< HB, true ><<< grid, 128, 0, stream >>>( a ); }
+      else { line_y_kernel< HB, false ><<< grid, 128, 0, stream >>>( a ); }
+   }
+   return cudaGetLastError();
+}
+
+// cudaErrorNotSupported when the pass is not one the fast path takes.
+cudaError_t launch_line_fast( LinePass const& p, cudaStream_t stream ) {
+   if( p.compute_double || p.src_dt != DT_SFLOAT || p.dst_dt != DT_SFLOAT || p.h < 0 || p.h > kFastMaxH ||
+       !bc_is_index_map( p.bc ) || getenv( "DIPCU_NO_FAST_LINE" )) {
+      return cudaErrorNotSupported;
+   }
+   LineFastArgs a{};
+   a.src = static_cast< float const* >( p.src );
+   a.dst = static_cast< float* >( p.dst );
+   a.ndims = p.ndims;
+   a.axis = p.axis;
+   a.h = static_cast< int32_t >( p.h );
+   a.odd = p.odd;
+   a.bc = p.bc;
+   a.n = p.sizes[ p.axis ];
+   for( int d = 0; d < p.ndims; ++d ) {
+      a.sizes[ d ] = p.sizes[ d ];
+      a.sst[ d ] = p.src_strides[ d ];
+      a.dstst[ d ] = p.dst_strides[ d ];
+   }
+   for( int k = 0; k <= kFastMaxH; ++k ) { a.taps[ k ] = k <= p.h ? static_cast< float >( p.taps[ k ] ) : 0.f; }
+   bool const along = p.src_strides[ p.axis ] == 1 && p.dst_strides[ p.axis ] == 1;
+   a.comp = -1;
+   if( !along ) {
+      for( int d = 0; d < p.ndims; ++d ) {
+         if( d != p.axis && p.sizes[ d ] > 1 && p.src_strides[ d ] == 1 && p.dst_strides[ d ] == 1 ) { a.comp = d; break; }
+      }
+      if( a.comp < 0 ) { return cudaErrorNotSupported; }
+   }
+   a.ncomp = along ? 1 : p.sizes[ a.comp ];
+   int64_t nouter = 1;
+   for( int d = 0; d < p.ndims; ++d ) {
+      if( d != a.axis && d != a.comp ) { nouter *= p.sizes[ d ]; }
+   }
+   a.nouter = nouter;
+   int const hb = p.h <= 4 ? 4 : p.h <= 8 ? 8 : p.h <= 16 ? 16 : 32;
+   switch( hb ) {
+      case 4: return launch_fast_bucket< 4 >( a, along, stream );
+      case 8: return launch_fast_bucket< 8 >( a, along, stream );
+      case 16: return launch_fast_bucket< 16 >( a, along, stream );
+      default: return launch_fast_bucket< 32 >( a, along, stream );
+   }
+}
+
 // Sample-type conversion of a whole image (dip::Image::Copy with clamp_cast), used when no
 // axis is filtered (framework_separable.cpp:155-159).
 template< typename T >
@@ -194,6 +381,10 @@ cudaError_t launch_line( LinePass const& p, cudaStream_t stream ) {
 
 cudaError_t launch_line_pass( LinePass const& p, cudaStream_t stream ) {
    if( p.h < 0 || p.h > kLineMaxHalf ) { return cudaErrorInvalidValue; }
+   {
+      cudaError_t const e = launch_line_fast( p, stream );
+      if( e != cudaErrorNotSupported ) { return e; }
+   }
    if( p.compute_double ) {
       return p.h < 64 ? launch_line< double, 64 >( p, stream ) : launch_line< double, kLineMaxHalf + 1 >( p, stream );
    }
