@@ -592,6 +592,156 @@ cudaError_t g2_launch( int b, G2Args const& a, int grid, cudaStream_t st ) {
    }
 }
 
+// ---- grouped line passes: every other image (periodic boundaries, half-widths 13 .. 32) as two
+// passes -- along x into a plan-owned intermediate, then along y into the output -- with the
+// register-window line kernels of the fast float path (k_line.cu), per-image tables and work
+// lists, one launch per pass and half-width bucket (4, 8, 16, 32).  Taps come from the weight
+// bank per work item (zero beyond the image's half-width).
+
+struct BLImage {
+   float const* src;
+   float* dst;
+   float* tmp;              // n0 x n1 intermediate (dense rows)
+   int64_t ss1, ds1;        // source and destination row strides (x stride 1)
+   int32_t n0, n1;
+   int32_t h[ 2 ], odd[ 2 ], bc[ 2 ], wofs[ 2 ];
+   int32_t nseg;            // x pass: segments of 512 outputs per row
+   int32_t ncb;             // y pass: column blocks of 128 per row block
+};
+
+struct BLArgs {
+   BLImage const* images;
+   BatchItem const* items;
+   float const* wbank;
+   int32_t* status;
+   int32_t nimages;
+   int32_t nitems;
+};
+
+constexpr int kBLBuckets[ 4 ] = { 4, 8, 16, 32 };
+constexpr int kBLT = 512;    // x pass: outputs per item
+constexpr int kBLR = 16;     // y pass: rows per item
+
+// Sample j of a line (base, stride st, length n), extended with the boundary condition.
+__device__ __forceinline__ float bl_load( float const* base, int64_t st, int64_t j, int64_t n, int32_t bc ) {
+   if( j >= 0 && j < n ) { return __ldg( base + j * st ); }
+   if( bc == BC_ADD_ZEROS ) { return 0.f; }
+   bool neg;
+   int64_t const i = bc_map_index( j, n, bc, &neg );
+   float const v = __ldg( base + i * st );
+   return neg ? -v : v;
+}
+
+template< int HB >
+__global__ void __launch_bounds__( 128 ) batch_line_x_kernel( BLArgs const __grid_constant__ a ) {
+   constexpr int W = kBLT + 2 * HB;
+   constexpr int RX = kBLT / 128;
+   __shared__ __align__( 16 ) float tile[ ( W + 3 ) / 4 * 4 ];
+   __shared__ float ws[ HB + 1 ];
+   int const tid = static_cast< int >( threadIdx.x );
+   for( int64_t t = blockIdx.x; t < a.nitems; t += gridDim.x ) {
+      BatchItem const it = a.items[ t ];
+      BLImage const* im = ( it.image >= 0 && it.image < a.nimages ) ? a.images + it.image : nullptr;
+      if( !im || it.tile < 0 || it.tile >= im->n1 * im->nseg ) {   // uniform over the CTA
+         if( tid == 0 ) { atomicExch( a.status, DIPCU_ERR_INVALID_ARG ); }
+         continue;
+      }
+      int const row = it.tile / im->nseg, seg = it.tile - row * im->nseg;
+      int64_t const a0 = static_cast< int64_t >( seg ) * kBLT, n = im->n0;
+      int32_t const bc = im->bc[ 0 ];
+      float const* srow = im->src + static_cast< int64_t >( row ) * im->ss1;
+      if( tid <= HB ) { ws[ tid ] = tid <= im->h[ 0 ] ? __ldg( a.wbank + im->wofs[ 0 ] + tid ) : 0.f; }
+      for( int e = tid; e < W; e += 128 ) { tile[ e ] = bl_load( srow, 1, a0 - HB + e, n, bc ); }
+      __syncthreads();
+      float v[ RX + 2 * HB + 4 ];
+      float4 const* w4 = reinterpret_cast< float4 const* >( tile + tid * RX );
+#pragma unroll
+      for( int q = 0; q < ( RX + 2 * HB + 3 ) / 4; ++q ) {
+         float4 const f = w4[ q ];
+         v[ 4 * q ] = f.x; v[ 4 * q + 1 ] = f.y; v[ 4 * q + 2 ] = f.z; v[ 4 * q + 3 ] = f.w;
+      }
+      float const sg = im->odd[ 0 ] ? -1.f : 1.f;
+      float acc[ RX ];
+#pragma unroll
+      for( int r = 0; r < RX; ++r ) { acc[ r ] = ws[ 0 ] * v[ HB + r ]; }   // the centre tap is 0 for odd kernels
+#pragma unroll
+      for( int k = 1; k <= HB; ++k ) {
+         float const w = ws[ k ];
+#pragma unroll
+         for( int r = 0; r < RX; ++r ) { acc[ r ] = fmaf( w, fmaf( sg, v[ HB + r - k ], v[ HB + r + k ] ), acc[ r ] ); }
+      }
+      float* const trow = im->tmp + static_cast< int64_t >( row ) * n;
+#pragma unroll
+      for( int r = 0; r < RX; ++r ) {
+         int64_t const i = a0 + tid * RX + r;
+         if( i < n ) { trow[ i ] = acc[ r ]; }
+      }
+      __syncthreads();   // tile and taps are rewritten by the next item
+   }
+}
+
+template< int HB >
+__global__ void __launch_bounds__( 128 ) batch_line_y_kernel( BLArgs const __grid_constant__ a ) {
+   __shared__ float ws[ HB + 1 ];
+   int const tid = static_cast< int >( threadIdx.x );
+   for( int64_t t = blockIdx.x; t < a.nitems; t += gridDim.x ) {
+      BatchItem const it = a.items[ t ];
+      BLImage const* im = ( it.image >= 0 && it.image < a.nimages ) ? a.images + it.image : nullptr;
+      int const nrb = im ? ( im->n1 + kBLR - 1 ) / kBLR : 0;
+      if( !im || it.tile < 0 || it.tile >= im->ncb * nrb ) {   // uniform over the CTA
+         if( tid == 0 ) { atomicExch( a.status, DIPCU_ERR_INVALID_ARG ); }
+         continue;
+      }
+      __syncthreads();   // the previous item's tap reads are done
+      if( tid <= HB ) { ws[ tid ] = tid <= im->h[ 1 ] ? __ldg( a.wbank + im->wofs[ 1 ] + tid ) : 0.f; }
+      __syncthreads();
+      int const rb = it.tile / im->ncb, cb = it.tile - rb * im->ncb;
+      int64_t const c = static_cast< int64_t >( cb ) * 128 + tid;
+      if( c >= im->n0 ) { continue; }
+      int64_t const n = im->n1, n0 = im->n0, i0 = static_cast< int64_t >( rb ) * kBLR;
+      int32_t const bc = im->bc[ 1 ];
+      float const* col = im->tmp + c;
+      float v[ kBLR + 2 * HB ];
+      if( i0 - HB >= 0 && i0 + kBLR + HB <= n ) {
+         float const* p = col + ( i0 - HB ) * n0;
+#pragma unroll
+         for( int j = 0; j < kBLR + 2 * HB; ++j ) { v[ j ] = __ldg( p + j * n0 ); }
+      } else {
+#pragma unroll
+         for( int j = 0; j < kBLR + 2 * HB; ++j ) { v[ j ] = bl_load( col, n0, i0 - HB + j, n, bc ); }
+      }
+      float const sg = im->odd[ 1 ] ? -1.f : 1.f;
+      float acc[ kBLR ];
+#pragma unroll
+      for( int r = 0; r < kBLR; ++r ) { acc[ r ] = ws[ 0 ] * v[ HB + r ]; }
+#pragma unroll
+      for( int k = 1; k <= HB; ++k ) {
+         float const w = ws[ k ];
+#pragma unroll
+         for( int r = 0; r < kBLR; ++r ) { acc[ r ] = fmaf( w, fmaf( sg, v[ HB + r - k ], v[ HB + r + k ] ), acc[ r ] ); }
+      }
+      float* const dcol = im->dst + c;
+#pragma unroll
+      for( int r = 0; r < kBLR; ++r ) {
+         int64_t const i = i0 + r;
+         if( i < n ) { dcol[ i * im->ds1 ] = acc[ r ]; }
+      }
+   }
+}
+
+cudaError_t bl_launch( int b, bool ypass, BLArgs const& a, cudaStream_t st ) {
+   int64_t g = a.nitems < 148 * 8 ? a.nitems : 148 * 8;
+   if( g < 1 ) { g = 1; }
+   unsigned const grid = static_cast< unsigned >( g );
+   switch( b ) {
+      case 0: if( ypass ) { batch_line_y_kernel< 4 ><<< grid, 128, 0, st >>>( a ); } else { batch_line_x_kernel< 4 ><<< grid, 128, 0, st >>>( a ); } break;
+      case 1: if( ypass ) { batch_line_y_kernel< 8 ><<< grid, 128, 0, st >>>( a ); } else { batch_line_x_kernel< 8 ><<< grid, 128, 0, st >>>( a ); } break;
+      case 2: if( ypass ) { batch_line_y_kernel< 16 ><<< grid, 128, 0, st >>>( a ); } else { batch_line_x_kernel< 16 ><<< grid, 128, 0, st >>>( a ); } break;
+      default: if( ypass ) { batch_line_y_kernel< 32 ><<< grid, 128, 0, st >>>( a ); } else { batch_line_x_kernel< 32 ><<< grid, 128, 0, st >>>( a ); } break;
+   }
+   return cudaGetLastError();
+}
+
 // Candidate tile shapes (the autotuner's search space).
 struct TileShape { int tx, ty; };
 constexpr TileShape kShapes[ 3 ] = { { 64, 32 }, { 64, 16 }, { 128, 32 } };
@@ -678,6 +828,16 @@ struct dipcu_batch_plan {
    G2Image* d_gimg[ 4 ] = {};
    BatchItem* d_gitems[ 4 ] = {};
    int g_nimg[ 4 ] = {}, g_nitems[ 4 ] = {}, g_grid[ 4 ] = {};
+   // Grouped line passes, per half-width bucket (4, 8, 16, 32), and their intermediate.
+   BLImage* d_limg[ 4 ] = {};
+   BatchItem* d_lxitems[ 4 ] = {};
+   BatchItem* d_lyitems[ 4 ] = {};
+   int l_nimg[ 4 ] = {}, l_nx[ 4 ] = {}, l_ny[ 4 ] = {};
+   float* d_tmp = nullptr;
+   // Fork / join of the per-bucket launches: bucket b runs on side[b], concurrently with the
+   // other buckets and the persistent kernel (parallel branches of the captured graph).
+   cudaStream_t side[ 4 ] = {};
+   cudaEvent_t ev_fork = nullptr, ev_join[ 4 ] = {};
    cudaStream_t cap_stream = nullptr;
    cudaGraph_t graph = nullptr;
    cudaGraphExec_t exec = nullptr;
@@ -695,7 +855,7 @@ int plan_fail( int code, std::string const& msg ) { return record_error( code, m
 // kernel gets no items of its own.
 int plan_groups( dipcu_batch_plan* p, int inject ) {
    p->gbucket.assign( static_cast< size_t >( p->count ), -1 );
-   if( getenv( "DIPCU_BATCH_NO_WS" )) { return DIPCU_OK; }
+   bool const no_ws = getenv( "DIPCU_BATCH_NO_WS" ) != nullptr;
    std::vector< G2Image > gimg[ 4 ];
    std::vector< BatchItem > gitems[ 4 ];
    int rest = 0;
@@ -703,7 +863,7 @@ int plan_groups( dipcu_batch_plan* p, int inject ) {
       BatchImage const& im = p->images[ static_cast< size_t >( i ) ];
       int const hm = std::max( im.h[ 0 ], im.h[ 1 ] );
       int const b = hm <= 4 ? 0 : hm <= 6 ? 1 : hm <= 9 ? 2 : hm <= 12 ? 3 : -1;
-      bool ok = b >= 0 && ( reinterpret_cast< uintptr_t >( im.src ) & 3 ) == 0 && im.ss[ 1 ] > 0 && im.ds[ 1 ] > 0 &&
+      bool ok = !no_ws && b >= 0 && ( reinterpret_cast< uintptr_t >( im.src ) & 3 ) == 0 && im.ss[ 1 ] > 0 && im.ds[ 1 ] > 0 &&
                 im.n[ 0 ] < ( 1 << 30 ) && im.n[ 1 ] < ( 1 << 30 );
       for( int d = 0; d < 2 && ok; ++d ) {
          int32_t const bc = im.bc[ d ];
@@ -741,11 +901,79 @@ int plan_groups( dipcu_batch_plan* p, int inject ) {
       gimg[ b ].push_back( g );
       p->gbucket[ static_cast< size_t >( i ) ] = b;
    }
+   // The rest: grouped line passes (every batch image qualifies: index-mapping boundary
+   // conditions or "add zeros", half-widths up to 32, unit x stride).
+   std::vector< BLImage > limg[ 4 ];
+   std::vector< BatchItem > lx[ 4 ], ly[ 4 ];
+   std::vector< int64_t > toff[ 4 ];   // intermediate offset of each image, per bucket
+   int64_t ttot = 0;
+   if( !getenv( "DIPCU_BATCH_NO_LINES" )) {
+      for( int i = 0; i < p->count; ++i ) {
+         if( p->gbucket[ static_cast< size_t >( i ) ] >= 0 ) { continue; }
+         BatchImage const& im = p->images[ static_cast< size_t >( i ) ];
+         int const hm = std::max( im.h[ 0 ], im.h[ 1 ] );
+         if( hm > 32 || ( reinterpret_cast< uintptr_t >( im.src ) & 3 ) || im.n[ 0 ] >= ( 1 << 30 ) || im.n[ 1 ] >= ( 1 << 30 )) { continue; }
+         int const lb = hm <= 4 ? 0 : hm <= 8 ? 1 : hm <= 16 ? 2 : 3;
+         BLImage l{};
+         l.src = im.src;
+         l.dst = im.dst;
+         l.ss1 = im.ss[ 1 ];
+         l.ds1 = im.ds[ 1 ];
+         l.n0 = static_cast< int32_t >( im.n[ 0 ] );
+         l.n1 = static_cast< int32_t >( im.n[ 1 ] );
+         for( int d = 0; d < 2; ++d ) {
+            l.h[ d ] = im.h[ d ];
+            l.odd[ d ] = im.odd[ d ];
+            l.bc[ d ] = im.bc[ d ];
+            l.wofs[ d ] = im.wofs[ d ];
+         }
+         l.nseg = ( l.n0 + kBLT - 1 ) / kBLT;
+         l.ncb = ( l.n0 + 127 ) / 128;
+         int const nrb = ( l.n1 + kBLR - 1 ) / kBLR;
+         int const li = static_cast< int >( limg[ lb ].size());
+         for( int t = 0; t < l.n1 * l.nseg; ++t ) { lx[ lb ].push_back( BatchItem{ li, t } ); }
+         for( int t = 0; t < l.ncb * nrb; ++t ) { ly[ lb ].push_back( BatchItem{ li, t } ); }
+         toff[ lb ].push_back( ttot );
+         ttot += static_cast< int64_t >( l.n0 ) * l.n1;
+         limg[ lb ].push_back( l );
+         p->gbucket[ static_cast< size_t >( i ) ] = 4 + lb;
+         --rest;
+      }
+   }
    if( inject && rest == 0 ) {
+      bool done = false;
       for( auto& v : gitems ) {
          if( v.empty()) { continue; }
          if( inject == 1 ) { v[ v.size() / 2 ].image = 1 << 20; } else { v[ v.size() / 2 ].tile = 1 << 30; }
+         done = true;
          break;
+      }
+      for( int b = 0; b < 4 && !done; ++b ) {
+         if( ly[ b ].empty()) { continue; }
+         if( inject == 1 ) { ly[ b ][ ly[ b ].size() / 2 ].image = 1 << 20; } else { ly[ b ][ ly[ b ].size() / 2 ].tile = 1 << 30; }
+         done = true;
+      }
+   }
+   if( ttot > 0 ) {
+      if( cudaMalloc( &p->d_tmp, sizeof( float ) * static_cast< size_t >( ttot )) != cudaSuccess ) {
+         return plan_fail( DIPCU_ERR_CUDA, "batch plan: line-pass intermediate" );
+      }
+      for( int b = 0; b < 4; ++b ) {
+         for( size_t k = 0; k < limg[ b ].size(); ++k ) { limg[ b ][ k ].tmp = p->d_tmp + toff[ b ][ k ]; }
+      }
+   }
+   for( int b = 0; b < 4; ++b ) {
+      p->l_nimg[ b ] = static_cast< int >( limg[ b ].size());
+      p->l_nx[ b ] = static_cast< int >( lx[ b ].size());
+      p->l_ny[ b ] = static_cast< int >( ly[ b ].size());
+      if( limg[ b ].empty()) { continue; }
+      if( cudaMalloc( &p->d_limg[ b ], sizeof( BLImage ) * limg[ b ].size()) != cudaSuccess ||
+          cudaMalloc( &p->d_lxitems[ b ], sizeof( BatchItem ) * lx[ b ].size()) != cudaSuccess ||
+          cudaMalloc( &p->d_lyitems[ b ], sizeof( BatchItem ) * ly[ b ].size()) != cudaSuccess ||
+          cudaMemcpy( p->d_limg[ b ], limg[ b ].data(), sizeof( BLImage ) * limg[ b ].size(), cudaMemcpyHostToDevice ) != cudaSuccess ||
+          cudaMemcpy( p->d_lxitems[ b ], lx[ b ].data(), sizeof( BatchItem ) * lx[ b ].size(), cudaMemcpyHostToDevice ) != cudaSuccess ||
+          cudaMemcpy( p->d_lyitems[ b ], ly[ b ].data(), sizeof( BatchItem ) * ly[ b ].size(), cudaMemcpyHostToDevice ) != cudaSuccess ) {
+         return plan_fail( DIPCU_ERR_CUDA, "batch plan: line-pass tables" );
       }
    }
    for( int b = 0; b < 4; ++b ) {
@@ -803,6 +1031,7 @@ int enqueue_run( dipcu_batch_plan* p, cudaStream_t st ) {
    cudaError_t e = launch_gauss_weights( p->d_sigmas, p->d_orders, 2 * p->count, p->truncation, p->d_bank, nullptr,
                                          nullptr, kBankStride, st );
    if( e != cudaSuccess ) { return plan_fail( DIPCU_ERR_CUDA, "gauss_weights_kernel" ); }
+   if( cudaEventRecord( p->ev_fork, st ) != cudaSuccess ) { return plan_fail( DIPCU_ERR_CUDA, "batch fork" ); }
    if( p->nitems > 0 ) {
       BatchArgs a{};
       a.images = p->d_images;
@@ -816,16 +1045,39 @@ int enqueue_run( dipcu_batch_plan* p, cudaStream_t st ) {
       if( e != cudaSuccess ) { return plan_fail( DIPCU_ERR_CUDA, std::string( "batch_kernel: " ) + cudaGetErrorString( e )); }
    }
    for( int b = 0; b < 4; ++b ) {
-      if( p->g_nitems[ b ] == 0 ) { continue; }
-      G2Args g{};
-      g.images = p->d_gimg[ b ];
-      g.items = p->d_gitems[ b ];
-      g.wbank = p->d_bank;
-      g.status = device_status_ptr();
-      g.nimages = p->g_nimg[ b ];
-      g.nitems = p->g_nitems[ b ];
-      e = g2_launch( b, g, std::min( p->g_grid[ b ], std::max( 1, p->g_nitems[ b ] / 4 )), st );
-      if( e != cudaSuccess ) { return plan_fail( DIPCU_ERR_CUDA, std::string( "batch_ws_kernel: " ) + cudaGetErrorString( e )); }
+      if( p->g_nitems[ b ] == 0 && p->l_nimg[ b ] == 0 ) { continue; }
+      cudaStream_t const sb = p->side[ b ];
+      if( cudaStreamWaitEvent( sb, p->ev_fork, 0 ) != cudaSuccess ) { return plan_fail( DIPCU_ERR_CUDA, "batch fork" ); }
+      if( p->g_nitems[ b ] > 0 ) {
+         G2Args g{};
+         g.images = p->d_gimg[ b ];
+         g.items = p->d_gitems[ b ];
+         g.wbank = p->d_bank;
+         g.status = device_status_ptr();
+         g.nimages = p->g_nimg[ b ];
+         g.nitems = p->g_nitems[ b ];
+         e = g2_launch( b, g, std::min( p->g_grid[ b ], std::max( 1, p->g_nitems[ b ] / 4 )), sb );
+         if( e != cudaSuccess ) { return plan_fail( DIPCU_ERR_CUDA, std::string( "batch_ws_kernel: " ) + cudaGetErrorString( e )); }
+      }
+      if( p->l_nimg[ b ] > 0 ) {
+         BLArgs l{};
+         l.images = p->d_limg[ b ];
+         l.wbank = p->d_bank;
+         l.status = device_status_ptr();
+         l.nimages = p->l_nimg[ b ];
+         l.items = p->d_lxitems[ b ];
+         l.nitems = p->l_nx[ b ];
+         e = bl_launch( b, false, l, sb );
+         if( e == cudaSuccess ) {
+            l.items = p->d_lyitems[ b ];
+            l.nitems = p->l_ny[ b ];
+            e = bl_launch( b, true, l, sb );
+         }
+         if( e != cudaSuccess ) { return plan_fail( DIPCU_ERR_CUDA, std::string( "batch line passes: " ) + cudaGetErrorString( e )); }
+      }
+      if( cudaEventRecord( p->ev_join[ b ], sb ) != cudaSuccess || cudaStreamWaitEvent( st, p->ev_join[ b ], 0 ) != cudaSuccess ) {
+         return plan_fail( DIPCU_ERR_CUDA, "batch join" );
+      }
    }
    return DIPCU_OK;
 }
@@ -911,6 +1163,12 @@ int dipcu_batch_plan_create( dipcu_image_desc const* ins, dipcu_image_desc const
       return plan_fail( DIPCU_ERR_CUDA, "device status word" );
    }
    if( int st = plan_groups( p, inject )) { dipcu_batch_plan_destroy( p ); return st; }
+   bool sok = cudaEventCreateWithFlags( &p->ev_fork, cudaEventDisableTiming ) == cudaSuccess;
+   for( int b = 0; b < 4 && sok; ++b ) {
+      sok = cudaStreamCreateWithFlags( &p->side[ b ], cudaStreamNonBlocking ) == cudaSuccess &&
+            cudaEventCreateWithFlags( &p->ev_join[ b ], cudaEventDisableTiming ) == cudaSuccess;
+   }
+   if( !sok ) { dipcu_batch_plan_destroy( p ); return plan_fail( DIPCU_ERR_CUDA, "batch plan: streams" ); }
    // Tile shape: the autotuner times every candidate on this batch (the filter outputs are
    // overwritten by the final runs), remembering the winner per batch signature.
    int shape = 0;
@@ -974,7 +1232,7 @@ int dipcu_batch_plan_info( dipcu_batch_plan const* plan, int* nitems, int* tile_
    if( !plan ) { return plan_fail( DIPCU_ERR_INVALID_ARG, "null plan" ); }
    if( nitems ) {
       *nitems = plan->nitems;
-      for( int b = 0; b < 4; ++b ) { *nitems += plan->g_nitems[ b ]; }
+      for( int b = 0; b < 4; ++b ) { *nitems += plan->g_nitems[ b ] + plan->l_nx[ b ] + plan->l_ny[ b ]; }
    }
    if( tile_x ) { *tile_x = kShapes[ plan->shape ].tx; }
    if( tile_y ) { *tile_y = kShapes[ plan->shape ].ty; }
@@ -986,8 +1244,8 @@ int dipcu_batch_plan_launches( dipcu_batch_plan const* plan, int* kernels, int* 
    if( !plan ) { return plan_fail( DIPCU_ERR_INVALID_ARG, "null plan" ); }
    int k = 1 + ( plan->nitems > 0 ? 1 : 0 ), g = 0;
    for( int b = 0; b < 4; ++b ) {
-      k += plan->g_nitems[ b ] > 0 ? 1 : 0;
-      g += plan->g_nitems[ b ];
+      k += ( plan->g_nitems[ b ] > 0 ? 1 : 0 ) + ( plan->l_nimg[ b ] > 0 ? 2 : 0 );
+      g += plan->g_nitems[ b ] + plan->l_nx[ b ] + plan->l_ny[ b ];
    }
    if( kernels ) { *kernels = k; }
    if( grouped_items ) { *grouped_items = g; }
@@ -1011,7 +1269,16 @@ int dipcu_batch_plan_destroy( dipcu_batch_plan* plan ) {
    for( int b = 0; b < 4; ++b ) {
       cudaFree( plan->d_gimg[ b ] );
       cudaFree( plan->d_gitems[ b ] );
+      cudaFree( plan->d_limg[ b ] );
+      cudaFree( plan->d_lxitems[ b ] );
+      cudaFree( plan->d_lyitems[ b ] );
    }
+   cudaFree( plan->d_tmp );
+   for( int b = 0; b < 4; ++b ) {
+      if( plan->side[ b ] ) { cudaStreamDestroy( plan->side[ b ] ); }
+      if( plan->ev_join[ b ] ) { cudaEventDestroy( plan->ev_join[ b ] ); }
+   }
+   if( plan->ev_fork ) { cudaEventDestroy( plan->ev_fork ); }
    delete plan;
    return DIPCU_OK;
 }
