@@ -142,16 +142,18 @@ int dipcu_structure_tensor_backward( dipcu_image_desc const* grad_out, dipcu_ima
  * boundary conditions (the index-mapping ones and "add zeros"; half-widths up to 32).  Images
  * with both half-widths up to 12 and "mirror", "zero order", "add zeros" or "asym mirror" along
  * both axes run through grouped warp-per-tile launches (one per half-width bucket, per-image work
- * lists); the others through one persistent launch that pulls (image, tile) work items from a
- * device queue.  No DIPlib counterpart (DIPlib filters one image per call; this is
- * dip::GaussFIR per image).
+ * lists); the others through grouped line passes (along x into an intermediate the plan owns,
+ * then along y; one pair of launches per half-width bucket); the buckets run as parallel
+ * branches.  A persistent launch that pulls (image, tile) work items from a device queue remains
+ * as the fallback (DIPCU_BATCH_NO_LINES routes the rest there).  No DIPlib counterpart (DIPlib
+ * filters one image per call; this is dip::GaussFIR per image).
  * `sigmas`, `orders`, `bcs`: host arrays of 2 * count entries (x then y of each image).
  * Flags: DIPCU_BATCH_GRAPH captures the run (queue reset, on-device weights, all launches)
  * into a CUDA graph so that dipcu_batch_plan_run is one graph launch; DIPCU_BATCH_AUTOTUNE times
- * the candidate tile shapes on this batch at creation (overwriting the outputs) and keeps the
+ * the persistent kernel's candidate tile shapes on this batch at creation (overwriting the outputs) and keeps the
  * fastest, remembered per batch signature.  The two INJECT flags are test hooks that plant one
  * impossible work item, which the kernels skip and report through dipcu_device_status.
- * The plan allocates its tables at creation; runs allocate nothing.  The images must stay alive
+ * The plan allocates its tables and the line-pass intermediate at creation; runs allocate nothing.  The images must stay alive
  * while the plan is used.  The sigma table (dipcu_batch_plan_sigmas, device, 2 * count doubles)
  * may be rewritten between runs, as long as no kernel length changes. */
 typedef struct dipcu_batch_plan dipcu_batch_plan;
