@@ -4,8 +4,9 @@
 // Gaussian method and no mask: the gradient g_k = GaussFIR(in, sigma_g, order e_k) along each
 // axis of size > 1 (dip::Gradient, src/linear/derivative.cpp:142-172), the symmetric products
 // g_i g_j in DIPlib's symmetric-matrix order (diagonal first, then the upper triangle row by row;
-// dip::Multiply( g, Transpose( g ))), and each product smoothed by GaussFIR(sigma_t).  Products are
-// formed per component and smoothed immediately, so at most one product image exists at a time.
+// dip::Multiply( g, Transpose( g ))), and each product smoothed by GaussFIR(sigma_t).  The
+// products are formed together and smoothed by one call over the component axis; when that much
+// scratch is not available, per component (at most one product image at a time).
 //
 // Backward (no DIPlib counterpart): for L = sum_c <W_c, T_c>,
 //   Q_c = S^T W_c (the smoothing's adjoint),
@@ -172,9 +173,36 @@ int dipcu_structure_tensor( dipcu_image_desc const* in, dipcu_image_desc const* 
       g.push_back( sc.get( bytes ));
       if( !g.back() ) { return record_error( DIPCU_ERR_CUDA, "cudaMallocAsync (gradient)" ); }
    }
-   void* prod = sc.get( bytes );
-   if( !prod ) { return record_error( DIPCU_ERR_CUDA, "cudaMallocAsync (product)" ); }
+   // All products at once, smoothed by one call with the components as an unfiltered batch axis
+   // (one launch of the tile kernel instead of one per component); where that buffer does not
+   // fit, one product at a time.
+   size_t const nc = s.comps.size();
+   void* prod_all = nc > 1 ? sc.get( bytes * nc ) : nullptr;
+   if( !prod_all ) { cudaGetLastError(); }   // a failed allocation is not a launch error
+   void* prod = prod_all ? nullptr : sc.get( bytes );
+   if( !prod_all && !prod ) { return record_error( DIPCU_ERR_CUDA, "cudaMallocAsync (product)" ); }
    if( int st = gradients( in, s, grad_sigmas, bcs, truncation, g, stream )) { return st; }
+   if( prod_all ) {
+      for( size_t c = 0; c < nc; ++c ) {
+         cudaError_t e = elementwise( s.cdouble, static_cast< char* >( prod_all ) + c * bytes,
+                                      g[ static_cast< size_t >( s.comps[ c ].first ) ], g[ static_cast< size_t >( s.comps[ c ].second ) ],
+                                      1.0, s.n, 0, stream );
+         if( e != cudaSuccess ) { return record_error( DIPCU_ERR_CUDA, cudaGetErrorString( e )); }
+      }
+      dipcu_image_desc pall = s.plain;
+      pall.ndims = s.nd + 1;
+      pall.data = prod_all;
+      pall.sizes[ s.nd ] = static_cast< int64_t >( nc );
+      pall.strides[ s.nd ] = s.n;
+      std::vector< double > sig( tensor_sigmas, tensor_sigmas + s.nd );
+      sig.push_back( 0.0 );
+      std::vector< uint32_t > ord0( static_cast< size_t >( s.nd + 1 ), 0u );
+      std::vector< int32_t > bc( bcs, bcs + s.nd );
+      bc.push_back( bcs[ 0 ] );
+      std::vector< AxisFilter > f4;
+      if( int st = build_filters( &pall, sig.data(), ord0.data(), bc.data(), truncation, f4, nullptr )) { return st; }
+      return run_filters( &pall, out, f4, s.cdouble, stream );
+   }
    std::vector< uint32_t > ord( static_cast< size_t >( s.nd ), 0u );
    dipcu_image_desc pimg = s.plain;
    pimg.data = prod;
