@@ -249,19 +249,45 @@ int dipcu_structure_tensor_backward( dipcu_image_desc const* grad_out, dipcu_ima
    std::vector< uint32_t > zero( static_cast< size_t >( s.nd ), 0u );
    dipcu_image_desc qimg = s.plain;
    qimg.data = q;
-   for( size_t c = 0; c < s.comps.size(); ++c ) {
-      dipcu_image_desc wc = component( grad_out, static_cast< int >( c ), s.nd );
-      if( int st = dipcu_gauss_fir_backward( &wc, nullptr, &qimg, nullptr, tensor_sigmas, zero.data(), bcs, truncation,
+   // Q_c of all components by one adjoint call over the component axis (unfiltered batch axis)
+   // where the scratch fits, else per component.
+   size_t const nc = s.comps.size();
+   void* q_all = nc > 1 ? sc.get( bytes * nc ) : nullptr;
+   if( !q_all ) { cudaGetLastError(); }   // a failed allocation is not a launch error
+   if( q_all ) {
+      dipcu_image_desc qa = s.plain;
+      qa.ndims = s.nd + 1;
+      qa.data = q_all;
+      qa.sizes[ s.nd ] = static_cast< int64_t >( nc );
+      qa.strides[ s.nd ] = s.n;
+      std::vector< double > sig( tensor_sigmas, tensor_sigmas + s.nd );
+      sig.push_back( 0.0 );
+      std::vector< uint32_t > zero4( static_cast< size_t >( s.nd + 1 ), 0u );
+      std::vector< int32_t > bc( bcs, bcs + s.nd );
+      bc.push_back( bcs[ 0 ] );
+      if( int st = dipcu_gauss_fir_backward( grad_out, nullptr, &qa, nullptr, sig.data(), zero4.data(), bc.data(), truncation,
                                              stream )) {
          return st;
+      }
+   }
+   for( size_t c = 0; c < nc; ++c ) {
+      void* qc = q;
+      if( q_all ) {
+         qc = static_cast< char* >( q_all ) + c * bytes;
+      } else {
+         dipcu_image_desc wc = component( grad_out, static_cast< int >( c ), s.nd );
+         if( int st = dipcu_gauss_fir_backward( &wc, nullptr, &qimg, nullptr, tensor_sigmas, zero.data(), bcs, truncation,
+                                                stream )) {
+            return st;
+         }
       }
       size_t const i = static_cast< size_t >( s.comps[ c ].first ), j = static_cast< size_t >( s.comps[ c ].second );
       cudaError_t e;
       if( i == j ) {
-         e = elementwise( s.cdouble, gb[ i ], q, g[ i ], 2.0, s.n, 1, stream );
+         e = elementwise( s.cdouble, gb[ i ], qc, g[ i ], 2.0, s.n, 1, stream );
       } else {
-         e = elementwise( s.cdouble, gb[ i ], q, g[ j ], 1.0, s.n, 1, stream );
-         if( e == cudaSuccess ) { e = elementwise( s.cdouble, gb[ j ], q, g[ i ], 1.0, s.n, 1, stream ); }
+         e = elementwise( s.cdouble, gb[ i ], qc, g[ j ], 1.0, s.n, 1, stream );
+         if( e == cudaSuccess ) { e = elementwise( s.cdouble, gb[ j ], qc, g[ i ], 1.0, s.n, 1, stream ); }
       }
       if( e != cudaSuccess ) { return record_error( DIPCU_ERR_CUDA, cudaGetErrorString( e )); }
    }
