@@ -632,68 +632,116 @@ __device__ __forceinline__ float bl_load( float const* base, int64_t st, int64_t
    return neg ? -v : v;
 }
 
+// Stages sample j of a line into `dst` (shared memory): an asynchronous 4-byte copy, zero fill
+// for "add zeros", a plain load and store for sources the boundary condition negates.
+__device__ __forceinline__ void bl_stage( float* dst, float const* base, int64_t j, int64_t n, int32_t bc ) {
+   float const* src = base;
+   int32_t bytes = 4;
+   if( j >= 0 && j < n ) {
+      src += j;
+   } else if( bc == BC_ADD_ZEROS ) {
+      bytes = 0;
+   } else {
+      bool neg;
+      src += bc_map_index( j, n, bc, &neg );
+      if( neg ) {
+         *dst = -__ldg( src );
+         return;
+      }
+   }
+   asm volatile( "cp.async.ca.shared.global [%0], [%1], 4, %2;" :: "r"( smem_u32( dst )), "l"( src ), "r"( bytes ) : "memory" );
+}
+
 template< int HB >
 __global__ void __launch_bounds__( 128 ) batch_line_x_kernel( BLArgs const __grid_constant__ a ) {
-   constexpr int W = kBLT + 2 * HB;
+   constexpr int W = kBLT + 2 * HB, WP = ( W + 3 ) / 4 * 4;
    constexpr int RX = kBLT / 128;
-   __shared__ __align__( 16 ) float tile[ ( W + 3 ) / 4 * 4 ];
-   __shared__ float ws[ HB + 1 ];
+   __shared__ __align__( 16 ) float tile[ 2 ][ WP ];
+   __shared__ float ws[ 2 ][ HB + 1 ];
    int const tid = static_cast< int >( threadIdx.x );
-   for( int64_t t = blockIdx.x; t < a.nitems; t += gridDim.x ) {
+   // Item t's image, row and segment start, or null for an item that names no image or row.
+   auto lookup = [ & ]( int64_t t, int& row, int64_t& a0 ) -> BLImage const* {
       BatchItem const it = a.items[ t ];
       BLImage const* im = ( it.image >= 0 && it.image < a.nimages ) ? a.images + it.image : nullptr;
-      if( !im || it.tile < 0 || it.tile >= im->n1 * im->nseg ) {   // uniform over the CTA
-         if( tid == 0 ) { atomicExch( a.status, DIPCU_ERR_INVALID_ARG ); }
-         continue;
+      if( !im || it.tile < 0 || it.tile >= im->n1 * im->nseg ) { return nullptr; }
+      row = it.tile / im->nseg;
+      a0 = static_cast< int64_t >( it.tile - row * im->nseg ) * kBLT;
+      return im;
+   };
+   // Double-buffered: the copies of the next item land while this one is filtered.
+   auto issue = [ & ]( int64_t t, int buf ) {
+      if( t < a.nitems ) {
+         int row;
+         int64_t a0;
+         BLImage const* im = lookup( t, row, a0 );
+         if( im ) {
+            if( tid <= HB ) { ws[ buf ][ tid ] = tid <= im->h[ 0 ] ? __ldg( a.wbank + im->wofs[ 0 ] + tid ) : 0.f; }
+            float const* srow = im->src + static_cast< int64_t >( row ) * im->ss1;
+            for( int e = tid; e < W; e += 128 ) { bl_stage( &tile[ buf ][ e ], srow, a0 - HB + e, im->n0, im->bc[ 0 ] ); }
+         }
       }
-      int const row = it.tile / im->nseg, seg = it.tile - row * im->nseg;
-      int64_t const a0 = static_cast< int64_t >( seg ) * kBLT, n = im->n0;
-      int32_t const bc = im->bc[ 0 ];
-      float const* srow = im->src + static_cast< int64_t >( row ) * im->ss1;
-      if( tid <= HB ) { ws[ tid ] = tid <= im->h[ 0 ] ? __ldg( a.wbank + im->wofs[ 0 ] + tid ) : 0.f; }
-      for( int e = tid; e < W; e += 128 ) { tile[ e ] = bl_load( srow, 1, a0 - HB + e, n, bc ); }
+      asm volatile( "cp.async.commit_group;" ::: "memory" );
+   };
+   issue( blockIdx.x, 0 );
+   int k = 0;
+   for( int64_t t = blockIdx.x; t < a.nitems; t += gridDim.x, ++k ) {
+      int const buf = k & 1;
+      issue( t + gridDim.x, buf ^ 1 );
+      asm volatile( "cp.async.wait_group 1;" ::: "memory" );
       __syncthreads();
-      float v[ RX + 2 * HB + 4 ];
-      float4 const* w4 = reinterpret_cast< float4 const* >( tile + tid * RX );
+      int row;
+      int64_t a0;
+      BLImage const* im = lookup( t, row, a0 );
+      if( !im ) {   // uniform over the CTA
+         if( tid == 0 ) { atomicExch( a.status, DIPCU_ERR_INVALID_ARG ); }
+      } else {
+         int64_t const n = im->n0;
+         float v[ RX + 2 * HB + 4 ];
+         float4 const* w4 = reinterpret_cast< float4 const* >( tile[ buf ] + tid * RX );
 #pragma unroll
-      for( int q = 0; q < ( RX + 2 * HB + 3 ) / 4; ++q ) {
-         float4 const f = w4[ q ];
-         v[ 4 * q ] = f.x; v[ 4 * q + 1 ] = f.y; v[ 4 * q + 2 ] = f.z; v[ 4 * q + 3 ] = f.w;
+         for( int q = 0; q < ( RX + 2 * HB + 3 ) / 4; ++q ) {
+            float4 const f = w4[ q ];
+            v[ 4 * q ] = f.x; v[ 4 * q + 1 ] = f.y; v[ 4 * q + 2 ] = f.z; v[ 4 * q + 3 ] = f.w;
+         }
+         float const sg = im->odd[ 0 ] ? -1.f : 1.f;
+         float acc[ RX ];
+#pragma unroll
+         for( int r = 0; r < RX; ++r ) { acc[ r ] = ws[ buf ][ 0 ] * v[ HB + r ]; }   // the centre tap is 0 for odd kernels
+#pragma unroll
+         for( int kk = 1; kk <= HB; ++kk ) {
+            float const w = ws[ buf ][ kk ];
+#pragma unroll
+            for( int r = 0; r < RX; ++r ) { acc[ r ] = fmaf( w, fmaf( sg, v[ HB + r - kk ], v[ HB + r + kk ] ), acc[ r ] ); }
+         }
+         float* const trow = im->tmp + static_cast< int64_t >( row ) * n;
+#pragma unroll
+         for( int r = 0; r < RX; ++r ) {
+            int64_t const i = a0 + tid * RX + r;
+            if( i < n ) { trow[ i ] = acc[ r ]; }
+         }
       }
-      float const sg = im->odd[ 0 ] ? -1.f : 1.f;
-      float acc[ RX ];
-#pragma unroll
-      for( int r = 0; r < RX; ++r ) { acc[ r ] = ws[ 0 ] * v[ HB + r ]; }   // the centre tap is 0 for odd kernels
-#pragma unroll
-      for( int k = 1; k <= HB; ++k ) {
-         float const w = ws[ k ];
-#pragma unroll
-         for( int r = 0; r < RX; ++r ) { acc[ r ] = fmaf( w, fmaf( sg, v[ HB + r - k ], v[ HB + r + k ] ), acc[ r ] ); }
-      }
-      float* const trow = im->tmp + static_cast< int64_t >( row ) * n;
-#pragma unroll
-      for( int r = 0; r < RX; ++r ) {
-         int64_t const i = a0 + tid * RX + r;
-         if( i < n ) { trow[ i ] = acc[ r ]; }
-      }
-      __syncthreads();   // tile and taps are rewritten by the next item
+      __syncthreads();   // this buffer and its taps are refilled two items later
    }
+   asm volatile( "cp.async.wait_group 0;" ::: "memory" );
 }
 
 template< int HB >
 __global__ void __launch_bounds__( 128 ) batch_line_y_kernel( BLArgs const __grid_constant__ a ) {
-   __shared__ float ws[ HB + 1 ];
+   __shared__ float ws[ 2 ][ HB + 1 ];   // taps of the current and the next item
    int const tid = static_cast< int >( threadIdx.x );
-   for( int64_t t = blockIdx.x; t < a.nitems; t += gridDim.x ) {
+   int k = 0;
+   for( int64_t t = blockIdx.x; t < a.nitems; t += gridDim.x, ++k ) {
+      float* const wk = ws[ k & 1 ];
       BatchItem const it = a.items[ t ];
       BLImage const* im = ( it.image >= 0 && it.image < a.nimages ) ? a.images + it.image : nullptr;
       int const nrb = im ? ( im->n1 + kBLR - 1 ) / kBLR : 0;
       if( !im || it.tile < 0 || it.tile >= im->ncb * nrb ) {   // uniform over the CTA
          if( tid == 0 ) { atomicExch( a.status, DIPCU_ERR_INVALID_ARG ); }
+         __syncthreads();   // keeps one barrier per item, so the tap buffers alternate safely
          continue;
       }
-      __syncthreads();   // the previous item's tap reads are done
-      if( tid <= HB ) { ws[ tid ] = tid <= im->h[ 1 ] ? __ldg( a.wbank + im->wofs[ 1 ] + tid ) : 0.f; }
+      // This buffer was last read two items ago, before the previous item's barrier.
+      if( tid <= HB ) { wk[ tid ] = tid <= im->h[ 1 ] ? __ldg( a.wbank + im->wofs[ 1 ] + tid ) : 0.f; }
       __syncthreads();
       int const rb = it.tile / im->ncb, cb = it.tile - rb * im->ncb;
       int64_t const c = static_cast< int64_t >( cb ) * 128 + tid;
@@ -713,12 +761,12 @@ __global__ void __launch_bounds__( 128 ) batch_line_y_kernel( BLArgs const __gri
       float const sg = im->odd[ 1 ] ? -1.f : 1.f;
       float acc[ kBLR ];
 #pragma unroll
-      for( int r = 0; r < kBLR; ++r ) { acc[ r ] = ws[ 0 ] * v[ HB + r ]; }
+      for( int r = 0; r < kBLR; ++r ) { acc[ r ] = wk[ 0 ] * v[ HB + r ]; }
 #pragma unroll
-      for( int k = 1; k <= HB; ++k ) {
-         float const w = ws[ k ];
+      for( int kk = 1; kk <= HB; ++kk ) {
+         float const w = wk[ kk ];
 #pragma unroll
-         for( int r = 0; r < kBLR; ++r ) { acc[ r ] = fmaf( w, fmaf( sg, v[ HB + r - k ], v[ HB + r + k ] ), acc[ r ] ); }
+         for( int r = 0; r < kBLR; ++r ) { acc[ r ] = fmaf( w, fmaf( sg, v[ HB + r - kk ], v[ HB + r + kk ] ), acc[ r ] ); }
       }
       float* const dcol = im->dst + c;
 #pragma unroll

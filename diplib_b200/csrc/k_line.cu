@@ -18,6 +18,7 @@
 
 #include "dipcu_common.cuh"
 #include "dipcu_internal.h"
+#include "tma.cuh"
 
 namespace dipcu {
 
@@ -170,20 +171,54 @@ __device__ __forceinline__ float fast_tap_sum( LineFastArgs const& a, float cons
    return s0 + s1;
 }
 
+// Stages sample j of a line into `dst` (shared memory): an asynchronous 4-byte copy for samples
+// inside the line and for boundary sources that keep their sign, zero fill for "add zeros", a
+// plain load and store for sources the boundary condition negates.
+__device__ __forceinline__ void fast_stage( LineFastArgs const& a, float* dst, int64_t base, int64_t st, int64_t j ) {
+   float const* src = a.src + base;
+   int32_t bytes = 4;
+   if( j >= 0 && j < a.n ) {
+      src += j * st;
+   } else if( a.bc == BC_ADD_ZEROS ) {
+      bytes = 0;
+   } else {
+      bool neg;
+      int64_t const i = bc_map_index( j, a.n, a.bc, &neg );
+      src += i * st;
+      if( neg ) {
+         *dst = -__ldg( src );
+         return;
+      }
+   }
+   asm volatile( "cp.async.ca.shared.global [%0], [%1], 4, %2;" :: "r"( smem_u32( dst )), "l"( src ), "r"( bytes ) : "memory" );
+}
+
 template< int HB, bool ODD >
 __global__ void __launch_bounds__( 128 ) line_x_kernel( LineFastArgs const __grid_constant__ a ) {
-   constexpr int T = 128 * kRX, W = T + 2 * HB;
-   __shared__ __align__( 16 ) float tile[ ( W + 3 ) / 4 * 4 ];
+   constexpr int T = 128 * kRX, W = T + 2 * HB, WP = ( W + 3 ) / 4 * 4;
+   __shared__ __align__( 16 ) float tile[ 2 ][ WP ];
    int const tid = static_cast< int >( threadIdx.x );
    int64_t const a0 = static_cast< int64_t >( blockIdx.x ) * T;
    int64_t const sa = a.sst[ a.axis ], da = a.dstst[ a.axis ];
-   for( int64_t u = blockIdx.y; u < a.nouter; u += gridDim.y ) {
+   // Double-buffered: the copies of the next line segment land while this one is filtered.
+   auto issue = [ & ]( int64_t u, float* buf ) {
+      if( u < a.nouter ) {
+         int64_t sb, db;
+         fast_decode( a, u, sb, db );
+         for( int e = tid; e < W; e += 128 ) { fast_stage( a, buf + e, sb, sa, a0 - HB + e ); }
+      }
+      asm volatile( "cp.async.commit_group;" ::: "memory" );
+   };
+   issue( blockIdx.y, tile[ 0 ] );
+   int k = 0;
+   for( int64_t u = blockIdx.y; u < a.nouter; u += gridDim.y, ++k ) {
+      issue( u + gridDim.y, tile[ ( k + 1 ) & 1 ] );
+      asm volatile( "cp.async.wait_group 1;" ::: "memory" );
+      __syncthreads();
       int64_t sb, db;
       fast_decode( a, u, sb, db );
-      for( int e = tid; e < W; e += 128 ) { tile[ e ] = fast_load( a, sb, sa, a0 - HB + e ); }
-      __syncthreads();
       float v[ kRX + 2 * HB + 4 ];
-      float4 const* w4 = reinterpret_cast< float4 const* >( tile + tid * kRX );
+      float4 const* w4 = reinterpret_cast< float4 const* >( tile[ k & 1 ] + tid * kRX );
 #pragma unroll
       for( int q = 0; q < ( kRX + 2 * HB + 3 ) / 4; ++q ) {
          float4 const f = w4[ q ];
@@ -194,8 +229,9 @@ __global__ void __launch_bounds__( 128 ) line_x_kernel( LineFastArgs const __gri
          int64_t const i = a0 + tid * kRX + r;
          if( i < a.n ) { a.dst[ db + i * da ] = fast_tap_sum< HB, ODD >( a, v + HB + r ); }
       }
-      __syncthreads();
+      __syncthreads();   // this buffer is refilled two segments later
    }
+   asm volatile( "cp.async.wait_group 0;" ::: "memory" );
 }
 
 template< int HB, bool ODD >
