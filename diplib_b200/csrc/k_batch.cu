@@ -619,7 +619,8 @@ struct BLArgs {
 };
 
 constexpr int kBLBuckets[ 4 ] = { 4, 8, 16, 32 };
-constexpr int kBLT = 512;    // x pass: outputs per item
+constexpr int kBLT = 256;    // x pass: outputs per item
+constexpr int kBLXT = 64;    // x pass: threads per CTA (4 outputs each)
 constexpr int kBLR = 16;     // y pass: rows per item
 
 // Sample j of a line (base, stride st, length n), extended with the boundary condition.
@@ -653,9 +654,9 @@ __device__ __forceinline__ void bl_stage( float* dst, float const* base, int64_t
 }
 
 template< int HB >
-__global__ void __launch_bounds__( 128 ) batch_line_x_kernel( BLArgs const __grid_constant__ a ) {
+__global__ void __launch_bounds__( kBLXT ) batch_line_x_kernel( BLArgs const __grid_constant__ a ) {
    constexpr int W = kBLT + 2 * HB, WP = ( W + 3 ) / 4 * 4;
-   constexpr int RX = kBLT / 128;
+   constexpr int RX = kBLT / kBLXT;
    __shared__ __align__( 16 ) float tile[ 2 ][ WP ];
    __shared__ float ws[ 2 ][ HB + 1 ];
    int const tid = static_cast< int >( threadIdx.x );
@@ -677,7 +678,7 @@ __global__ void __launch_bounds__( 128 ) batch_line_x_kernel( BLArgs const __gri
          if( im ) {
             if( tid <= HB ) { ws[ buf ][ tid ] = tid <= im->h[ 0 ] ? __ldg( a.wbank + im->wofs[ 0 ] + tid ) : 0.f; }
             float const* srow = im->src + static_cast< int64_t >( row ) * im->ss1;
-            for( int e = tid; e < W; e += 128 ) { bl_stage( &tile[ buf ][ e ], srow, a0 - HB + e, im->n0, im->bc[ 0 ] ); }
+            for( int e = tid; e < W; e += kBLXT ) { bl_stage( &tile[ buf ][ e ], srow, a0 - HB + e, im->n0, im->bc[ 0 ] ); }
          }
       }
       asm volatile( "cp.async.commit_group;" ::: "memory" );
@@ -778,14 +779,15 @@ __global__ void __launch_bounds__( 128 ) batch_line_y_kernel( BLArgs const __gri
 }
 
 cudaError_t bl_launch( int b, bool ypass, BLArgs const& a, cudaStream_t st ) {
-   int64_t g = a.nitems < 148 * 8 ? a.nitems : 148 * 8;
+   int64_t const cap = ypass ? 148 * 8 : 148 * 16;
+   int64_t g = a.nitems < cap ? a.nitems : cap;
    if( g < 1 ) { g = 1; }
    unsigned const grid = static_cast< unsigned >( g );
    switch( b ) {
-      case 0: if( ypass ) { batch_line_y_kernel< 4 ><<< grid, 128, 0, st >>>( a ); } else { batch_line_x_kernel< 4 ><<< grid, 128, 0, st >>>( a ); } break;
-      case 1: if( ypass ) { batch_line_y_kernel< 8 ><<< grid, 128, 0, st >>>( a ); } else { batch_line_x_kernel< 8 ><<< grid, 128, 0, st >>>( a ); } break;
-      case 2: if( ypass ) { batch_line_y_kernel< 16 ><<< grid, 128, 0, st >>>( a ); } else { batch_line_x_kernel< 16 ><<< grid, 128, 0, st >>>( a ); } break;
-      default: if( ypass ) { batch_line_y_kernel< 32 ><<< grid, 128, 0, st >>>( a ); } else { batch_line_x_kernel< 32 ><<< grid, 128, 0, st >>>( a ); } break;
+      case 0: if( ypass ) { batch_line_y_kernel< 4 ><<< grid, 128, 0, st >>>( a ); } else { batch_line_x_kernel< 4 ><<< grid, kBLXT, 0, st >>>( a ); } break;
+      case 1: if( ypass ) { batch_line_y_kernel< 8 ><<< grid, 128, 0, st >>>( a ); } else { batch_line_x_kernel< 8 ><<< grid, kBLXT, 0, st >>>( a ); } break;
+      case 2: if( ypass ) { batch_line_y_kernel< 16 ><<< grid, 128, 0, st >>>( a ); } else { batch_line_x_kernel< 16 ><<< grid, kBLXT, 0, st >>>( a ); } break;
+      default: if( ypass ) { batch_line_y_kernel< 32 ><<< grid, 128, 0, st >>>( a ); } else { batch_line_x_kernel< 32 ><<< grid, kBLXT, 0, st >>>( a ); } break;
    }
    return cudaGetLastError();
 }
