@@ -113,7 +113,7 @@ __global__ void __launch_bounds__( 256 ) line_pass_kernel( LineArgs< T, MAXH1 > 
 // Float input and output, half-widths up to 32, the index-mapping boundary conditions and "add
 // zeros", and a unit-stride axis in both images: the same pass with the taps unrolled over a
 // compile-time bucket HB >= h (zero beyond h) and register windows.
-//   * Along the unit-stride axis (line_x_kernel): a CTA stages one line segment of 128 R_X outputs
+//   * Along the unit-stride axis (line_x_kernel): a CTA stages one line segment of nt R_X outputs
 //     plus the halo in shared memory (coalesced loads, boundary extension at the line ends); each
 //     thread evaluates R_X consecutive outputs from a float4 window of R_X + 2 HB samples.
 //   * Along any other axis (line_y_kernel): threads run along the unit-stride axis (coalesced),
@@ -195,9 +195,10 @@ __device__ __forceinline__ void fast_stage( LineFastArgs const& a, float* dst, i
 
 template< int HB, bool ODD >
 __global__ void __launch_bounds__( 128 ) line_x_kernel( LineFastArgs const __grid_constant__ a ) {
-   constexpr int T = 128 * kRX, W = T + 2 * HB, WP = ( W + 3 ) / 4 * 4;
+   constexpr int WP = ( 128 * kRX + 2 * HB + 3 ) / 4 * 4;   // tile for the widest CTA (128 threads)
    __shared__ __align__( 16 ) float tile[ 2 ][ WP ];
-   int const tid = static_cast< int >( threadIdx.x );
+   int const tid = static_cast< int >( threadIdx.x ), nt = static_cast< int >( blockDim.x );
+   int const T = nt * kRX, W = T + 2 * HB;
    int64_t const a0 = static_cast< int64_t >( blockIdx.x ) * T;
    int64_t const sa = a.sst[ a.axis ], da = a.dstst[ a.axis ];
    // Double-buffered: the copies of the next line segment land while this one is filtered.
@@ -205,7 +206,7 @@ __global__ void __launch_bounds__( 128 ) line_x_kernel( LineFastArgs const __gri
       if( u < a.nouter ) {
          int64_t sb, db;
          fast_decode( a, u, sb, db );
-         for( int e = tid; e < W; e += 128 ) { fast_stage( a, buf + e, sb, sa, a0 - HB + e ); }
+         for( int e = tid; e < W; e += nt ) { fast_stage( a, buf + e, sb, sa, a0 - HB + e ); }
       }
       asm volatile( "cp.async.commit_group;" ::: "memory" );
    };
@@ -236,7 +237,7 @@ __global__ void __launch_bounds__( 128 ) line_x_kernel( LineFastArgs const __gri
 
 template< int HB, bool ODD >
 __global__ void __launch_bounds__( 128 ) line_y_kernel( LineFastArgs const __grid_constant__ a ) {
-   int64_t const c = static_cast< int64_t >( blockIdx.x ) * 128 + threadIdx.x;
+   int64_t const c = static_cast< int64_t >( blockIdx.x ) * blockDim.x + threadIdx.x;
    if( c >= a.ncomp ) { return; }
    int64_t const sa = a.sst[ a.axis ], da = a.dstst[ a.axis ];
    int64_t const nblk = ( a.n + kRY - 1 ) / kRY;
@@ -264,23 +265,37 @@ __global__ void __launch_bounds__( 128 ) line_y_kernel( LineFastArgs const __gri
    }
 }
 
+// CTA width (32, 64 or 128 threads) that leaves the fewest idle threads for `n` items of
+// `per` outputs per thread; the widest on ties.
+int fast_width( int64_t n, int per ) {
+   int best = 128;
+   int64_t waste = ( n + 128 * per - 1 ) / ( 128 * per ) * ( 128 * per ) - n;
+   for( int w : { 64, 32 } ) {
+      int64_t const wv = ( n + w * per - 1 ) / ( w * per ) * ( w * per ) - n;
+      if( wv < waste ) { waste = wv; best = w; }
+   }
+   return best;
+}
+
 template< int HB >
 cudaError_t launch_fast_bucket( LineFastArgs const& a, bool along, cudaStream_t stream ) {
    if( along ) {
-      int64_t const gx = ( a.n + 128 * kRX - 1 ) / ( 128 * kRX );
+      int const nt = fast_width( a.n, kRX );
+      int64_t const gx = ( a.n + nt * kRX - 1 ) / ( nt * kRX );
       int64_t const gy = a.nouter < 65535 ? a.nouter : 65535;
       if( gx > 0x7fffffff ) { return cudaErrorInvalidValue; }
       dim3 const grid( static_cast< unsigned >( gx ), static_cast< unsigned >( gy ));
-      if( a.odd ) { line_x_kernel< HB, true ><<< grid, 128, 0, stream >>>( a ); }
-      else { line_x_kernel< HB, false ><<< grid, 128, 0, stream >>>( a ); }
+      if( a.odd ) { line_x_kernel< HB, true ><<< grid, nt, 0, stream >>>( a ); }
+      else { line_x_kernel< HB, false ><<< grid, nt, 0, stream >>>( a ); }
    } else {
-      int64_t const gx = ( a.ncomp + 127 ) / 128;
+      int const nt = fast_width( a.ncomp, 1 );
+      int64_t const gx = ( a.ncomp + nt - 1 ) / nt;
       int64_t const work = a.nouter * (( a.n + kRY - 1 ) / kRY );
       int64_t const gy = work < 65535 ? work : 65535;
       if( gx > 0x7fffffff ) { return cudaErrorInvalidValue; }
       dim3 const grid( static_cast< unsigned >( gx ), static_cast< unsigned >( gy ));
-      if( a.odd ) { line_y_kernel< HB, true ><<< grid, 128, 0, stream >>>( a ); }
-      else { line_y_kernel< HB, false ><<< grid, 128, 0, stream >>>( a ); }
+      if( a.odd ) { line_y_kernel< HB, true ><<< grid, nt, 0, stream >>>( a ); }
+      else { line_y_kernel< HB, false ><<< grid, nt, 0, stream >>>( a ); }
    }
    return cudaGetLastError();
 }
