@@ -548,7 +548,7 @@ def run_batch(args):
     line["config"]["plan"] = plan.info()
     ach = 8 * npx / (avg * 1e-3) / 1e9
     line["roofline"] = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
-                        "traffic": None, "peak_source": kind, "kernel": "batch_kernel (persistent work queue)",
+                        "traffic": None, "peak_source": kind, "kernel": "whole batch run (grouped tile and line kernels)",
                         "bytes_per_voxel": 8, "avg_kernel_ms": avg}
     line["clocks"] = clk
     line["gpu_launches"] = plan.info()["kernels_per_run"] * args.steps   # all kernels of the captured graph

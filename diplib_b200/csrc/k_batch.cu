@@ -234,15 +234,19 @@ __global__ void __launch_bounds__( 256 ) batch_kernel( BatchArgs const __grid_co
 // round-robin over the warps of a persistent grid.  Taps come from the plan's weight bank per
 // tile (zero beyond each axis' half-width), so a sigma-table update replays correctly.  Images
 // whose row stride is not a multiple of 16 bytes (TMA global strides are) get the same boxes
-// from per-lane 4-byte cp.async copies with zero fill; every stage fill commits one copy group
-// (empty for TMA boxes), so waiting until SPW - 1 groups are pending finds the current stage's
-// copies done.
+// from per-lane cp.async copies with zero fill (8 bytes per lane and row when the row stride and
+// width are even, else 4); every stage fill commits one copy group (empty for TMA boxes), so
+// waiting until SPW - 1 groups are pending finds the current stage's copies done.  Output tiles
+// go out as one TMA store each where the destination layout allows, else as per-lane stores.
 
 struct alignas( 128 ) G2Image {
    CUtensorMap tmap;        // 4D (x, y, 1, 1) tiled map of the source, box = tile + halo (if tma)
+   CUtensorMap tout;        // 4D tiled map of the destination, box = tile (if tma_store)
    float const* src;        // the source, for images whose layout TMA cannot take
    int64_t ss1;             // source row stride (x stride 1)
    int32_t tma;             // 1: boxes by TMA; 0: by per-lane asynchronous copies
+   int32_t pair8;           // per-lane copies of 8 bytes (column pairs wholly inside or outside)
+   int32_t tma_store;       // 1: output tiles by TMA stores
    float* dst;
    int64_t ds1;             // destination row stride (x stride 1)
    int32_t n[ 2 ];
@@ -334,19 +338,28 @@ __global__ void __launch_bounds__( W2Geom< float, B, 32 >::NT, 2 ) batch_ws_kern
             if( ok ) {
                // Box rows of BW floats, two columns per lane; outside the image: zero fill.
                int const nx = im->n[ 0 ], ny = im->n[ 1 ];
-               int const bx = x0 - G::LEAD, by = y0 - B;
-               float* const dst = reinterpret_cast< float* >( stages + st * G::STAGE_STRIDE );
-               for( int r = 0; r < BH; ++r ) {
-                  int const y = by + r;
-                  bool const yin = y >= 0 && y < ny;
-#pragma unroll
-                  for( int h = 0; h < 2; ++h ) {
-                     int const c = 2 * lane + h;
-                     int const x = bx + c;
-                     bool const in = yin && x >= 0 && x < nx;
-                     float const* src = in ? im->src + static_cast< int64_t >( y ) * im->ss1 + x : im->src;
+               int const by = y0 - B, xa = x0 - G::LEAD + 2 * lane;
+               bool const in0 = xa >= 0 && xa < nx, in1 = xa + 1 >= 0 && xa + 1 < nx;
+               float const* const src0 = im->src;
+               int64_t const ss1 = im->ss1;
+               int64_t off = static_cast< int64_t >( by ) * ss1 + xa;   // used only inside the image
+               uint32_t d = smem_u32( stages + st * G::STAGE_STRIDE ) + 8u * static_cast< uint32_t >( lane );
+               if( im->pair8 ) {
+#pragma unroll 4
+                  for( int r = 0; r < BH; ++r, off += ss1, d += BW * 4 ) {
+                     bool const in = static_cast< unsigned >( by + r ) < static_cast< unsigned >( ny ) && in0;
+                     asm volatile( "cp.async.ca.shared.global [%0], [%1], 8, %2;"
+                                   :: "r"( d ), "l"( in ? src0 + off : src0 ), "r"( in ? 8 : 0 ) : "memory" );
+                  }
+               } else {
+#pragma unroll 4
+                  for( int r = 0; r < BH; ++r, off += ss1, d += BW * 4 ) {
+                     bool const yin = static_cast< unsigned >( by + r ) < static_cast< unsigned >( ny );
+                     bool const i0 = yin && in0, i1 = yin && in1;
                      asm volatile( "cp.async.ca.shared.global [%0], [%1], 4, %2;"
-                                   :: "r"( smem_u32( dst + r * BW + c )), "l"( src ), "r"( in ? 4 : 0 ) : "memory" );
+                                   :: "r"( d ), "l"( i0 ? src0 + off : src0 ), "r"( i0 ? 4 : 0 ) : "memory" );
+                     asm volatile( "cp.async.ca.shared.global [%0], [%1], 4, %2;"
+                                   :: "r"( d + 4u ), "l"( i1 ? src0 + off + 1 : src0 ), "r"( i1 ? 4 : 0 ) : "memory" );
                   }
                }
             }
@@ -473,7 +486,10 @@ __global__ void __launch_bounds__( W2Geom< float, B, 32 >::NT, 2 ) batch_ws_kern
          }
          __syncwarp();
       }
-      // x pass: lane -> (row pair, strip of SW columns), results staged in `ot`
+      // x pass: lane -> (row pair, strip of SW columns), results staged in `ot` (after any
+      // earlier TMA store of this warp has finished reading it)
+      if( lane == 0 ) { asm volatile( "cp.async.bulk.wait_group.read 0;" ::: "memory" ); }
+      __syncwarp();
 #pragma unroll 1
       for( int grp = 0; grp < TY / 16; ++grp ) {
          int const rp = ( lane >> 2 ) + 8 * grp, c0 = ( lane & 3 ) * G::SW;
@@ -503,28 +519,44 @@ __global__ void __launch_bounds__( W2Geom< float, B, 32 >::NT, 2 ) batch_ws_kern
             *reinterpret_cast< float2* >( ot + ( 2 * rp + 1 ) * G::OTS + c0 + c ) = make_float2( out[ c ].y, out[ c + 1 ].y );
          }
       }
+      if( im->tma_store ) {
+         // One TMA store of the staged tile (clipped at the image edges by the tensor map).
+         fence_proxy_async();
+         __syncwarp();
+         if( lane == 0 ) {
+            asm volatile( "cp.async.bulk.tensor.4d.global.shared::cta.bulk_group [%0, {%1, %2, %3, %4}], [%5];"
+                          :: "l"( reinterpret_cast< uint64_t >( &im->tout )), "r"( x0 ), "r"( y0 ), "r"( 0 ), "r"( 0 ),
+                             "r"( smem_u32( ot )) : "memory" );
+            asm volatile( "cp.async.bulk.commit_group;" ::: "memory" );
+         }
+         __syncwarp();
+         continue;
+      }
       __syncwarp();
-      // coalesced stores of the staged tile: lanes sweep rows in column pairs
-      float* const dst = im->dst;
-      int64_t const ds1 = im->ds1;
-      bool const vec = im->vec_store != 0;
-#pragma unroll 4
-      for( int e = lane; e < TY * ( TX / 2 ); e += 32 ) {
-         int const r = e / ( TX / 2 ), cp = e - r * ( TX / 2 );
-         int const xo = x0 + 2 * cp, yo = y0 + r;
-         if( xo < nx && yo < ny ) {
-            float2 const val = *reinterpret_cast< float2 const* >( ot + r * G::OTS + 2 * cp );
-            float* const p = dst + static_cast< int64_t >( yo ) * ds1 + xo;
-            if( xo + 1 < nx && vec ) {
-               *reinterpret_cast< float2* >( p ) = val;
-            } else {
-               p[ 0 ] = val.x;
-               if( xo + 1 < nx ) { p[ 1 ] = val.y; }
+      // Per-lane stores of the staged tile: lane -> column pair, down the tile's rows (a warp
+      // store covers TX / 2 consecutive pairs of one row).
+      static_assert( TX / 2 <= 32, "one column pair per lane" );
+      int const xo = x0 + 2 * lane;
+      if( lane < TX / 2 && xo < nx ) {
+         int const rows = ny - y0 < TY ? ny - y0 : TY;
+         int64_t const ds1 = im->ds1;
+         float* p = im->dst + static_cast< int64_t >( y0 ) * ds1 + xo;
+         float const* q = ot + 2 * lane;
+         if( xo + 1 < nx && im->vec_store ) {
+#pragma unroll 8
+            for( int r = 0; r < rows; ++r, p += ds1, q += G::OTS ) { *reinterpret_cast< float2* >( p ) = *reinterpret_cast< float2 const* >( q ); }
+         } else {
+            bool const two = xo + 1 < nx;
+#pragma unroll 8
+            for( int r = 0; r < rows; ++r, p += ds1, q += G::OTS ) {
+               p[ 0 ] = q[ 0 ];
+               if( two ) { p[ 1 ] = q[ 1 ]; }
             }
          }
       }
       __syncwarp();   // b2, tables, taps and staging reads done before the next tile
    }
+   if( lane == 0 ) { asm volatile( "cp.async.bulk.wait_group 0;" ::: "memory" ); }
 }
 
 template< int B >
@@ -933,8 +965,18 @@ int plan_groups( dipcu_batch_plan* p, int inject ) {
          cuuint32_t box[ 4 ] = { 64, static_cast< cuuint32_t >( g2_box_h( b )), 1, 1 };
          g.tma = encode_source_map( &g.tmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, im.src, dims, strides, box ) == CUDA_SUCCESS ? 1 : 0;
       }
+      g.pair8 = (( reinterpret_cast< uintptr_t >( im.src ) & 7 ) == 0 && im.ss[ 1 ] % 2 == 0 && im.n[ 0 ] % 2 == 0 ) ? 1 : 0;
       g.dst = im.dst;
       g.ds1 = im.ds[ 1 ];
+      g.tma_store = 0;
+      if(( reinterpret_cast< uintptr_t >( im.dst ) & 15 ) == 0 && ( im.ds[ 1 ] * 4 ) % 16 == 0 && !getenv( "DIPCU_NO_TMA_STORE" )) {
+         cuuint64_t dims[ 4 ] = { static_cast< cuuint64_t >( im.n[ 0 ] ), static_cast< cuuint64_t >( im.n[ 1 ] ), 1, 1 };
+         cuuint64_t plane = static_cast< cuuint64_t >( im.ds[ 1 ] * im.n[ 1 ] * 4 );
+         plane = ( plane + 15 ) / 16 * 16;
+         cuuint64_t strides[ 3 ] = { static_cast< cuuint64_t >( im.ds[ 1 ] * 4 ), plane, plane };
+         cuuint32_t box[ 4 ] = { static_cast< cuuint32_t >( g2_tile_x( b )), 32, 1, 1 };
+         g.tma_store = encode_source_map( &g.tout, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, im.dst, dims, strides, box ) == CUDA_SUCCESS ? 1 : 0;
+      }
       for( int d = 0; d < 2; ++d ) {
          g.n[ d ] = static_cast< int32_t >( im.n[ d ] );
          g.bc[ d ] = im.bc[ d ];
