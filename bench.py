@@ -10,7 +10,8 @@ sfloat output -- run twice, with derivative orders (0,0,0) and (1,0,0).
             (672 MB touched per rotation, > 126 MB L2), so every step reads cold data.
   e2e    -- the same metric through the public API with host buffers: per step a pinned
             host->device copy of the input, the two filter calls, and device->host copies of
-            both outputs.
+            both outputs, pipelined over three streams (upload, filters, download) with
+            double-buffered device buffers.
   roofline, cpu_baseline, clocks, gpu_launches -- see the keys below.
 
 --impl reference times DIPlib's own OpenMP CPU implementation (oracle/_ref, built from the
@@ -272,34 +273,19 @@ def run_gpu_arm(args):
     host_call_us = (time.perf_counter() - t0) / 20 * 1e6
     torch.cuda.synchronize()
 
-    # End to end through the public API with pinned host buffers.
+    # End to end through the public API with pinned host buffers (pipelined: _e2e).
     h_in = torch.from_numpy(host.astype(np.int32)).to(torch.uint16).pin_memory()
     h_out = [torch.empty(SHAPE, dtype=torch.float32).pin_memory() for _ in ORDERS]
-    d_in = torch.empty(SHAPE, dtype=torch.uint16, device=dev)
-    d_out = [torch.empty(SHAPE, dtype=torch.float32, device=dev) for _ in ORDERS]
+    d_in = [torch.empty(SHAPE, dtype=torch.uint16, device=dev) for _ in range(2)]
+    d_out = [[torch.empty(SHAPE, dtype=torch.float32, device=dev) for _ in ORDERS] for _ in range(2)]
 
-    def e2e_step():
-        d_in.copy_(h_in, non_blocking=True)
-        for j, o in enumerate(ORDERS):
-            dipcu.GaussFIR(d_in, SIGMAS, o, BCS, TRUNC, out=d_out[j])
-            h_out[j].copy_(d_out[j], non_blocking=True)
+    def up(k):
+        d_in[k].copy_(h_in, non_blocking=True)
 
-    e2e_steps = max(3, min(args.steps, 20))
-    for _ in range(2):
-        e2e_step()
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(e2e_steps):
-        e2e_step()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1) / e2e_steps
-    if world > 1:
-        t = torch.tensor([e2e_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = world * nvox / (e2e_ms * 1e-3) / 1e9
+    parts = [(lambda k, j=j: dipcu.GaussFIR(d_in[k], SIGMAS, ORDERS[j], BCS, TRUNC, out=d_out[k][j]),
+              lambda k, j=j: h_out[j].copy_(d_out[k][j], non_blocking=True)) for j in range(len(ORDERS))]
+    e2e = _e2e(up, parts, nvox, dev, world, h_in.numel() * 2, sum(h.numel() * 4 for h in h_out),
+               steps=max(3, min(args.steps, 20)))
 
     peak, peak_kind = load_peaks()
     avg_kernel_ms = sum(kernel_ms) / len(kernel_ms)
@@ -313,8 +299,7 @@ def run_gpu_arm(args):
                      "traffic": traffic_from_profiles(), "peak_source": peak_kind,
                      "kernel": "fused3d_ws_kernel (warp-specialised z-marching tile kernel)", "bytes_per_voxel": BYTES_PER_VOXEL,
                      "avg_kernel_ms": avg_kernel_ms},
-        "e2e": {"value": e2e_value, "unit": "Gvox/s", "h2d_bytes_per_step": int(h_in.numel() * 2),
-                "d2h_bytes_per_step": int(sum(h.numel() * 4 for h in h_out)), "ms_per_step": e2e_ms},
+        "e2e": e2e,
         "clocks": clk.summary(),
         "host_us_per_call": host_call_us,
         "gpu_launches": args.steps * len(ORDERS),
@@ -459,14 +444,11 @@ def run_gauss2d(args):
     # e2e: pinned host image in, result out.
     h_in = torch.from_numpy(host).pin_memory()
     h_out = torch.empty(G2_SHAPE, dtype=torch.float32).pin_memory()
-    d_in, d_out = torch.empty_like(xs[0]), torch.empty_like(ys[0])
-
-    def e2e():
-        d_in.copy_(h_in, non_blocking=True)
-        dipcu.GaussFIR(d_in, [2.0, 2.0], [0, 0], ["mirror"], 3.0, out=d_out)
-        h_out.copy_(d_out, non_blocking=True)
-
-    line["e2e"] = _e2e(e2e, npx, dev, world, 4 * npx, 4 * npx)
+    d_in = [torch.empty_like(xs[0]) for _ in range(2)]
+    d_out = [torch.empty_like(ys[0]) for _ in range(2)]
+    line["e2e"] = _e2e(lambda k: d_in[k].copy_(h_in, non_blocking=True),
+                       [(lambda k: dipcu.GaussFIR(d_in[k], [2.0, 2.0], [0, 0], ["mirror"], 3.0, out=d_out[k]),
+                         lambda k: h_out.copy_(d_out[k], non_blocking=True))], npx, dev, world, 4 * npx, 4 * npx)
     if rank == 0 and not args.no_cpu_baseline:
         import oracle
         if oracle.ref_available():
@@ -476,17 +458,52 @@ def run_gauss2d(args):
     return _finish(line, world)
 
 
-def _e2e(step, nvox, dev, world, h2d, d2h, steps=20):
+def _e2e(up, parts, nvox, dev, world, h2d, d2h, steps=20):
+    """End-to-end throughput through the public API, pipelined the way a caller streaming data
+    runs it: every step uploads its inputs from pinned host memory (copy stream), runs its work
+    (compute stream) and downloads its results (copy-back stream).  up(k) and each (work, down)
+    pair of `parts` issue the step's pieces for device buffer set k (two sets, alternating) on the
+    current stream; a part's download waits for that part's work only.  So step i's work overlaps
+    step i + 1's upload and step i - 1's download.  Every step still moves its own inputs up and
+    results down inside the timed region."""
     import torch
-    for _ in range(2):
-        step()
+    main = torch.cuda.current_stream(dev)
+    st = [torch.cuda.Stream(dev) for _ in range(3)]
+    ev_up = [torch.cuda.Event() for _ in range(2)]
+    ev_work = [[torch.cuda.Event() for _ in range(2)] for _ in parts]
+    ev_down = [torch.cuda.Event() for _ in range(2)]
+
+    def step(i):
+        k = i % 2
+        st[0].wait_event(ev_work[-1][k])            # set k's previous work has read its inputs
+        with torch.cuda.stream(st[0]):
+            up(k)
+        ev_up[k].record(st[0])
+        st[1].wait_event(ev_up[k])
+        st[1].wait_event(ev_down[k])                # set k's previous results are downloaded
+        for j, (work, down) in enumerate(parts):
+            with torch.cuda.stream(st[1]):
+                work(k)
+            ev_work[j][k].record(st[1])
+            st[2].wait_event(ev_work[j][k])
+            with torch.cuda.stream(st[2]):
+                down(k)
+        ev_down[k].record(st[2])
+
+    def run(n):
+        for s_ in st:
+            s_.wait_stream(main)
+        for i in range(n):
+            step(i)
+        for s_ in st:
+            main.wait_stream(s_)
+
+    run(2)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    stream = torch.cuda.current_stream(dev)
-    e0.record(stream)
-    for _ in range(steps):
-        step()
-    e1.record(stream)
+    e0.record(main)
+    run(steps)
+    e1.record(main)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / steps
     if world > 1:
@@ -495,7 +512,8 @@ def _e2e(step, nvox, dev, world, h2d, d2h, steps=20):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
     return {"value": world * nvox / (ms * 1e-3) / 1e9, "unit": "Gvox/s", "h2d_bytes_per_step": int(h2d),
-            "d2h_bytes_per_step": int(d2h), "ms_per_step": ms}
+            "d2h_bytes_per_step": int(d2h), "ms_per_step": ms,
+            "pipelining": "uploads, work and downloads on three streams, two device buffer sets"}
 
 
 # ---- batched uneven 2D (512 images) --------------------------------------------------------------
@@ -578,18 +596,25 @@ def run_batch(args):
     line["vs_single_image"] = {"single_image_gvox_s": single_rate, "ratio": value / world / single_rate,
                                "how": "plain dipcu_gauss_fir on one 4096^2 image per (sigma, orders, boundary "
                                       "condition) combination, weighted by the batch's pixel shares", "rates": rates}
-    # e2e: every image in from pinned host memory, every result back.
+    # e2e: every image in from pinned host memory, every result back; a second plan over a second
+    # set of device buffers for the pipelined steps.
     h_in = [t.cpu().pin_memory() for t in ins]
     h_out = [torch.empty(s).pin_memory() for s in shapes]
+    ins2 = [t.clone() for t in ins]
+    outs2 = [torch.empty_like(t) for t in outs]
+    plan2 = BatchPlan(ins2, outs2, [p[0] for p in params], [p[1] for p in params], [p[2] for p in params],
+                      graph=True, autotune=True)
+    sets = [(plan, ins, outs), (plan2, ins2, outs2)]
 
-    def e2e():
-        for a, b in zip(h_in, ins):
+    def up(k):
+        for a, b in zip(h_in, sets[k][1]):
             b.copy_(a, non_blocking=True)
-        plan.run()
-        for a, b in zip(h_out, outs):
+
+    def down(k):
+        for a, b in zip(h_out, sets[k][2]):
             a.copy_(b, non_blocking=True)
 
-    line["e2e"] = _e2e(e2e, npx, dev, world, 4 * npx, 4 * npx, steps=5)
+    line["e2e"] = _e2e(up, [(lambda k: sets[k][0].run(), down)], npx, dev, world, 4 * npx, 4 * npx, steps=5)
     if rank == 0 and not args.no_cpu_baseline:
         import oracle
         if oracle.ref_available():
