@@ -335,11 +335,14 @@ cudaError_t launch_line_fast( LinePass const& p, cudaStream_t stream ) {
       if( d != a.axis && d != a.comp ) { nouter *= p.sizes[ d ]; }
    }
    a.nouter = nouter;
-   int const hb = p.h <= 4 ? 4 : p.h <= 8 ? 8 : p.h <= 16 ? 16 : 32;
+   // Buckets at the half-widths of sigma 4 and 8 with order 0 (12, 24) as well as the powers of two.
+   int const hb = p.h <= 4 ? 4 : p.h <= 8 ? 8 : p.h <= 12 ? 12 : p.h <= 16 ? 16 : p.h <= 24 ? 24 : 32;
    switch( hb ) {
       case 4: return launch_fast_bucket< 4 >( a, along, stream );
       case 8: return launch_fast_bucket< 8 >( a, along, stream );
+      case 12: return launch_fast_bucket< 12 >( a, along, stream );
       case 16: return launch_fast_bucket< 16 >( a, along, stream );
+      case 24: return launch_fast_bucket< 24 >( a, along, stream );
       default: return launch_fast_bucket< 32 >( a, along, stream );
    }
 }
