@@ -626,9 +626,10 @@ cudaError_t g2_launch( int b, G2Args const& a, int grid, cudaStream_t st ) {
 
 // ---- grouped line passes: every other image (periodic boundaries, half-widths 13 .. 32) as two
 // passes -- along x into a plan-owned intermediate, then along y into the output -- with the
-// register-window line kernels of the fast float path (k_line.cu), per-image tables and work
-// lists, one launch per pass and half-width bucket (4, 8, 16, 32).  Taps come from the weight
-// bank per work item (zero beyond the image's half-width).
+// register-window line kernels of the fast float path (k_line.cu), one table of images and work
+// lists per pass and per half-width bucket of that pass' axis (4, 8, 12, 16, 24, 32): one launch
+// each, the y passes after every x pass.  Taps come from the weight bank per work item (zero
+// beyond the axis' half-width).
 
 struct BLImage {
    float const* src;
@@ -650,7 +651,8 @@ struct BLArgs {
    int32_t nitems;
 };
 
-constexpr int kBLBuckets[ 4 ] = { 4, 8, 16, 32 };
+constexpr int kNBL = 6;      // half-width buckets of the line passes, per axis
+constexpr int kBLBuckets[ kNBL ] = { 4, 8, 12, 16, 24, 32 };
 constexpr int kBLT = 256;    // x pass: outputs per item
 constexpr int kBLXT = 64;    // x pass: threads per CTA (4 outputs each)
 constexpr int kBLR = 16;     // y pass: rows per item
@@ -810,16 +812,23 @@ __global__ void __launch_bounds__( 128 ) batch_line_y_kernel( BLArgs const __gri
    }
 }
 
+template< int HB >
+void bl_launch_hb( bool ypass, BLArgs const& a, unsigned grid, cudaStream_t st ) {
+   if( ypass ) { batch_line_y_kernel< HB ><<< grid, 128, 0, st >>>( a ); } else { batch_line_x_kernel< HB ><<< grid, kBLXT, 0, st >>>( a ); }
+}
+
 cudaError_t bl_launch( int b, bool ypass, BLArgs const& a, cudaStream_t st ) {
    int64_t const cap = ypass ? 148 * 8 : 148 * 16;
    int64_t g = a.nitems < cap ? a.nitems : cap;
    if( g < 1 ) { g = 1; }
    unsigned const grid = static_cast< unsigned >( g );
    switch( b ) {
-      case 0: if( ypass ) { batch_line_y_kernel< 4 ><<< grid, 128, 0, st >>>( a ); } else { batch_line_x_kernel< 4 ><<< grid, kBLXT, 0, st >>>( a ); } break;
-      case 1: if( ypass ) { batch_line_y_kernel< 8 ><<< grid, 128, 0, st >>>( a ); } else { batch_line_x_kernel< 8 ><<< grid, kBLXT, 0, st >>>( a ); } break;
-      case 2: if( ypass ) { batch_line_y_kernel< 16 ><<< grid, 128, 0, st >>>( a ); } else { batch_line_x_kernel< 16 ><<< grid, kBLXT, 0, st >>>( a ); } break;
-      default: if( ypass ) { batch_line_y_kernel< 32 ><<< grid, 128, 0, st >>>( a ); } else { batch_line_x_kernel< 32 ><<< grid, kBLXT, 0, st >>>( a ); } break;
+      case 0: bl_launch_hb< 4 >( ypass, a, grid, st ); break;
+      case 1: bl_launch_hb< 8 >( ypass, a, grid, st ); break;
+      case 2: bl_launch_hb< 12 >( ypass, a, grid, st ); break;
+      case 3: bl_launch_hb< 16 >( ypass, a, grid, st ); break;
+      case 4: bl_launch_hb< 24 >( ypass, a, grid, st ); break;
+      default: bl_launch_hb< 32 >( ypass, a, grid, st ); break;
    }
    return cudaGetLastError();
 }
@@ -910,16 +919,19 @@ struct dipcu_batch_plan {
    G2Image* d_gimg[ 4 ] = {};
    BatchItem* d_gitems[ 4 ] = {};
    int g_nimg[ 4 ] = {}, g_nitems[ 4 ] = {}, g_grid[ 4 ] = {};
-   // Grouped line passes, per half-width bucket (4, 8, 16, 32), and their intermediate.
-   BLImage* d_limg[ 4 ] = {};
-   BatchItem* d_lxitems[ 4 ] = {};
-   BatchItem* d_lyitems[ 4 ] = {};
-   int l_nimg[ 4 ] = {}, l_nx[ 4 ] = {}, l_ny[ 4 ] = {};
+   // Grouped line passes: one image table, work items per pass and per half-width bucket of
+   // that pass' axis (4, 8, 12, 16, 24, 32), and their intermediate.
+   BLImage* d_limg = nullptr;
+   BatchItem* d_lxitems[ kNBL ] = {};
+   BatchItem* d_lyitems[ kNBL ] = {};
+   int l_nimg = 0, l_nx[ kNBL ] = {}, l_ny[ kNBL ] = {};
    float* d_tmp = nullptr;
-   // Fork / join of the per-bucket launches: bucket b runs on side[b], concurrently with the
-   // other buckets and the persistent kernel (parallel branches of the captured graph).
+   // Fork / join: side stream s runs the x passes of the line buckets b = s (mod 4), then -- once
+   // every stream's x passes are done (ev_x) -- their y passes, then warp-per-tile bucket s;
+   // the streams run concurrently with each other and the persistent kernel (parallel branches
+   // of the captured graph).
    cudaStream_t side[ 4 ] = {};
-   cudaEvent_t ev_fork = nullptr, ev_join[ 4 ] = {};
+   cudaEvent_t ev_fork = nullptr, ev_join[ 4 ] = {}, ev_x[ 4 ] = {};
    cudaStream_t cap_stream = nullptr;
    cudaGraph_t graph = nullptr;
    cudaGraphExec_t exec = nullptr;
@@ -995,17 +1007,18 @@ int plan_groups( dipcu_batch_plan* p, int inject ) {
    }
    // The rest: grouped line passes (every batch image qualifies: index-mapping boundary
    // conditions or "add zeros", half-widths up to 32, unit x stride).
-   std::vector< BLImage > limg[ 4 ];
-   std::vector< BatchItem > lx[ 4 ], ly[ 4 ];
-   std::vector< int64_t > toff[ 4 ];   // intermediate offset of each image, per bucket
+   std::vector< BLImage > limg;
+   std::vector< BatchItem > lx[ kNBL ], ly[ kNBL ];
+   std::vector< int64_t > toff;   // intermediate offset of each image
    int64_t ttot = 0;
+   auto bucket = []( int h ) { int b = 0; while( b < kNBL - 1 && h > kBLBuckets[ b ] ) { ++b; } return b; };
    if( !getenv( "DIPCU_BATCH_NO_LINES" )) {
       for( int i = 0; i < p->count; ++i ) {
          if( p->gbucket[ static_cast< size_t >( i ) ] >= 0 ) { continue; }
          BatchImage const& im = p->images[ static_cast< size_t >( i ) ];
          int const hm = std::max( im.h[ 0 ], im.h[ 1 ] );
          if( hm > 32 || ( reinterpret_cast< uintptr_t >( im.src ) & 3 ) || im.n[ 0 ] >= ( 1 << 30 ) || im.n[ 1 ] >= ( 1 << 30 )) { continue; }
-         int const lb = hm <= 4 ? 0 : hm <= 8 ? 1 : hm <= 16 ? 2 : 3;
+         int const lbx = bucket( im.h[ 0 ] ), lby = bucket( im.h[ 1 ] );
          BLImage l{};
          l.src = im.src;
          l.dst = im.dst;
@@ -1022,13 +1035,13 @@ int plan_groups( dipcu_batch_plan* p, int inject ) {
          l.nseg = ( l.n0 + kBLT - 1 ) / kBLT;
          l.ncb = ( l.n0 + 127 ) / 128;
          int const nrb = ( l.n1 + kBLR - 1 ) / kBLR;
-         int const li = static_cast< int >( limg[ lb ].size());
-         for( int t = 0; t < l.n1 * l.nseg; ++t ) { lx[ lb ].push_back( BatchItem{ li, t } ); }
-         for( int t = 0; t < l.ncb * nrb; ++t ) { ly[ lb ].push_back( BatchItem{ li, t } ); }
-         toff[ lb ].push_back( ttot );
+         int const li = static_cast< int >( limg.size());
+         for( int t = 0; t < l.n1 * l.nseg; ++t ) { lx[ lbx ].push_back( BatchItem{ li, t } ); }
+         for( int t = 0; t < l.ncb * nrb; ++t ) { ly[ lby ].push_back( BatchItem{ li, t } ); }
+         toff.push_back( ttot );
          ttot += static_cast< int64_t >( l.n0 ) * l.n1;
-         limg[ lb ].push_back( l );
-         p->gbucket[ static_cast< size_t >( i ) ] = 4 + lb;
+         limg.push_back( l );
+         p->gbucket[ static_cast< size_t >( i ) ] = 4 + lby;
          --rest;
       }
    }
@@ -1040,7 +1053,7 @@ int plan_groups( dipcu_batch_plan* p, int inject ) {
          done = true;
          break;
       }
-      for( int b = 0; b < 4 && !done; ++b ) {
+      for( int b = 0; b < kNBL && !done; ++b ) {
          if( ly[ b ].empty()) { continue; }
          if( inject == 1 ) { ly[ b ][ ly[ b ].size() / 2 ].image = 1 << 20; } else { ly[ b ][ ly[ b ].size() / 2 ].tile = 1 << 30; }
          done = true;
@@ -1050,21 +1063,20 @@ int plan_groups( dipcu_batch_plan* p, int inject ) {
       if( cudaMalloc( &p->d_tmp, sizeof( float ) * static_cast< size_t >( ttot )) != cudaSuccess ) {
          return plan_fail( DIPCU_ERR_CUDA, "batch plan: line-pass intermediate" );
       }
-      for( int b = 0; b < 4; ++b ) {
-         for( size_t k = 0; k < limg[ b ].size(); ++k ) { limg[ b ][ k ].tmp = p->d_tmp + toff[ b ][ k ]; }
-      }
+      for( size_t k = 0; k < limg.size(); ++k ) { limg[ k ].tmp = p->d_tmp + toff[ k ]; }
    }
-   for( int b = 0; b < 4; ++b ) {
-      p->l_nimg[ b ] = static_cast< int >( limg[ b ].size());
+   p->l_nimg = static_cast< int >( limg.size());
+   if( !limg.empty() && ( cudaMalloc( &p->d_limg, sizeof( BLImage ) * limg.size()) != cudaSuccess ||
+                          cudaMemcpy( p->d_limg, limg.data(), sizeof( BLImage ) * limg.size(), cudaMemcpyHostToDevice ) != cudaSuccess )) {
+      return plan_fail( DIPCU_ERR_CUDA, "batch plan: line-pass tables" );
+   }
+   for( int b = 0; b < kNBL; ++b ) {
       p->l_nx[ b ] = static_cast< int >( lx[ b ].size());
       p->l_ny[ b ] = static_cast< int >( ly[ b ].size());
-      if( limg[ b ].empty()) { continue; }
-      if( cudaMalloc( &p->d_limg[ b ], sizeof( BLImage ) * limg[ b ].size()) != cudaSuccess ||
-          cudaMalloc( &p->d_lxitems[ b ], sizeof( BatchItem ) * lx[ b ].size()) != cudaSuccess ||
-          cudaMalloc( &p->d_lyitems[ b ], sizeof( BatchItem ) * ly[ b ].size()) != cudaSuccess ||
-          cudaMemcpy( p->d_limg[ b ], limg[ b ].data(), sizeof( BLImage ) * limg[ b ].size(), cudaMemcpyHostToDevice ) != cudaSuccess ||
-          cudaMemcpy( p->d_lxitems[ b ], lx[ b ].data(), sizeof( BatchItem ) * lx[ b ].size(), cudaMemcpyHostToDevice ) != cudaSuccess ||
-          cudaMemcpy( p->d_lyitems[ b ], ly[ b ].data(), sizeof( BatchItem ) * ly[ b ].size(), cudaMemcpyHostToDevice ) != cudaSuccess ) {
+      if(( !lx[ b ].empty() && ( cudaMalloc( &p->d_lxitems[ b ], sizeof( BatchItem ) * lx[ b ].size()) != cudaSuccess ||
+                                 cudaMemcpy( p->d_lxitems[ b ], lx[ b ].data(), sizeof( BatchItem ) * lx[ b ].size(), cudaMemcpyHostToDevice ) != cudaSuccess )) ||
+         ( !ly[ b ].empty() && ( cudaMalloc( &p->d_lyitems[ b ], sizeof( BatchItem ) * ly[ b ].size()) != cudaSuccess ||
+                                 cudaMemcpy( p->d_lyitems[ b ], ly[ b ].data(), sizeof( BatchItem ) * ly[ b ].size(), cudaMemcpyHostToDevice ) != cudaSuccess ))) {
          return plan_fail( DIPCU_ERR_CUDA, "batch plan: line-pass tables" );
       }
    }
@@ -1136,38 +1148,42 @@ int enqueue_run( dipcu_batch_plan* p, cudaStream_t st ) {
       e = launch_shape( p->shape, p->grid, a, st );
       if( e != cudaSuccess ) { return plan_fail( DIPCU_ERR_CUDA, std::string( "batch_kernel: " ) + cudaGetErrorString( e )); }
    }
-   for( int b = 0; b < 4; ++b ) {
-      if( p->g_nitems[ b ] == 0 && p->l_nimg[ b ] == 0 ) { continue; }
-      cudaStream_t const sb = p->side[ b ];
+   BLArgs l{};
+   l.images = p->d_limg;
+   l.wbank = p->d_bank;
+   l.status = device_status_ptr();
+   l.nimages = p->l_nimg;
+   auto line_pass = [ & ]( int b, bool ypass, cudaStream_t sb ) -> cudaError_t {
+      l.items = ypass ? p->d_lyitems[ b ] : p->d_lxitems[ b ];
+      l.nitems = ypass ? p->l_ny[ b ] : p->l_nx[ b ];
+      return l.nitems > 0 ? bl_launch( b, ypass, l, sb ) : cudaSuccess;
+   };
+   for( int s = 0; s < 4; ++s ) {
+      cudaStream_t const sb = p->side[ s ];
       if( cudaStreamWaitEvent( sb, p->ev_fork, 0 ) != cudaSuccess ) { return plan_fail( DIPCU_ERR_CUDA, "batch fork" ); }
-      if( p->g_nitems[ b ] > 0 ) {
+      for( int b = s; b < kNBL && e == cudaSuccess; b += 4 ) { e = line_pass( b, false, sb ); }
+      if( e != cudaSuccess ) { return plan_fail( DIPCU_ERR_CUDA, std::string( "batch line x pass: " ) + cudaGetErrorString( e )); }
+      if( cudaEventRecord( p->ev_x[ s ], sb ) != cudaSuccess ) { return plan_fail( DIPCU_ERR_CUDA, "batch line join" ); }
+   }
+   for( int s = 0; s < 4; ++s ) {
+      cudaStream_t const sb = p->side[ s ];
+      for( int t = 0; t < 4; ++t ) {   // the y passes read every image's intermediate
+         if( t != s && cudaStreamWaitEvent( sb, p->ev_x[ t ], 0 ) != cudaSuccess ) { return plan_fail( DIPCU_ERR_CUDA, "batch line join" ); }
+      }
+      for( int b = s; b < kNBL && e == cudaSuccess; b += 4 ) { e = line_pass( b, true, sb ); }
+      if( e != cudaSuccess ) { return plan_fail( DIPCU_ERR_CUDA, std::string( "batch line y pass: " ) + cudaGetErrorString( e )); }
+      if( p->g_nitems[ s ] > 0 ) {
          G2Args g{};
-         g.images = p->d_gimg[ b ];
-         g.items = p->d_gitems[ b ];
+         g.images = p->d_gimg[ s ];
+         g.items = p->d_gitems[ s ];
          g.wbank = p->d_bank;
          g.status = device_status_ptr();
-         g.nimages = p->g_nimg[ b ];
-         g.nitems = p->g_nitems[ b ];
-         e = g2_launch( b, g, std::min( p->g_grid[ b ], std::max( 1, p->g_nitems[ b ] / 4 )), sb );
+         g.nimages = p->g_nimg[ s ];
+         g.nitems = p->g_nitems[ s ];
+         e = g2_launch( s, g, std::min( p->g_grid[ s ], std::max( 1, p->g_nitems[ s ] / 4 )), sb );
          if( e != cudaSuccess ) { return plan_fail( DIPCU_ERR_CUDA, std::string( "batch_ws_kernel: " ) + cudaGetErrorString( e )); }
       }
-      if( p->l_nimg[ b ] > 0 ) {
-         BLArgs l{};
-         l.images = p->d_limg[ b ];
-         l.wbank = p->d_bank;
-         l.status = device_status_ptr();
-         l.nimages = p->l_nimg[ b ];
-         l.items = p->d_lxitems[ b ];
-         l.nitems = p->l_nx[ b ];
-         e = bl_launch( b, false, l, sb );
-         if( e == cudaSuccess ) {
-            l.items = p->d_lyitems[ b ];
-            l.nitems = p->l_ny[ b ];
-            e = bl_launch( b, true, l, sb );
-         }
-         if( e != cudaSuccess ) { return plan_fail( DIPCU_ERR_CUDA, std::string( "batch line passes: " ) + cudaGetErrorString( e )); }
-      }
-      if( cudaEventRecord( p->ev_join[ b ], sb ) != cudaSuccess || cudaStreamWaitEvent( st, p->ev_join[ b ], 0 ) != cudaSuccess ) {
+      if( cudaEventRecord( p->ev_join[ s ], sb ) != cudaSuccess || cudaStreamWaitEvent( st, p->ev_join[ s ], 0 ) != cudaSuccess ) {
          return plan_fail( DIPCU_ERR_CUDA, "batch join" );
       }
    }
@@ -1258,7 +1274,8 @@ int dipcu_batch_plan_create( dipcu_image_desc const* ins, dipcu_image_desc const
    bool sok = cudaEventCreateWithFlags( &p->ev_fork, cudaEventDisableTiming ) == cudaSuccess;
    for( int b = 0; b < 4 && sok; ++b ) {
       sok = cudaStreamCreateWithFlags( &p->side[ b ], cudaStreamNonBlocking ) == cudaSuccess &&
-            cudaEventCreateWithFlags( &p->ev_join[ b ], cudaEventDisableTiming ) == cudaSuccess;
+            cudaEventCreateWithFlags( &p->ev_join[ b ], cudaEventDisableTiming ) == cudaSuccess &&
+            cudaEventCreateWithFlags( &p->ev_x[ b ], cudaEventDisableTiming ) == cudaSuccess;
    }
    if( !sok ) { dipcu_batch_plan_destroy( p ); return plan_fail( DIPCU_ERR_CUDA, "batch plan: streams" ); }
    // Tile shape: the autotuner times every candidate on this batch (the filter outputs are
@@ -1324,7 +1341,8 @@ int dipcu_batch_plan_info( dipcu_batch_plan const* plan, int* nitems, int* tile_
    if( !plan ) { return plan_fail( DIPCU_ERR_INVALID_ARG, "null plan" ); }
    if( nitems ) {
       *nitems = plan->nitems;
-      for( int b = 0; b < 4; ++b ) { *nitems += plan->g_nitems[ b ] + plan->l_nx[ b ] + plan->l_ny[ b ]; }
+      for( int b = 0; b < 4; ++b ) { *nitems += plan->g_nitems[ b ]; }
+      for( int b = 0; b < kNBL; ++b ) { *nitems += plan->l_nx[ b ] + plan->l_ny[ b ]; }
    }
    if( tile_x ) { *tile_x = kShapes[ plan->shape ].tx; }
    if( tile_y ) { *tile_y = kShapes[ plan->shape ].ty; }
@@ -1336,8 +1354,12 @@ int dipcu_batch_plan_launches( dipcu_batch_plan const* plan, int* kernels, int* 
    if( !plan ) { return plan_fail( DIPCU_ERR_INVALID_ARG, "null plan" ); }
    int k = 1 + ( plan->nitems > 0 ? 1 : 0 ), g = 0;
    for( int b = 0; b < 4; ++b ) {
-      k += ( plan->g_nitems[ b ] > 0 ? 1 : 0 ) + ( plan->l_nimg[ b ] > 0 ? 2 : 0 );
-      g += plan->g_nitems[ b ] + plan->l_nx[ b ] + plan->l_ny[ b ];
+      k += plan->g_nitems[ b ] > 0 ? 1 : 0;
+      g += plan->g_nitems[ b ];
+   }
+   for( int b = 0; b < kNBL; ++b ) {
+      k += ( plan->l_nx[ b ] > 0 ? 1 : 0 ) + ( plan->l_ny[ b ] > 0 ? 1 : 0 );
+      g += plan->l_nx[ b ] + plan->l_ny[ b ];
    }
    if( kernels ) { *kernels = k; }
    if( grouped_items ) { *grouped_items = g; }
@@ -1361,7 +1383,9 @@ int dipcu_batch_plan_destroy( dipcu_batch_plan* plan ) {
    for( int b = 0; b < 4; ++b ) {
       cudaFree( plan->d_gimg[ b ] );
       cudaFree( plan->d_gitems[ b ] );
-      cudaFree( plan->d_limg[ b ] );
+   }
+   cudaFree( plan->d_limg );
+   for( int b = 0; b < kNBL; ++b ) {
       cudaFree( plan->d_lxitems[ b ] );
       cudaFree( plan->d_lyitems[ b ] );
    }
@@ -1369,6 +1393,7 @@ int dipcu_batch_plan_destroy( dipcu_batch_plan* plan ) {
    for( int b = 0; b < 4; ++b ) {
       if( plan->side[ b ] ) { cudaStreamDestroy( plan->side[ b ] ); }
       if( plan->ev_join[ b ] ) { cudaEventDestroy( plan->ev_join[ b ] ); }
+      if( plan->ev_x[ b ] ) { cudaEventDestroy( plan->ev_x[ b ] ); }
    }
    if( plan->ev_fork ) { cudaEventDestroy( plan->ev_fork ); }
    delete plan;

@@ -143,8 +143,8 @@ int dipcu_structure_tensor_backward( dipcu_image_desc const* grad_out, dipcu_ima
  * with both half-widths up to 12 and "mirror", "zero order", "add zeros" or "asym mirror" along
  * both axes run through grouped warp-per-tile launches (one per half-width bucket, per-image work
  * lists); the others through grouped line passes (along x into an intermediate the plan owns,
- * then along y; one pair of launches per half-width bucket); the buckets run as parallel
- * branches.  A persistent launch that pulls (image, tile) work items from a device queue remains
+ * then along y; one launch per pass and per half-width bucket of that pass' axis, the y passes
+ * after all x passes); the buckets run as parallel branches.  A persistent launch that pulls (image, tile) work items from a device queue remains
  * as the fallback (DIPCU_BATCH_NO_LINES routes the rest there).  No DIPlib counterpart (DIPlib
  * filters one image per call; this is dip::GaussFIR per image).
  * `sigmas`, `orders`, `bcs`: host arrays of 2 * count entries (x then y of each image).
