@@ -236,7 +236,8 @@ __global__ void __launch_bounds__( 256 ) batch_kernel( BatchArgs const __grid_co
 // whose row stride is not a multiple of 16 bytes (TMA global strides are) get the same boxes
 // from per-lane cp.async copies with zero fill (8 bytes per lane and row when the row stride and
 // width are even, else 4); every stage fill commits one copy group (empty for TMA boxes), so
-// waiting until SPW - 1 groups are pending finds the current stage's copies done.  Output tiles
+// waiting until SPW - 1 groups are pending finds the current stage's copies done.  Edge tiles of
+// images with "periodic" edges fill their boxes the same way, with the indices wrapped.  Output tiles
 // go out as one TMA store each where the destination layout allows, else as per-lane stores.
 
 struct alignas( 128 ) G2Image {
@@ -256,6 +257,7 @@ struct alignas( 128 ) G2Image {
    int32_t odd[ 2 ];
    int32_t tiles_x, tiles_y;
    int32_t vec_store;       // float2 stores are 8-byte aligned
+   int32_t wrap[ 2 ];       // "periodic" / "asym periodic" along x, y: edge tiles gather their boxes
 };
 
 struct G2Args {
@@ -328,7 +330,55 @@ __global__ void __launch_bounds__( W2Geom< float, B, 32 >::NT, 2 ) batch_ws_kern
          G2Image const* im;
          int x0, y0;
          bool const ok = lookup( t, im, x0, y0 );
-         if( ok && im->tma ) {
+         // A tile that reads samples past a periodic edge gathers its box with wrapped indices.
+         bool const gather = ok && (( im->wrap[ 0 ] && ( x0 - B < 0 || x0 + TX + B > im->n[ 0 ] )) ||
+                                    ( im->wrap[ 1 ] && ( y0 - B < 0 || y0 + TY + B > im->n[ 1 ] )));
+         if( gather ) {
+            if( lane == 0 ) { mbar_arrive( &full[ st ] ); }
+            // Box rows of BW floats, two columns per lane.  Along a periodic axis every index
+            // outside the image is wrapped (negated for "asym periodic": a plain load and store);
+            // along the other axis it is zero-filled, as in the copies below.
+            int const nx = im->n[ 0 ], ny = im->n[ 1 ];
+            int const by = y0 - B, xa = x0 - G::LEAD + 2 * lane;
+            int cx[ 2 ];
+            bool cin[ 2 ], cneg[ 2 ];
+#pragma unroll
+            for( int h = 0; h < 2; ++h ) {
+               int const x = xa + h;
+               cx[ h ] = x;
+               cin[ h ] = x >= 0 && x < nx;
+               cneg[ h ] = false;
+               if( !cin[ h ] && im->wrap[ 0 ] ) {
+                  bool ng;
+                  cx[ h ] = static_cast< int >( bc_map_index( x, nx, im->bc[ 0 ], &ng ));
+                  cin[ h ] = true;
+                  cneg[ h ] = ng;
+               }
+            }
+            float* const dst = reinterpret_cast< float* >( stages + st * G::STAGE_STRIDE );
+            for( int r = 0; r < BH; ++r ) {
+               int const y = by + r;
+               int ry = y;
+               bool rin = y >= 0 && y < ny, rneg = false;
+               if( !rin && im->wrap[ 1 ] ) {
+                  bool ng;
+                  ry = static_cast< int >( bc_map_index( y, ny, im->bc[ 1 ], &ng ));
+                  rin = true;
+                  rneg = ng;
+               }
+#pragma unroll
+               for( int h = 0; h < 2; ++h ) {
+                  bool const in = rin && cin[ h ];
+                  float const* src = in ? im->src + static_cast< int64_t >( ry ) * im->ss1 + cx[ h ] : im->src;
+                  float* const d = dst + r * BW + 2 * lane + h;
+                  if( in && ( rneg != cneg[ h ] )) {
+                     *d = -__ldg( src );
+                  } else {
+                     asm volatile( "cp.async.ca.shared.global [%0], [%1], 4, %2;" :: "r"( smem_u32( d )), "l"( src ), "r"( in ? 4 : 0 ) : "memory" );
+                  }
+               }
+            }
+         } else if( ok && im->tma ) {
             if( lane == 0 ) {
                mbar_arrive_expect_tx( &full[ st ], G::STAGE_BYTES );
                tma_load_4d( stages + st * G::STAGE_STRIDE, &im->tmap, &full[ st ], x0 - G::LEAD, y0 - B, 0, 0 );
@@ -624,7 +674,7 @@ cudaError_t g2_launch( int b, G2Args const& a, int grid, cudaStream_t st ) {
    }
 }
 
-// ---- grouped line passes: every other image (periodic boundaries, half-widths 13 .. 32) as two
+// ---- grouped line passes: every other image (half-widths 13 .. 32, layouts the tile path does not take) as two
 // passes -- along x into a plan-owned intermediate, then along y into the output -- with the
 // register-window line kernels of the fast float path (k_line.cu), one table of images and work
 // lists per pass and per half-width bucket of that pass' axis (4, 8, 12, 16, 24, 32): one launch
@@ -712,7 +762,23 @@ __global__ void __launch_bounds__( kBLXT ) batch_line_x_kernel( BLArgs const __g
          if( im ) {
             if( tid <= HB ) { ws[ buf ][ tid ] = tid <= im->h[ 0 ] ? __ldg( a.wbank + im->wofs[ 0 ] + tid ) : 0.f; }
             float const* srow = im->src + static_cast< int64_t >( row ) * im->ss1;
-            for( int e = tid; e < W; e += kBLXT ) { bl_stage( &tile[ buf ][ e ], srow, a0 - HB + e, im->n0, im->bc[ 0 ] ); }
+            // Segments inside the row whose first sample is 16- (8-) byte aligned go as 16- (8-)
+            // byte copies (W and a0 - HB are multiples of 4).
+            float const* const g = srow + ( a0 - HB );
+            uintptr_t const ga = reinterpret_cast< uintptr_t >( g );
+            if( a0 - HB >= 0 && a0 - HB + W <= im->n0 && ( ga & 7 ) == 0 ) {
+               if(( ga & 15 ) == 0 ) {
+                  for( int e = 4 * tid; e < W; e += 4 * kBLXT ) {
+                     asm volatile( "cp.async.cg.shared.global [%0], [%1], 16;" :: "r"( smem_u32( &tile[ buf ][ e ] )), "l"( g + e ) : "memory" );
+                  }
+               } else {
+                  for( int e = 2 * tid; e < W; e += 2 * kBLXT ) {
+                     asm volatile( "cp.async.ca.shared.global [%0], [%1], 8;" :: "r"( smem_u32( &tile[ buf ][ e ] )), "l"( g + e ) : "memory" );
+                  }
+               }
+            } else {
+               for( int e = tid; e < W; e += kBLXT ) { bl_stage( &tile[ buf ][ e ], srow, a0 - HB + e, im->n0, im->bc[ 0 ] ); }
+            }
          }
       }
       asm volatile( "cp.async.commit_group;" ::: "memory" );
@@ -941,10 +1007,11 @@ namespace {
 
 int plan_fail( int code, std::string const& msg ) { return record_error( code, msg.c_str() ); }
 
-// Images the grouped warp-per-tile path takes: both half-widths up to 12, x-y boundary
-// conditions with every halo source inside the staged box ("mirror", "zero order", "add zeros",
-// "asym mirror"; sizes above the bucket), 4-byte aligned rows (TMA boxes where the layout allows,
-// per-lane copies otherwise).  Their tables and work
+// Images the grouped warp-per-tile path takes: both half-widths up to 12, sizes above the bucket,
+// x-y boundary conditions with every halo source inside the staged box ("mirror", "zero order",
+// "add zeros", "asym mirror") or "periodic" / "asym periodic" (whose edge tiles gather their boxes
+// with wrapped indices), 4-byte aligned rows (TMA boxes where the layout allows, per-lane copies
+// otherwise).  Their tables and work
 // items are uploaded once per plan; `inject` plants one impossible item when the persistent tile
 // kernel gets no items of its own.
 int plan_groups( dipcu_batch_plan* p, int inject ) {
@@ -961,8 +1028,8 @@ int plan_groups( dipcu_batch_plan* p, int inject ) {
                 im.n[ 0 ] < ( 1 << 30 ) && im.n[ 1 ] < ( 1 << 30 );
       for( int d = 0; d < 2 && ok; ++d ) {
          int32_t const bc = im.bc[ d ];
-         ok = ( bc == BC_SYMMETRIC_MIRROR || bc == BC_ZERO_ORDER_EXTRAPOLATE || bc == BC_ADD_ZEROS || bc == BC_ASYMMETRIC_MIRROR ) &&
-              im.n[ d ] > kG2Buckets[ b ];
+         ok = ( bc == BC_SYMMETRIC_MIRROR || bc == BC_ZERO_ORDER_EXTRAPOLATE || bc == BC_ADD_ZEROS || bc == BC_ASYMMETRIC_MIRROR ||
+                bc == BC_PERIODIC || bc == BC_ASYMMETRIC_PERIODIC ) && im.n[ d ] > kG2Buckets[ b ];
       }
       G2Image g{};
       if( !ok ) { ++rest; continue; }
@@ -1000,6 +1067,7 @@ int plan_groups( dipcu_batch_plan* p, int inject ) {
       g.tiles_x = static_cast< int32_t >(( im.n[ 0 ] + tx - 1 ) / tx );
       g.tiles_y = static_cast< int32_t >(( im.n[ 1 ] + 31 ) / 32 );
       g.vec_store = (( reinterpret_cast< uintptr_t >( im.dst ) & 7 ) == 0 && im.ds[ 1 ] % 2 == 0 ) ? 1 : 0;
+      for( int d = 0; d < 2; ++d ) { g.wrap[ d ] = ( im.bc[ d ] == BC_PERIODIC || im.bc[ d ] == BC_ASYMMETRIC_PERIODIC ) ? 1 : 0; }
       int const gi = static_cast< int >( gimg[ b ].size());
       for( int t = 0; t < g.tiles_x * g.tiles_y; ++t ) { gitems[ b ].push_back( BatchItem{ gi, t } ); }
       gimg[ b ].push_back( g );

@@ -202,11 +202,27 @@ __global__ void __launch_bounds__( 128 ) line_x_kernel( LineFastArgs const __gri
    int64_t const a0 = static_cast< int64_t >( blockIdx.x ) * T;
    int64_t const sa = a.sst[ a.axis ], da = a.dstst[ a.axis ];
    // Double-buffered: the copies of the next line segment land while this one is filtered.
+   // Segments inside the line whose first sample is 16- (8-) byte aligned go as 16- (8-) byte
+   // copies (W and a0 - HB are multiples of 4: T = 4 nt, HB a multiple of 4; sa is 1 here).
    auto issue = [ & ]( int64_t u, float* buf ) {
       if( u < a.nouter ) {
          int64_t sb, db;
          fast_decode( a, u, sb, db );
-         for( int e = tid; e < W; e += nt ) { fast_stage( a, buf + e, sb, sa, a0 - HB + e ); }
+         float const* const g = a.src + sb + ( a0 - HB );
+         uintptr_t const ga = reinterpret_cast< uintptr_t >( g );
+         if( a0 - HB >= 0 && a0 - HB + W <= a.n && ( ga & 7 ) == 0 ) {
+            if(( ga & 15 ) == 0 ) {
+               for( int e = 4 * tid; e < W; e += 4 * nt ) {
+                  asm volatile( "cp.async.cg.shared.global [%0], [%1], 16;" :: "r"( smem_u32( buf + e )), "l"( g + e ) : "memory" );
+               }
+            } else {
+               for( int e = 2 * tid; e < W; e += 2 * nt ) {
+                  asm volatile( "cp.async.ca.shared.global [%0], [%1], 8;" :: "r"( smem_u32( buf + e )), "l"( g + e ) : "memory" );
+               }
+            }
+         } else {
+            for( int e = tid; e < W; e += nt ) { fast_stage( a, buf + e, sb, sa, a0 - HB + e ); }
+         }
       }
       asm volatile( "cp.async.commit_group;" ::: "memory" );
    };

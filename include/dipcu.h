@@ -140,8 +140,8 @@ int dipcu_structure_tensor_backward( dipcu_image_desc const* grad_out, dipcu_ima
 
 /* Many 2D sfloat images of uneven sizes, each with its own per-axis sigmas, orders (0..3) and
  * boundary conditions (the index-mapping ones and "add zeros"; half-widths up to 32).  Images
- * with both half-widths up to 12 and "mirror", "zero order", "add zeros" or "asym mirror" along
- * both axes run through grouped warp-per-tile launches (one per half-width bucket, per-image work
+ * with both half-widths up to 12 and "mirror", "zero order", "add zeros", "asym mirror",
+ * "periodic" or "asym periodic" along both axes run through grouped warp-per-tile launches (one per half-width bucket, per-image work
  * lists); the others through grouped line passes (along x into an intermediate the plan owns,
  * then along y; one launch per pass and per half-width bucket of that pass' axis, the y passes
  * after all x passes); the buckets run as parallel branches.  A persistent launch that pulls (image, tile) work items from a device queue remains

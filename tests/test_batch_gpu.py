@@ -110,3 +110,25 @@ def test_batch_tile_path_aligned_and_unaligned_rows(cuda):
     plan, ins, outs = run_plan(imgs, params, graph=False, autotune=False)
     check_all(imgs, params, outs)
     plan.close()
+
+
+def test_batch_tile_path_periodic_edges(cuda):
+    """Images the grouped tile path takes with "periodic" / "asym periodic" edges along one or
+    both axes (their edge tiles gather the boxes with wrapped indices) beside "mirror" / "add
+    zeros" along the other axis; widths multiple of 4 and not, one image narrower than a box."""
+    rng = np.random.default_rng(11)
+    cases = [(64, 0.8, ["periodic", "periodic"]), (67, 1.0, ["asym periodic", "mirror"]),
+             (130, 2.0, ["mirror", "periodic"]), (131, 2.0, ["periodic", "add zeros"]),
+             (200, 3.0, ["asym periodic", "asym periodic"]), (203, 1.0, ["add zeros", "asym periodic"]),
+             (96, 4.0, ["periodic", "periodic"]), (26, 1.0, ["periodic", "asym periodic"])]
+    imgs, params = [], []
+    for i, (w, s, bc) in enumerate(cases):
+        imgs.append(rng.random((45 + 7 * i, w), dtype=np.float32) - 0.5)
+        params.append((s, [i % 3, (i + 1) % 3] if s < 3 else [0, i % 2], bc))
+    plan, ins, outs = run_plan(imgs, params, graph=False, autotune=False)
+    assert plan.info()["grouped_items"] > 0
+    for i, (a, (s, o, bc)) in enumerate(zip(imgs, params)):
+        ref = oracle.gauss_fir(a, [s, s], o, bc, 3.0)
+        err = np.abs(outs[i].cpu().numpy() - ref).max()
+        assert err <= 1e-5 * max(1.0, float(a.max() - a.min())), (i, a.shape, s, o, bc, err)
+    plan.close()
