@@ -7,6 +7,8 @@ runs in libdipcu.so's CUDA kernels through the C-ABI declared in include/dipcu.h
 from .filtering import (BestGaussMethod, BoundaryConditionFromString, Derivative, Error, Gauss, GaussFIR,
                         ParameterError, RunTimeError, flex_dtype, image_desc)
 from .analysis import StructureTensor
+from .derivatives import Gradient, GradientMagnitude, Hessian, Laplace
 
-__all__ = ["BestGaussMethod", "BoundaryConditionFromString", "Derivative", "Error", "Gauss", "GaussFIR",
-           "ParameterError", "StructureTensor", "RunTimeError", "flex_dtype", "image_desc"]
+__all__ = ["BestGaussMethod", "BoundaryConditionFromString", "Derivative", "Error", "Gauss", "GaussFIR", "Gradient",
+           "GradientMagnitude", "Hessian", "Laplace", "ParameterError", "StructureTensor", "RunTimeError",
+           "flex_dtype", "image_desc"]

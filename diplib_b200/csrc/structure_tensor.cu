@@ -3,8 +3,9 @@
 // Forward, as dip::StructureTensor (src/analysis/structure_tensor.cpp:33-59 in DIPlib) with a
 // Gaussian method and no mask: the gradient g_k = GaussFIR(in, sigma_g, order e_k) along each
 // axis of size > 1 (dip::Gradient, src/linear/derivative.cpp:142-172), the symmetric products
-// g_i g_j in DIPlib's symmetric-matrix order (diagonal first, then the upper triangle row by row;
-// dip::Multiply( g, Transpose( g ))), and each product smoothed by GaussFIR(sigma_t).  The
+// g_i g_j in DIPlib's symmetric-matrix order (diagonal first, then the upper triangle column by
+// column, include/diplib/library/tensor.h:100-110, which for the m <= 3 axes here is also row by
+// row; dip::Multiply( g, Transpose( g ))), and each product smoothed by GaussFIR(sigma_t).  The
 // products are formed together and smoothed by one call over the component axis; when that much
 // scratch is not available, per component (at most one product image at a time).
 //

@@ -120,7 +120,7 @@ int dipcu_gauss_fir_backward( dipcu_image_desc const* grad_out, dipcu_image_desc
  * (dip::FindGradientDimensions, src/linear/derivative.cpp:120-138).  `out`: an image of
  * ndims + 1 dimensions, the input's sizes followed by the component axis of m(m+1)/2 entries
  * (m gradient axes) in DIPlib's symmetric-matrix order (diagonal first, then the upper triangle
- * row by row), of the flex type (sfloat, dfloat for 32/64-bit integer and dfloat input); any
+ * column by column: xx, yy, zz, xy, xz, yz), of the flex type (sfloat, dfloat for 32/64-bit integer and dfloat input); any
  * strides, so DIPlib's own layout (component stride 1) and a planar one both work.
  * `grad_sigmas`, `tensor_sigmas`, `bcs`: one entry per input dimension (already broadcast, as
  * dip::ArrayUseParameter does).  The gradient images are scratch of the call (stream-ordered

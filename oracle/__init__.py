@@ -198,13 +198,68 @@ def separable_fir(x: np.ndarray, taps, odd, bcs, out_dtype=None) -> np.ndarray:
     return out
 
 
+def symmetric_pairs(m: int) -> list:
+    """Index pairs of DIPlib's symmetric-matrix storage (include/diplib/library/tensor.h:100-110):
+    the diagonal first, then the elements above it column by column."""
+    return [(i, i) for i in range(m)] + [(i, j) for j in range(1, m) for i in range(j)]
+
+
+def derivative_dims(shape, sigmas, process=None) -> list:
+    """FindGradientDimensions (src/linear/derivative.cpp:120-138) for the Gaussian methods: the
+    DIPlib axes (x first) with process set, size > 1 and sigma > 0."""
+    nd = len(shape)
+    pr = _broadcast(process, nd, True)
+    return [d for d in range(nd) if pr[d] and shape[nd - 1 - d] > 1 and sigmas[d] > 0]
+
+
+def gradient(x: np.ndarray, sigmas, bcs=("mirror",), truncation: float = 3.0, process=None) -> np.ndarray:
+    """dip::Gradient (src/linear/derivative.cpp:142-172): one first derivative per kept axis."""
+    nd = x.ndim
+    sg = _broadcast([sigmas] if np.isscalar(sigmas) else sigmas, nd, 1.0)
+    out = []
+    for d in derivative_dims(x.shape, sg, process):
+        o = [0] * nd
+        o[d] = 1
+        out.append(gauss_fir(x, sg, o, list(bcs), truncation))
+    return np.stack(out)
+
+
+def hessian(x: np.ndarray, sigmas, bcs=("mirror",), truncation: float = 3.0, process=None) -> np.ndarray:
+    """dip::Hessian (src/linear/derivative.cpp:330-372): second derivatives d_ii on the diagonal,
+    mixed d_ij above it, in symmetric-matrix storage order."""
+    nd = x.ndim
+    sg = _broadcast([sigmas] if np.isscalar(sigmas) else sigmas, nd, 1.0)
+    dims = derivative_dims(x.shape, sg, process)
+    out = []
+    for i, j in symmetric_pairs(len(dims)):
+        o = [0] * nd
+        o[dims[i]] += 1
+        o[dims[j]] += 1
+        out.append(gauss_fir(x, sg, o, list(bcs), truncation))
+    return np.stack(out)
+
+
+def laplace(x: np.ndarray, sigmas, bcs=("mirror",), truncation: float = 3.0, process=None) -> np.ndarray:
+    """dip::Laplace, Gaussian methods (src/linear/derivative.cpp:374-418): the sum of the second
+    derivatives along the kept axes, accumulated in the flex type."""
+    nd = x.ndim
+    sg = _broadcast([sigmas] if np.isscalar(sigmas) else sigmas, nd, 1.0)
+    acc = None
+    for d in derivative_dims(x.shape, sg, process):
+        o = [0] * nd
+        o[d] = 2
+        t = gauss_fir(x, sg, o, list(bcs), truncation)
+        acc = t if acc is None else (acc + t).astype(t.dtype)
+    return acc
+
+
 def structure_tensor(x: np.ndarray, grad_sigma, tensor_sigma, bc="mirror", truncation: float = 3.0) -> np.ndarray:
     """dip::StructureTensor (src/analysis/structure_tensor.cpp:33-59) built from the restated
     GaussFIR: the gradient along the axes FindGradientDimensions keeps (src/linear/derivative.cpp:120-138:
     size > 1 and sigma > 0), the products g_i g_j, and the smoothing of each product.  Sigmas and
     boundary conditions are scalars or per-axis lists in DIPlib order.  Returns an array of shape
     (ncomp,) + x.shape with DIPlib's symmetric-matrix component order (diagonal first, then the
-    upper triangle row by row)."""
+    upper triangle column by column, include/diplib/library/tensor.h:100-110)."""
     nd = x.ndim
     gs = [float(grad_sigma)] * nd if np.isscalar(grad_sigma) else [float(s) for s in grad_sigma]
     ts = [float(tensor_sigma)] * nd if np.isscalar(tensor_sigma) else [float(s) for s in tensor_sigma]
@@ -216,7 +271,7 @@ def structure_tensor(x: np.ndarray, grad_sigma, tensor_sigma, bc="mirror", trunc
         o[d] = 1
         grads.append(gauss_fir(x, gs, o, bcs, truncation))
     m = len(dims)
-    pairs = [(i, i) for i in range(m)] + [(i, j) for i in range(m) for j in range(i + 1, m)]
+    pairs = symmetric_pairs(m)
     comps = [gauss_fir((grads[i] * grads[j]).astype(grads[0].dtype), ts, [0] * nd, bcs, truncation)
              for i, j in pairs]
     return np.stack(comps)
