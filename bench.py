@@ -225,12 +225,14 @@ def run_gpu_arm(args):
     # One CUDA graph per (input set, order): each replays exactly one filter launch, so the host
     # keeps the GPU busy and the events below bracket device time only.
     graphs = {}
+    n_launch0 = _launch_count()
     for s in range(NSETS):
         for j in range(len(ORDERS)):
             g = torch.cuda.CUDAGraph()
             with torch.cuda.graph(g):
                 call(s, j)
             graphs[s, j] = g
+    launches_per_step = (_launch_count() - n_launch0) // NSETS   # a step replays one set's graphs
     for s in range(NSETS):
         for j in range(len(ORDERS)):
             graphs[s, j].replay()
@@ -302,7 +304,7 @@ def run_gpu_arm(args):
         "e2e": e2e,
         "clocks": clk.summary(),
         "host_us_per_call": host_call_us,
-        "gpu_launches": args.steps * len(ORDERS),
+        "gpu_launches": args.steps * launches_per_step,
     }
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(host)
@@ -332,6 +334,12 @@ def _device(args):
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     return world, rank, dev
+
+
+def _launch_count() -> int:
+    """Kernel launches libdipcu has issued (host side: a captured launch counts once, at capture)."""
+    from diplib_b200 import _abi
+    return int(_abi.lib().dipcu_launch_count())
 
 
 def _capture(fn):
@@ -678,7 +686,9 @@ def run_fwdbwd(args):
             bwd(i, o)
     torch.cuda.synchronize()
     g_f = [[_capture(lambda i=i, o=o: fwd(i, o)) for o in D_ORDERS] for i in range(nsets)]
+    n0 = _launch_count()
     g_fb = [[_capture(lambda i=i, o=o: (fwd(i, o), bwd_raw(i, o))) for o in D_ORDERS] for i in range(nsets)]
+    launches_per_step = (_launch_count() - n0) // nsets     # a step replays one set's graphs
     for gl in g_f + g_fb:
         for g in gl:
             g.replay()
@@ -695,7 +705,7 @@ def run_fwdbwd(args):
     line["forward_only"] = {"ms_per_step": t_f / args.steps, "gvox_s": world * npx * args.steps / (t_f * 1e-3) / 1e9,
                             "fwd_plus_bwd_over_fwd": t_fb / t_f}
     line["clocks"] = clk
-    line["gpu_launches"] = None
+    line["gpu_launches"] = launches_per_step * args.steps
     if rank == 0 and not args.no_cpu_baseline:
         import oracle
         if oracle.ref_available():
@@ -747,7 +757,9 @@ def run_structure_tensor(args):
         fb(i)
     torch.cuda.synchronize()
     g_f = [[_capture(lambda i=i: fwd(i)) for i in range(S_BATCH)]]
+    n0 = _launch_count()
     g_fb = [[_capture(lambda i=i: fb(i)) for i in range(S_BATCH)]]
+    launches_per_step = _launch_count() - n0               # a step replays all eight graphs
     for gl in g_f + g_fb:
         for g in gl:
             g.replay()
@@ -768,7 +780,7 @@ def run_structure_tensor(args):
     line["forward_only"] = {"ms_per_step": t_f / steps, "gvox_s": world * nvox * steps / (t_f * 1e-3) / 1e9,
                             "fwd_plus_bwd_over_fwd": t_fb / t_f}
     line["clocks"] = clk
-    line["gpu_launches"] = None
+    line["gpu_launches"] = launches_per_step * steps
     if rank == 0 and not args.no_cpu_baseline:
         import oracle
         if oracle.ref_available():

@@ -74,6 +74,7 @@ SIGNATURES = {
     "dipcu_bc_from_string": (ctypes.c_int, [ctypes.c_char_p]),
     "dipcu_last_error_message": (ctypes.c_char_p, []),
     "dipcu_version": (ctypes.c_char_p, []),
+    "dipcu_launch_count": (ctypes.c_uint64, []),
 }
 
 

@@ -1,6 +1,7 @@
 // The C-ABI of libdipcu.so (include/dipcu.h): parameter validation with DIPlib's rules, the
 // per-axis filter set-up of dip::GaussFIR, the pass planning of dip::Framework::Separable, and
 // dispatch to the fused tile kernels (K1) or the line kernel (K2).
+#include <atomic>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -317,6 +318,13 @@ int run_filters( dipcu_image_desc const* in, dipcu_image_desc const* out, std::v
    return status;
 }
 
+namespace {
+std::atomic< uint64_t > g_launches{ 0 };
+} // namespace
+
+void count_launch() { g_launches.fetch_add( 1, std::memory_order_relaxed ); }
+uint64_t launches_so_far() { return g_launches.load( std::memory_order_relaxed ); }
+
 } // namespace dipcu
 
 using namespace dipcu;
@@ -329,6 +337,10 @@ char const* dipcu_last_error_message( void ) {
 
 char const* dipcu_version( void ) {
    return "dipcu 0.1 (sm_100a)";
+}
+
+uint64_t dipcu_launch_count( void ) {
+   return dipcu::launches_so_far();
 }
 
 int dipcu_bc_from_string( char const* bc ) {

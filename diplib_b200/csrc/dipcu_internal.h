@@ -124,6 +124,10 @@ cudaError_t launch_dot( ConvertArgs const& a, bool compute_double, double* out, 
 // Records `msg` as this thread's dipcu_last_error_message() and returns `code`.
 int record_error( int code, char const* msg );
 
+// Counts one kernel launch of this library (host side: a launch captured into a CUDA graph counts
+// once, at capture).  Every launch site calls it right after its <<< >>> statement.
+void count_launch();
+
 // Per-axis filter as dip::GaussFIR builds it (src/linear/gauss.cpp:255-284).
 struct AxisFilter {
    bool process = false;

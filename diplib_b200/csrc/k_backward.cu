@@ -121,7 +121,7 @@ cudaError_t run_fold( FoldPass const& p, cudaStream_t s ) {
    if( a.nentries == 0 || a.nlines == 0 ) { return cudaSuccess; }
    int64_t blocks = ( a.nlines + 127 ) / 128;
    if( blocks > 0x7fffffff ) { return cudaErrorInvalidValue; }
-   fold_kernel< T ><<< static_cast< unsigned >( blocks ), 128, 0, s >>>( a );
+   fold_kernel< T ><<< static_cast< unsigned >( blocks ), 128, 0, s >>>( a ); count_launch();
    return cudaGetLastError();
 }
 
@@ -137,9 +137,9 @@ cudaError_t launch_dot( ConvertArgs const& a, bool compute_double, double* out, 
    if( blocks > 148 * 8 ) { blocks = 148 * 8; }
    if( blocks < 1 ) { blocks = 1; }
    if( compute_double ) {
-      dot_kernel< double ><<< static_cast< unsigned >( blocks ), 256, 0, stream >>>( a, out );
+      dot_kernel< double ><<< static_cast< unsigned >( blocks ), 256, 0, stream >>>( a, out ); count_launch();
    } else {
-      dot_kernel< float ><<< static_cast< unsigned >( blocks ), 256, 0, stream >>>( a, out );
+      dot_kernel< float ><<< static_cast< unsigned >( blocks ), 256, 0, stream >>>( a, out ); count_launch();
    }
    return cudaGetLastError();
 }

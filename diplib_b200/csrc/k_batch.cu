@@ -611,7 +611,7 @@ __global__ void __launch_bounds__( W2Geom< float, B, 32 >::NT, 2 ) batch_ws_kern
 
 template< int B >
 cudaError_t launch_batch_ws( G2Args const& a, int grid, cudaStream_t st ) {
-   batch_ws_kernel< B ><<< grid, W2Geom< float, B, 32 >::NT, G2Geom< B >::BYTES, st >>>( a );
+   batch_ws_kernel< B ><<< grid, W2Geom< float, B, 32 >::NT, G2Geom< B >::BYTES, st >>>( a ); count_launch();
    return cudaGetLastError();
 }
 
@@ -880,7 +880,7 @@ __global__ void __launch_bounds__( 128 ) batch_line_y_kernel( BLArgs const __gri
 
 template< int HB >
 void bl_launch_hb( bool ypass, BLArgs const& a, unsigned grid, cudaStream_t st ) {
-   if( ypass ) { batch_line_y_kernel< HB ><<< grid, 128, 0, st >>>( a ); } else { batch_line_x_kernel< HB ><<< grid, kBLXT, 0, st >>>( a ); }
+   if( ypass ) { batch_line_y_kernel< HB ><<< grid, 128, 0, st >>>( a ); count_launch(); } else { batch_line_x_kernel< HB ><<< grid, kBLXT, 0, st >>>( a ); count_launch(); }
 }
 
 cudaError_t bl_launch( int b, bool ypass, BLArgs const& a, cudaStream_t st ) {
@@ -925,9 +925,9 @@ void const* shape_kernel( int s ) {
 cudaError_t launch_shape( int s, int grid, BatchArgs const& a, cudaStream_t st ) {
    size_t smem = shape_smem( s );
    switch( s ) {
-      case 0: batch_kernel< 64, 32 ><<< grid, 256, smem, st >>>( a ); break;
-      case 1: batch_kernel< 64, 16 ><<< grid, 256, smem, st >>>( a ); break;
-      default: batch_kernel< 128, 32 ><<< grid, 256, smem, st >>>( a ); break;
+      case 0: batch_kernel< 64, 32 ><<< grid, 256, smem, st >>>( a ); count_launch(); break;
+      case 1: batch_kernel< 64, 16 ><<< grid, 256, smem, st >>>( a ); count_launch(); break;
+      default: batch_kernel< 128, 32 ><<< grid, 256, smem, st >>>( a ); count_launch(); break;
    }
    return cudaGetLastError();
 }

@@ -189,7 +189,7 @@ cudaError_t run3d_tma( FusedArgs& a, cudaStream_t s ) {
    int64_t max_ctas = z.units / ( 4 * HZ + 4 );   // keep chunks long against the 2*HZ halo planes
    if( nctas > max_ctas ) { nctas = max_ctas; }
    if( nctas < 1 ) { nctas = 1; }
-   kern<<< static_cast< unsigned >( nctas ), G::NT, smem, s >>>( z );
+   kern<<< static_cast< unsigned >( nctas ), G::NT, smem, s >>>( z ); count_launch();
    return cudaGetLastError();
 }
 
@@ -255,7 +255,7 @@ cudaError_t run3d_ws( FusedArgs& a, cudaStream_t s ) {
       int64_t max_ctas = z.units / ( 4 * HZ + 4 );   // keep chunks long against the 2*HZ halo planes
       if( nctas > max_ctas ) { nctas = max_ctas; }
       if( nctas < 1 ) { nctas = 1; }
-      kern<<< static_cast< unsigned >( nctas ), G::NT, smem, s >>>( z );
+      kern<<< static_cast< unsigned >( nctas ), G::NT, smem, s >>>( z ); count_launch();
       return cudaGetLastError();
    }
 }
@@ -327,7 +327,7 @@ cudaError_t run2d_ws( FusedArgs& a, int32_t const* odd, cudaStream_t s ) {
    int64_t const need = ( z.ntiles + G::NW - 1 ) / G::NW;
    if( nctas > need ) { nctas = need; }
    if( nctas < 1 ) { nctas = 1; }
-   kern<<< static_cast< unsigned >( nctas ), G::NT, smem, s >>>( z );
+   kern<<< static_cast< unsigned >( nctas ), G::NT, smem, s >>>( z ); count_launch();
    return cudaGetLastError();
 }
 
@@ -418,7 +418,7 @@ cudaError_t run_adj2d( Adj2Params const& p, cudaStream_t s ) {
    int64_t const need = ( z.ntiles + G::NW - 1 ) / G::NW;
    if( nctas > need ) { nctas = need; }
    if( nctas < 1 ) { nctas = 1; }
-   kern<<< static_cast< unsigned >( nctas ), G::NT, smem, s >>>( z );
+   kern<<< static_cast< unsigned >( nctas ), G::NT, smem, s >>>( z ); count_launch();
    return cudaGetLastError();
 }
 
@@ -455,7 +455,7 @@ cudaError_t run2d( FusedArgs& a, cudaStream_t s ) {
    a.lz = 1;
    int64_t grid = static_cast< int64_t >( a.tiles_x ) * a.tiles_y * a.nb;
    if( grid > 0x7fffffff ) { return cudaErrorInvalidValue; }
-   kern<<< static_cast< unsigned >( grid ), kNT, smem, s >>>( a );
+   kern<<< static_cast< unsigned >( grid ), kNT, smem, s >>>( a ); count_launch();
    return cudaGetLastError();
 }
 
@@ -493,7 +493,7 @@ cudaError_t run3d( FusedArgs& a, cudaStream_t s ) {
    a.lz = static_cast< int32_t >( lz );
    int64_t grid = base * zchunks;
    if( grid > 0x7fffffff ) { return cudaErrorInvalidValue; }
-   kern<<< static_cast< unsigned >( grid ), kNT, smem, s >>>( a );
+   kern<<< static_cast< unsigned >( grid ), kNT, smem, s >>>( a ); count_launch();
    return cudaGetLastError();
 }
 

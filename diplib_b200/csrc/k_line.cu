@@ -301,8 +301,8 @@ cudaError_t launch_fast_bucket( LineFastArgs const& a, bool along, cudaStream_t 
       int64_t const gy = a.nouter < 65535 ? a.nouter : 65535;
       if( gx > 0x7fffffff ) { return cudaErrorInvalidValue; }
       dim3 const grid( static_cast< unsigned >( gx ), static_cast< unsigned >( gy ));
-      if( a.odd ) { line_x_kernel< HB, true ><<< grid, nt, 0, stream >>>( a ); }
-      else { line_x_kernel< HB, false ><<< grid, nt, 0, stream >>>( a ); }
+      if( a.odd ) { line_x_kernel< HB, true ><<< grid, nt, 0, stream >>>( a ); count_launch(); }
+      else { line_x_kernel< HB, false ><<< grid, nt, 0, stream >>>( a ); count_launch(); }
    } else {
       int const nt = fast_width( a.ncomp, 1 );
       int64_t const gx = ( a.ncomp + nt - 1 ) / nt;
@@ -310,8 +310,8 @@ cudaError_t launch_fast_bucket( LineFastArgs const& a, bool along, cudaStream_t 
       int64_t const gy = work < 65535 ? work : 65535;
       if( gx > 0x7fffffff ) { return cudaErrorInvalidValue; }
       dim3 const grid( static_cast< unsigned >( gx ), static_cast< unsigned >( gy ));
-      if( a.odd ) { line_y_kernel< HB, true ><<< grid, nt, 0, stream >>>( a ); }
-      else { line_y_kernel< HB, false ><<< grid, nt, 0, stream >>>( a ); }
+      if( a.odd ) { line_y_kernel< HB, true ><<< grid, nt, 0, stream >>>( a ); count_launch(); }
+      else { line_y_kernel< HB, false ><<< grid, nt, 0, stream >>>( a ); count_launch(); }
    }
    return cudaGetLastError();
 }
@@ -443,7 +443,7 @@ cudaError_t launch_line( LinePass const& p, cudaStream_t stream ) {
    int64_t gy = nouter < 65535 ? nouter : 65535;
    if( gx > 0x7fffffff ) { return cudaErrorInvalidValue; }
    line_pass_kernel< T, MAXH1 ><<< dim3( static_cast< unsigned >( gx ), static_cast< unsigned >( gy )), 256,
-                                   static_cast< size_t >( smem ), stream >>>( a );
+                                   static_cast< size_t >( smem ), stream >>>( a ); count_launch();
    return cudaGetLastError();
 }
 
@@ -466,9 +466,9 @@ cudaError_t launch_convert( ConvertArgs const& a, bool compute_double, cudaStrea
    if( blocks > 148 * 16 ) { blocks = 148 * 16; }
    if( blocks < 1 ) { blocks = 1; }
    if( compute_double ) {
-      convert_kernel< double ><<< static_cast< unsigned >( blocks ), 256, 0, stream >>>( a );
+      convert_kernel< double ><<< static_cast< unsigned >( blocks ), 256, 0, stream >>>( a ); count_launch();
    } else {
-      convert_kernel< float ><<< static_cast< unsigned >( blocks ), 256, 0, stream >>>( a );
+      convert_kernel< float ><<< static_cast< unsigned >( blocks ), 256, 0, stream >>>( a ); count_launch();
    }
    return cudaGetLastError();
 }

@@ -42,7 +42,7 @@ cudaError_t launch_gauss_weights( double const* sigmas, uint32_t const* orders, 
    if( count <= 0 ) { return cudaSuccess; }
    int threads = 64;
    int blocks = ( count + threads - 1 ) / threads;
-   gauss_weights_kernel<<< blocks, threads, 0, stream >>>( sigmas, orders, count, truncation, weights, dweights, lengths, stride );
+   gauss_weights_kernel<<< blocks, threads, 0, stream >>>( sigmas, orders, count, truncation, weights, dweights, lengths, stride ); count_launch();
    return cudaGetLastError();
 }
 

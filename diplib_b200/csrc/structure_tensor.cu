@@ -50,11 +50,11 @@ cudaError_t elementwise( bool dbl, void* dst, void const* a, void const* b, doub
    if( blocks < 1 ) { blocks = 1; }
    if( dbl ) {
       elementwise_kernel< double ><<< static_cast< unsigned >( blocks ), 256, 0, st >>>(
-            static_cast< double* >( dst ), static_cast< double const* >( a ), static_cast< double const* >( b ), s, n, mode );
+            static_cast< double* >( dst ), static_cast< double const* >( a ), static_cast< double const* >( b ), s, n, mode ); count_launch();
    } else {
       elementwise_kernel< float ><<< static_cast< unsigned >( blocks ), 256, 0, st >>>(
             static_cast< float* >( dst ), static_cast< float const* >( a ), static_cast< float const* >( b ),
-            static_cast< float >( s ), n, mode );
+            static_cast< float >( s ), n, mode ); count_launch();
    }
    return cudaGetLastError();
 }

@@ -206,6 +206,11 @@ char const* dipcu_last_error_message( void );
 /* Library version string. */
 char const* dipcu_version( void );
 
+/* Kernel launches this library has issued since it was loaded, counted on the host: a launch
+ * captured into a CUDA graph counts once, at capture, so a graph's replays launch the count that
+ * its capture added. */
+uint64_t dipcu_launch_count( void );
+
 #ifdef __cplusplus
 }
 #endif

@@ -206,3 +206,17 @@ def test_device_weights_match_oracle(cuda):
         np.testing.assert_array_max_ulp(w[i, :ref.size], ref, maxulp=1)
         exact += int(np.array_equal(w[i, :ref.size], ref))
     assert exact >= len(pairs) * 0.9
+
+
+def test_launch_counter_counts_kernel_launches(cuda):
+    """dipcu_launch_count: one fused-tile launch per plain 2D float GaussFIR call, none for a call
+    that filters nothing (every sigma 0: a conversion copy only when the types differ)."""
+    import torch
+    import diplib_b200 as dip
+    from diplib_b200 import _abi
+    x = torch.rand((256, 300), device="cuda")
+    dip.GaussFIR(x, [2.0], [0], ["mirror"])
+    torch.cuda.synchronize()
+    n0 = _abi.lib().dipcu_launch_count()
+    dip.GaussFIR(x, [2.0], [0], ["mirror"])
+    assert _abi.lib().dipcu_launch_count() - n0 == 1
