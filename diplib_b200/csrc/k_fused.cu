@@ -506,8 +506,8 @@ struct Entry {
 
 // (input type, half-widths, odd flags) instantiated ahead of time.  The set covers the
 // benchmark workloads (2D sigma 2; 2D sigma 3 orders 0..2; 3D sigma (1.5, 1.5, 3) orders
-// (0,0,0)/(1,0,0); the structure tensor's sigma 1 gradients and sigma 4 smoothing) and
-// small-sigma configurations used by the parity tests.
+// (0,0,0)/(1,0,0); the structure tensor's sigma 1 gradients) and small-sigma configurations
+// used by the parity tests.
 #define E2( T, DT, HX, HY, OX, OY ) { 2, DT, HX, HY, 0, OX, OY, 0, &run2d< T, HX, HY, OX, OY > }
 #define E3( T, DT, HX, HY, HZ, OX, OY, OZ ) { 3, DT, HX, HY, HZ, OX, OY, OZ, &run3d< T, HX, HY, HZ, OX, OY, OZ > }
 
@@ -533,8 +533,8 @@ Entry const kTable[] = {
    E3( float, DT_SFLOAT, 3, 4, 3, 0, 1, 0 ),
    E3( float, DT_SFLOAT, 3, 3, 4, 0, 0, 1 ),
    E3( float, DT_SFLOAT, 3, 3, 3, 0, 0, 0 ),
-   // 3D sigma 4 smoothing (structure tensor)
-   E3( float, DT_SFLOAT, 12, 12, 12, 0, 0, 0 ),
+   // (3D sigma 4, half-width 12 on every axis, runs faster as three fast line passes than on the
+   // previous tile kernel, the warp-specialised one not fitting its ring: no entry.)
 };
 
 #undef E2

@@ -133,6 +133,10 @@ struct LineFastArgs {
    int64_t n, ncomp, nouter;    // length along axis, size along comp, lines (x) / column groups (y)
    int64_t sizes[ DIPCU_MAX_DIMS ];
    int64_t sst[ DIPCU_MAX_DIMS ], dstst[ DIPCU_MAX_DIMS ];
+   // The other axes of size > 1, fastest first, with axes that nest in both images (stride =
+   // the previous axis' stride times its size) merged: a contiguous image has one.
+   int32_t nod;
+   int64_t osz[ DIPCU_MAX_DIMS ], osst[ DIPCU_MAX_DIMS ], odst[ DIPCU_MAX_DIMS ];
    float taps[ kFastMaxH + 1 ];  // centre first, zero beyond h
 };
 
@@ -149,14 +153,18 @@ __device__ __forceinline__ float fast_load( LineFastArgs const& a, int64_t base,
 
 // Offsets of the line / column group u over all axes but `axis` (and `comp`).
 __device__ __forceinline__ void fast_decode( LineFastArgs const& a, int64_t u, int64_t& sb, int64_t& db ) {
+   if( a.nod == 1 ) {   // u < osz[ 0 ]
+      sb = u * a.osst[ 0 ];
+      db = u * a.odst[ 0 ];
+      return;
+   }
    sb = 0;
    db = 0;
-   for( int d = 0; d < a.ndims; ++d ) {
-      if( d == a.axis || d == a.comp ) { continue; }
-      int64_t const c = u % a.sizes[ d ];
-      u /= a.sizes[ d ];
-      sb += c * a.sst[ d ];
-      db += c * a.dstst[ d ];
+   for( int d = 0; d < a.nod; ++d ) {
+      int64_t const c = u % a.osz[ d ];
+      u /= a.osz[ d ];
+      sb += c * a.osst[ d ];
+      db += c * a.odst[ d ];
    }
 }
 
@@ -351,6 +359,25 @@ cudaError_t launch_line_fast( LinePass const& p, cudaStream_t stream ) {
       if( d != a.axis && d != a.comp ) { nouter *= p.sizes[ d ]; }
    }
    a.nouter = nouter;
+   a.nod = 0;
+   for( int d = 0; d < p.ndims; ++d ) {
+      if( d == a.axis || d == a.comp || p.sizes[ d ] <= 1 ) { continue; }
+      int const k = a.nod - 1;
+      if( k >= 0 && p.src_strides[ d ] == a.osst[ k ] * a.osz[ k ] && p.dst_strides[ d ] == a.odst[ k ] * a.osz[ k ] ) {
+         a.osz[ k ] *= p.sizes[ d ];
+      } else {
+         a.osz[ a.nod ] = p.sizes[ d ];
+         a.osst[ a.nod ] = p.src_strides[ d ];
+         a.odst[ a.nod ] = p.dst_strides[ d ];
+         ++a.nod;
+      }
+   }
+   if( a.nod == 0 ) {   // a single line (or column group)
+      a.nod = 1;
+      a.osz[ 0 ] = 1;
+      a.osst[ 0 ] = 0;
+      a.odst[ 0 ] = 0;
+   }
    // Buckets at the half-widths of sigma 4 and 8 with order 0 (12, 24) as well as the powers of two.
    int const hb = p.h <= 4 ? 4 : p.h <= 8 ? 8 : p.h <= 12 ? 12 : p.h <= 16 ? 16 : p.h <= 24 ? 24 : 32;
    switch( hb ) {
