@@ -1,20 +1,28 @@
 // K4: batched Gaussian FIR -- many 2D sfloat images of uneven sizes, each with its own sigmas,
-// derivative orders and boundary conditions, filtered by ONE persistent launch.
+// derivative orders and boundary conditions, filtered by a few grouped launches captured as one
+// CUDA graph.
 //
-// A plan (dipcu_batch_plan_*) uploads a table of per-image descriptors, a list of (image, tile)
-// work items sorted by cost, and a device table of (sigma, order) per image axis.  Each run:
-//   1. resets the work-queue counter,
-//   2. builds every image's kernel weights on the device (K0, gauss_weights_kernel), so that a
+// A plan (dipcu_batch_plan_*) classifies every image once and uploads per-group tables of image
+// descriptors and (image, tile) work items, plus a device table of (sigma, order) per image axis.
+// Each run:
+//   1. builds every image's kernel weights on the device (K0, gauss_weights_kernel), so that a
 //      captured run can be replayed after the sigma table is updated in place,
-//   3. launches the persistent kernel: #SMs x occupancy CTAs pop work items from the queue with
-//      one atomicAdd per tile (no waits) until it is empty, and filter their tile with the fused
-//      2D routine specialised for the image's half-width bucket (4, 8, 16 or 32; taps beyond the
-//      image's own half-width are zero).
-// The three steps are captured once into a CUDA graph; a run is one graph launch.  Tile shapes
-// are chosen by an autotuner that times the candidates on the plan's own batch.
+//   2. forks onto four side streams (parallel branches of the graph):
+//      * the grouped line passes (images with half-widths 13-32 or layouts the tile path does not
+//        take): one launch per half-width bucket of the x axis into a plan-owned intermediate,
+//        a join, then one launch per bucket of the y axis into the outputs;
+//      * the grouped warp-per-tile launches (both half-widths up to 12): one per bucket, each warp
+//        streaming its own boxes (TMA where the rows allow, else per-lane copies, gathered with
+//        wrapped indices at periodic edges) through the y and x passes, tiles out by TMA stores
+//        where the destination allows;
+//   3. runs the persistent queue kernel for whatever is left (#SMs x occupancy CTAs pop (image,
+//      tile) items with one atomicAdd each and filter them with the fused 2D routine of the
+//      image's half-width bucket, 4, 8, 16 or 32), and joins the branches.
+// Taps beyond an image's own half-width are zero in every bucketed kernel.  The persistent
+// kernel's tile shape is chosen by an autotuner that times the candidates on the plan's batch.
 //
-// Items that name a non-existent image or tile (a corrupted queue) are skipped and reported as
-// DIPCU_ERR_INVALID_ARG in the device status word -- the kernel never waits on anything.
+// Items that name a non-existent image or tile (a corrupted list) are skipped and reported as
+// DIPCU_ERR_INVALID_ARG in the device status word -- no kernel waits on anything it cannot get.
 #include <cuda_runtime.h>
 
 #include <algorithm>
