@@ -22,7 +22,7 @@
 // kernel's tile shape is chosen by an autotuner that times the candidates on the plan's batch.
 //
 // Items that name a non-existent image or tile (a corrupted list) are skipped and reported as
-// DIPCU_ERR_INVALID_ARG in the device status word -- no kernel waits on anything it cannot get.
+// DIPCU_ERR_INVALID_ARG in the device status word; every wait in these kernels is bounded.
 #include <cuda_runtime.h>
 
 #include <algorithm>
