@@ -7,7 +7,8 @@
 // correlation with the flipped kernel (run by the line kernel with "add zeros" and mirrored taps);
 // the part of C^T y_bar that falls on the 2h halo positions is folded back onto the samples each
 // halo sample was made from, with the coefficients of E (host-computed from the same boundary code
-// the forward uses).  fold_kernel does that fold, one thread per line.
+// the forward uses).  fold_kernel does that fold, one thread per line, or two (one per halo
+// side) when the two sides fold onto disjoint samples.
 //
 // dot_kernel reduces <a, b> over an image in double: the sigma gradient of axis a is
 // <y_bar, G_a'(x)>, with G_a' the forward filter whose axis-a taps are d(taps)/d(sigma).
@@ -29,14 +30,19 @@ struct FoldArgs {
    int64_t gst[ DIPCU_MAX_DIMS ], xst[ DIPCU_MAX_DIMS ];
    int64_t n, nlines;
    int32_t h, odd, nentries;
+   int32_t split;            // > 0: entries [0, split) and [split, nentries) by two threads per line
    T w[ kFoldMaxHalf + 1 ];  // forward taps, centre first
    FoldEntry e[ kFoldMaxEntries ];
 };
 
 template< typename T >
 __global__ void fold_kernel( FoldArgs< T > const __grid_constant__ a ) {
-   int64_t const line = static_cast< int64_t >( blockIdx.x ) * blockDim.x + threadIdx.x;
+   int64_t const tid = static_cast< int64_t >( blockIdx.x ) * blockDim.x + threadIdx.x;
+   bool const two = a.split > 0;
+   int64_t const line = two ? tid >> 1 : tid;
    if( line >= a.nlines ) { return; }
+   int const k0 = ( two && ( tid & 1 )) ? a.split : 0;
+   int const k1 = ( two && !( tid & 1 )) ? a.split : a.nentries;
    int64_t rem = line, gb = 0, xbb = 0;
    for( int d = 0; d < a.ndims; ++d ) {
       if( d == a.axis ) { continue; }
@@ -48,7 +54,7 @@ __global__ void fold_kernel( FoldArgs< T > const __grid_constant__ a ) {
    int64_t const gs = a.gst[ a.axis ], xs = a.xst[ a.axis ];
    int32_t jprev = 0x7fffffff;
    double zj = 0.0;
-   for( int k = 0; k < a.nentries; ++k ) {
+   for( int k = k0; k < k1; ++k ) {
       FoldEntry const en = a.e[ k ];
       if( en.j != jprev ) {
          // Halo gradient: z_bar_j = sum_t g_t w_{j-t} over in-range t with |j - t| <= h.
@@ -57,6 +63,7 @@ __global__ void fold_kernel( FoldArgs< T > const __grid_constant__ a ) {
          int64_t t0 = en.j - a.h, t1 = en.j + a.h;
          if( t0 < 0 ) { t0 = 0; }
          if( t1 > a.n - 1 ) { t1 = a.n - 1; }
+#pragma unroll 4
          for( int64_t t = t0; t <= t1; ++t ) {
             int64_t kk = en.j - t;
             int64_t ak = kk < 0 ? -kk : kk;
@@ -119,7 +126,20 @@ cudaError_t run_fold( FoldPass const& p, cudaStream_t s ) {
    for( int k = 0; k <= p.h; ++k ) { a.w[ k ] = static_cast< T >( p.taps[ k ] ); }
    for( int k = 0; k < p.nentries; ++k ) { a.e[ k ] = p.entries[ k ]; }
    if( a.nentries == 0 || a.nlines == 0 ) { return cudaSuccess; }
-   int64_t blocks = ( a.nlines + 127 ) / 128;
+   // The entries come left halo first (j < 0), then right (j >= n); two threads per line when no
+   // sample receives from both sides.
+   a.split = 0;
+   int split = 0;
+   while( split < p.nentries && p.entries[ split ].j < 0 ) { ++split; }
+   if( split > 0 && split < p.nentries ) {
+      bool disjoint = true;
+      for( int k = 0; k < split && disjoint; ++k ) {
+         for( int m = split; m < p.nentries; ++m ) { disjoint &= p.entries[ k ].i != p.entries[ m ].i; }
+      }
+      if( disjoint ) { a.split = split; }
+   }
+   int64_t const threads = a.nlines * ( a.split > 0 ? 2 : 1 );
+   int64_t blocks = ( threads + 127 ) / 128;
    if( blocks > 0x7fffffff ) { return cudaErrorInvalidValue; }
    fold_kernel< T ><<< static_cast< unsigned >( blocks ), 128, 0, s >>>( a ); count_launch();
    return cudaGetLastError();
