@@ -59,6 +59,114 @@ cudaError_t elementwise( bool dbl, void* dst, void const* a, void const* b, doub
    return cudaGetLastError();
 }
 
+// All products of the structure tensor in one pass: dst[c n + i] = g_{pi[c]}[i] g_{pj[c]}[i] for
+// the nc <= 6 component pairs of m <= 3 gradient images (each gradient sample read once).
+template< typename T >
+struct ProdArgs {
+   T const* g[ 3 ];
+   T* dst;
+   int64_t n;
+   int32_t m, nc;
+   int32_t pi[ 6 ], pj[ 6 ];
+};
+
+template< typename T >
+__device__ __forceinline__ T pick3( T const* v, int k ) { return k == 0 ? v[ 0 ] : k == 1 ? v[ 1 ] : v[ 2 ]; }
+
+template< typename T >
+__global__ void __launch_bounds__( 256 ) products_kernel( ProdArgs< T > const __grid_constant__ a ) {
+   for( int64_t i = static_cast< int64_t >( blockIdx.x ) * blockDim.x + threadIdx.x; i < a.n;
+        i += static_cast< int64_t >( gridDim.x ) * blockDim.x ) {
+      T v[ 3 ] = { T( 0 ), T( 0 ), T( 0 ) };
+#pragma unroll
+      for( int k = 0; k < 3; ++k ) { if( k < a.m ) { v[ k ] = a.g[ k ][ i ]; } }
+#pragma unroll
+      for( int c = 0; c < 6; ++c ) {
+         if( c < a.nc ) { a.dst[ c * a.n + i ] = pick3( v, a.pi[ c ] ) * pick3( v, a.pj[ c ] ); }
+      }
+   }
+}
+
+// The gradient images' adjoints in one pass: for every component c = (i, j) in order,
+// gb_i += 2 q_c g_i (i == j), else gb_i += q_c g_j and gb_j += q_c g_i -- the same operations, in
+// the same order, as one accumulation launch per term; gb starts at zero.
+template< typename T >
+struct GbarArgs {
+   T const* q;       // nc components, stride n
+   T const* g[ 3 ];
+   T* gb[ 3 ];
+   int64_t n;
+   int32_t m, nc;
+   int32_t pi[ 6 ], pj[ 6 ];
+};
+
+template< typename T >
+__global__ void __launch_bounds__( 256 ) gbar_kernel( GbarArgs< T > const __grid_constant__ a ) {
+   for( int64_t i = static_cast< int64_t >( blockIdx.x ) * blockDim.x + threadIdx.x; i < a.n;
+        i += static_cast< int64_t >( gridDim.x ) * blockDim.x ) {
+      T v[ 3 ] = { T( 0 ), T( 0 ), T( 0 ) }, acc[ 3 ] = { T( 0 ), T( 0 ), T( 0 ) };
+#pragma unroll
+      for( int k = 0; k < 3; ++k ) { if( k < a.m ) { v[ k ] = a.g[ k ][ i ]; } }
+#pragma unroll
+      for( int c = 0; c < 6; ++c ) {
+         if( c >= a.nc ) { continue; }
+         T const qc = a.q[ c * a.n + i ];
+         int const ci = a.pi[ c ], cj = a.pj[ c ];
+#pragma unroll
+         for( int k = 0; k < 3; ++k ) {
+            if( ci == cj ) {
+               if( k == ci ) { acc[ k ] = fma( qc * v[ k ], T( 2 ), acc[ k ] ); }
+            } else if( k == ci ) {
+               acc[ k ] = fma( qc * pick3( v, cj ), T( 1 ), acc[ k ] );
+            } else if( k == cj ) {
+               acc[ k ] = fma( qc * pick3( v, ci ), T( 1 ), acc[ k ] );
+            }
+         }
+      }
+#pragma unroll
+      for( int k = 0; k < 3; ++k ) { if( k < a.m ) { a.gb[ k ][ i ] = acc[ k ]; } }
+   }
+}
+
+template< typename Args, typename Kern >
+cudaError_t launch_flat( Kern kern, Args const& a, int64_t n, cudaStream_t st ) {
+   int64_t blocks = ( n + 255 ) / 256;
+   if( blocks > 148 * 16 ) { blocks = 148 * 16; }
+   if( blocks < 1 ) { blocks = 1; }
+   kern<<< static_cast< unsigned >( blocks ), 256, 0, st >>>( a ); count_launch();
+   return cudaGetLastError();
+}
+
+using Pairs = std::vector< std::pair< int, int >>;
+
+template< typename T >
+cudaError_t products( int64_t n, Pairs const& comps, std::vector< void* > const& g, void* dst, cudaStream_t st ) {
+   ProdArgs< T > a{};
+   for( size_t k = 0; k < g.size() && k < 3; ++k ) { a.g[ k ] = static_cast< T const* >( g[ k ] ); }
+   a.dst = static_cast< T* >( dst );
+   a.n = n;
+   a.m = static_cast< int32_t >( g.size());
+   a.nc = static_cast< int32_t >( comps.size());
+   for( size_t c = 0; c < comps.size(); ++c ) { a.pi[ c ] = comps[ c ].first; a.pj[ c ] = comps[ c ].second; }
+   return launch_flat( products_kernel< T >, a, n, st );
+}
+
+template< typename T >
+cudaError_t gradient_adjoints( int64_t n, Pairs const& comps, void const* q_all, std::vector< void* > const& g,
+                               std::vector< void* > const& gb, cudaStream_t st ) {
+   GbarArgs< T > a{};
+   a.q = static_cast< T const* >( q_all );
+   for( size_t k = 0; k < g.size() && k < 3; ++k ) {
+      a.g[ k ] = static_cast< T const* >( g[ k ] );
+      a.gb[ k ] = static_cast< T* >( gb[ k ] );
+   }
+   a.n = n;
+   a.m = static_cast< int32_t >( g.size());
+   a.nc = static_cast< int32_t >( comps.size());
+   for( size_t c = 0; c < comps.size(); ++c ) { a.pi[ c ] = comps[ c ].first; a.pj[ c ] = comps[ c ].second; }
+   return launch_flat( gbar_kernel< T >, a, n, st );
+}
+
 struct Scratch {
    std::vector< void* > bufs;
    cudaStream_t st;
@@ -184,12 +292,9 @@ int dipcu_structure_tensor( dipcu_image_desc const* in, dipcu_image_desc const* 
    if( !prod_all && !prod ) { return record_error( DIPCU_ERR_CUDA, "cudaMallocAsync (product)" ); }
    if( int st = gradients( in, s, grad_sigmas, bcs, truncation, g, stream )) { return st; }
    if( prod_all ) {
-      for( size_t c = 0; c < nc; ++c ) {
-         cudaError_t e = elementwise( s.cdouble, static_cast< char* >( prod_all ) + c * bytes,
-                                      g[ static_cast< size_t >( s.comps[ c ].first ) ], g[ static_cast< size_t >( s.comps[ c ].second ) ],
-                                      1.0, s.n, 0, stream );
-         if( e != cudaSuccess ) { return record_error( DIPCU_ERR_CUDA, cudaGetErrorString( e )); }
-      }
+      cudaError_t const e = s.cdouble ? products< double >( s.n, s.comps, g, prod_all, stream )
+                                      : products< float >( s.n, s.comps, g, prod_all, stream );
+      if( e != cudaSuccess ) { return record_error( DIPCU_ERR_CUDA, cudaGetErrorString( e )); }
       dipcu_image_desc pall = s.plain;
       pall.ndims = s.nd + 1;
       pall.data = prod_all;
@@ -271,11 +376,14 @@ int dipcu_structure_tensor_backward( dipcu_image_desc const* grad_out, dipcu_ima
          return st;
       }
    }
-   for( size_t c = 0; c < nc; ++c ) {
+   if( q_all ) {   // all components' adjoints at hand: one pass over the images
+      cudaError_t const e = s.cdouble ? gradient_adjoints< double >( s.n, s.comps, q_all, g, gb, stream )
+                                      : gradient_adjoints< float >( s.n, s.comps, q_all, g, gb, stream );
+      if( e != cudaSuccess ) { return record_error( DIPCU_ERR_CUDA, cudaGetErrorString( e )); }
+   }
+   for( size_t c = 0; c < nc && !q_all; ++c ) {
       void* qc = q;
-      if( q_all ) {
-         qc = static_cast< char* >( q_all ) + c * bytes;
-      } else {
+      {
          dipcu_image_desc wc = component( grad_out, static_cast< int >( c ), s.nd );
          if( int st = dipcu_gauss_fir_backward( &wc, nullptr, &qimg, nullptr, tensor_sigmas, zero.data(), bcs, truncation,
                                                 stream )) {
