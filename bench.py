@@ -322,6 +322,18 @@ def _device(args):
     return world, rank, dev
 
 
+def _max_over_ranks(v: float, dev) -> float:
+    """The largest `v` over all ranks of the process group (every rank takes this collective
+    step), or `v` itself on one process."""
+    import torch
+    import torch.distributed as dist
+    if not dist.is_available() or not dist.is_initialized() or dist.get_world_size() == 1:
+        return float(v)
+    t = torch.tensor([float(v)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def _launch_count() -> int:
     """Kernel launches libdipcu has issued (host side: a captured launch counts once, at capture)."""
     from diplib_b200 import _abi
@@ -360,11 +372,7 @@ def _timed_steps(rot, nrot, singles, steps, dev):
         torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    total = start.elapsed_time(stop)
-    if world > 1:
-        t = torch.tensor([total], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total = float(t.item())
+    total = _max_over_ranks(start.elapsed_time(stop), dev)
     return total, clk.summary()
 
 
@@ -391,11 +399,7 @@ def _timed(graph_lists, steps, dev):
         torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    total = start.elapsed_time(stop)
-    if world > 1:
-        t = torch.tensor([total], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total = float(t.item())
+    total = _max_over_ranks(start.elapsed_time(stop), dev)
     return total, [a.elapsed_time(b) for a, b in ev], clk.summary()
 
 
@@ -534,12 +538,7 @@ def _e2e(up, parts, nvox, dev, world, h2d, d2h, steps=20):
     run(steps)
     e1.record(main)
     torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / steps
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = _max_over_ranks(e0.elapsed_time(e1) / steps, dev)
     return {"value": world * nvox / (ms * 1e-3) / 1e9, "unit": "Gvox/s", "h2d_bytes_per_step": int(h2d),
             "d2h_bytes_per_step": int(d2h), "ms_per_step": ms,
             "pipelining": "uploads, work and downloads on three streams, two device buffer sets"}
