@@ -90,6 +90,11 @@ def ref_lib():
                                                  ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
                                                  ctypes.POINTER(ctypes.c_int), ctypes.c_char_p,
                                                  ctypes.c_int]
+        _ref.dipref_derivative_op.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _i64p,
+                                              ctypes.c_void_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_int,
+                                              ctypes.c_double, ctypes.c_char_p, ctypes.c_void_p, ctypes.c_int,
+                                              ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                              ctypes.c_char_p, ctypes.c_int]
     return _ref
 
 
@@ -351,3 +356,30 @@ def ref_structure_tensor(x: np.ndarray, grad_sigma: float, tensor_sigma: float, 
         raise RuntimeError(errbuf.value.decode() or "StructureTensor failed")
     out = out[:x.size * ncomp.value].reshape(x.shape + (ncomp.value,))
     return np.moveaxis(out, -1, 0).copy()
+
+
+def ref_derivative_op(which: str, x: np.ndarray, sigmas, bcs=("mirror",), truncation: float = 3.0,
+                      method: str = "gaussFIR") -> np.ndarray:
+    """dip::Gradient / GradientMagnitude / Hessian / Laplace of the reference
+    (src/linear/derivative.cpp:142-418); returns (ncomp,) + x.shape, or x.shape for the scalar
+    results (GradientMagnitude, Laplace)."""
+    code_of = {"gradient": 0, "gradient_magnitude": 1, "hessian": 2, "laplace": 3}
+    nd = x.ndim
+    maxcomp = nd * (nd + 1) // 2
+    sizes, _ = _dip_geometry(x)
+    x = np.ascontiguousarray(x)
+    sg = np.asarray([sigmas] if np.isscalar(sigmas) else list(sigmas), dtype=np.float64)
+    bl = [bcs] if isinstance(bcs, str) else list(bcs)
+    out = np.zeros(x.size * maxcomp, suggest_flex(x.dtype))
+    code = ctypes.c_int(0)
+    ncomp = ctypes.c_int(0)
+    errbuf = ctypes.create_string_buffer(512)
+    rc = ref_lib().dipref_derivative_op(code_of[which], x.ctypes.data, DTYPE_CODES[x.dtype], nd, sizes,
+                                        sg.ctypes.data, len(sg), "\n".join(bl).encode(), int(len(bl) > 0),
+                                        truncation, method.encode(), out.ctypes.data, maxcomp, ctypes.byref(code),
+                                        ctypes.byref(ncomp), errbuf, 512)
+    if rc != 0:
+        raise RuntimeError(errbuf.value.decode() or which + " failed")
+    n = ncomp.value
+    out = out[:x.size * n].reshape(x.shape + (n,))
+    return out[..., 0].copy() if which in ("gradient_magnitude", "laplace") else np.moveaxis(out, -1, 0).copy()

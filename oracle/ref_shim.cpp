@@ -4,6 +4,7 @@
 // CPU leg can call the reference's own Gaussian FIR path on raw host buffers:
 //   dip::Gauss               src/linear/derivative.cpp:62-86
 //   dip::StructureTensor     src/analysis/structure_tensor.cpp:33-59
+//   dip::Gradient, GradientMagnitude, Hessian, Laplace  src/linear/derivative.cpp:142-418
 //   dip::MakeHalfGaussian    src/linear/gauss.cpp:151-165
 //   dip::detail::ExpandBuffer src/library/copy_buffer.cpp:751-813
 //   dip::ReadPixelWithBoundaryCondition src/library/boundary.cpp:47-128
@@ -146,6 +147,36 @@ int dipref_structure_tensor(
       *out_dtype = TypeToCode( res.DataType() );
       *ncomp = static_cast< int >( res.TensorElements() );
       if( *ncomp > ndims * ( ndims + 1 ) / 2 ) { return 1; }
+      CopyOut( res, out );
+      return 0;
+   } catch( dip::Error const& e ) {
+      SetErr( err, errlen, e.what() );
+      return 1;
+   }
+}
+
+// which: 0 dip::Gradient, 1 dip::GradientMagnitude, 2 dip::Hessian, 3 dip::Laplace, with the
+// given method; `bcs` as in dipref_gauss.  Output: the tensor components per pixel, interleaved
+// (normal strides), at most `maxcomp` of them; the data type in *out_dtype, the count in *ncomp.
+int dipref_derivative_op(
+      int which, void const* in, int in_dtype, int ndims, int64_t const* sizes,
+      double const* sigmas, int nsigmas, char const* bcs, int has_bcs, double truncation, char const* method,
+      void* out, int maxcomp, int* out_dtype, int* ncomp, char* err, int errlen ) {
+   try {
+      dip::Image img = Wrap( in, in_dtype, ndims, sizes, nullptr );
+      dip::FloatArray s( static_cast< dip::uint >( nsigmas ));
+      for( int ii = 0; ii < nsigmas; ++ii ) { s[ ii ] = sigmas[ ii ]; }
+      dip::StringArray bc = SplitList( bcs, has_bcs != 0 );
+      dip::Image res;
+      switch( which ) {
+         case 0: dip::Gradient( img, res, s, method, bc, {}, truncation ); break;
+         case 1: dip::GradientMagnitude( img, res, s, method, bc, {}, truncation ); break;
+         case 2: dip::Hessian( img, res, s, method, bc, {}, truncation ); break;
+         default: dip::Laplace( img, res, s, method, bc, {}, truncation ); break;
+      }
+      *out_dtype = TypeToCode( res.DataType() );
+      *ncomp = static_cast< int >( res.TensorElements() );
+      if( *ncomp > maxcomp ) { return 1; }
       CopyOut( res, out );
       return 0;
    } catch( dip::Error const& e ) {

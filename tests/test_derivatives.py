@@ -73,3 +73,22 @@ def test_derivatives_reject_what_the_fir_path_does_not_take(cuda):
         dip.Hessian(x, [1.0], "finitediff")
     with pytest.raises(dip.ParameterError):
         dip.Gradient(x, [0.0])          # no axis with sigma > 0: DIPlib's E::DIMENSIONALITY_NOT_SUPPORTED
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="the compiled reference (oracle/_ref) is not built")
+@pytest.mark.parametrize("case", range(len(CASES)))
+def test_oracle_compositions_are_the_reference(case):
+    """Pins the oracle's compositions to the reference's own dip::Gradient / GradientMagnitude /
+    Hessian / Laplace (oracle/_ref): bit-exact for the first three (the same GaussFIR calls in
+    the same order, the Hessian's components in the same storage order), within float rounding
+    for the magnitude, which this test forms in double."""
+    shape, sg, bc, dt, _ = CASES[case]
+    x = _input(shape, dt, 60 + case)
+    for which, fn in (("gradient", oracle.gradient), ("hessian", oracle.hessian), ("laplace", oracle.laplace)):
+        ref = oracle.ref_derivative_op(which, x, sg, bc)
+        got = fn(x, sg, bc, 3.0)
+        assert ref.shape == got.shape and ref.dtype == got.dtype, which
+        assert np.array_equal(ref, got), (which, float(np.abs(ref - got).max()))
+    ref = oracle.ref_derivative_op("gradient_magnitude", x, sg, bc)
+    g = oracle.gradient(x, sg, bc, 3.0).astype(np.float64)
+    assert np.abs(ref - np.sqrt((g ** 2).sum(axis=0))).max() <= 1e-6 * max(1.0, float(np.abs(ref).max()))
