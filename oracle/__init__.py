@@ -383,3 +383,20 @@ def ref_derivative_op(which: str, x: np.ndarray, sigmas, bcs=("mirror",), trunca
     n = ncomp.value
     out = out[:x.size * n].reshape(x.shape + (n,))
     return out[..., 0].copy() if which in ("gradient_magnitude", "laplace") else np.moveaxis(out, -1, 0).copy()
+
+
+def ref_read_pixel_bc(img: np.ndarray, coords, bcs) -> float:
+    """dip::ReadPixelWithBoundaryCondition of the reference (src/library/boundary.cpp:47-128) on a
+    scalar sfloat image; `coords` (which may lie outside the image) and `bcs` (enumerator codes)
+    in DIPlib order, x first."""
+    img = np.ascontiguousarray(img, np.float32)
+    nd = img.ndim
+    sizes = (ctypes.c_int64 * nd)(*reversed(img.shape))
+    c = (ctypes.c_int64 * nd)(*coords)
+    b = (ctypes.c_int * nd)(*bcs)
+    out = ctypes.c_float(0.0)
+    rc = ref_lib().dipref_read_pixel_bc(ctypes.c_void_p(img.ctypes.data), ctypes.c_int(nd), sizes, c, b,
+                                        ctypes.byref(out))
+    if rc != 0:
+        raise RuntimeError("ReadPixelWithBoundaryCondition failed")
+    return float(out.value)

@@ -121,3 +121,31 @@ def test_boundary_closed_forms_match_expand_buffer():
                     np.testing.assert_allclose(got, ref, rtol=1e-6, atol=1e-5)
                 else:
                     assert np.array_equal(got, ref), (bc, n, border)
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="the compiled reference (oracle/_ref) is not built")
+def test_read_pixel_known_answers_of_the_reference():
+    """The reference's own check of ReadPixelWithBoundaryCondition (src/library/boundary.cpp:331-381):
+    a 15 x 10 sfloat image of uniform noise in [0.5, 3.8), read at coordinates just outside the
+    image and around the turn into the second reflection or period, for every boundary condition
+    it lists.  Here the kernels' closed-form extension, applied separably (rows along x, then
+    columns along y), must give the reference's value exactly."""
+    l = _hl()
+    rng = np.random.default_rng(11)
+    img = rng.uniform(0.5, 3.8, size=(10, 15)).astype(np.float32)   # DIPlib sizes {15, 10}
+    coords = [(0, 0), (-1, 0), (0, -1), (-1, -1), (20, 14), (19, 15), (20, 15), (28, -9), (29, -9), (28, -10),
+              (29, -10), (30, -10), (29, -11), (30, -11)]
+    bx, by = 20, 16
+
+    def ext(line, border, code):
+        line = np.ascontiguousarray(line, np.float32)
+        out = np.zeros(line.size + 2 * border, np.float32)
+        l.hl_extend_f32(line.ctypes.data, line.size, border, code, out.ctypes.data)
+        return out
+
+    for bc in ["mirror", "asym mirror", "periodic", "asym periodic", "add zeros", "add max", "add min", "zero order"]:
+        code = oracle.BC_CODES[bc]
+        rows = np.stack([ext(img[y], bx, code) for y in range(img.shape[0])])
+        full = np.stack([ext(rows[:, c], by, code) for c in range(rows.shape[1])], axis=1)
+        for x, y in coords:
+            assert full[y + by, x + bx] == oracle.ref_read_pixel_bc(img, [x, y], [code, code]), (bc, x, y)

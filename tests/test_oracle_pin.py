@@ -110,3 +110,19 @@ def test_structure_tensor_matches_live_reference():
         got = oracle.structure_tensor(x, gsig, tsig, bc, 3.0)
         assert got.shape == ref.shape and got.dtype == ref.dtype, (shape, got.shape, ref.shape)
         np.testing.assert_allclose(got, ref, rtol=0, atol=1e-6 * np.abs(ref).max(), err_msg=str((shape, bc)))
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="the compiled reference (oracle/_ref) is not built")
+def test_reference_one_thread_equals_all_threads():
+    """The reference's own multithreading check (src/linear/gauss.cpp:547-569): dip::Gauss with
+    sigma 2 of a 256 x 192 x 59 dfloat noise volume gives the same samples with one thread and
+    with all of them -- the configuration the bench's reference arm runs in."""
+    x = np.random.default_rng(0).standard_normal((59, 192, 256))
+    try:
+        oracle.ref_set_threads(1)
+        one = oracle.ref_gauss(x, [2.0], [0], None, 3.0)
+        oracle.ref_set_threads(0)
+        many = oracle.ref_gauss(x, [2.0], [0], None, 3.0)
+    finally:
+        oracle.ref_set_threads(0)
+    assert np.array_equal(one, many)
