@@ -185,7 +185,7 @@ def run_reference_arm(args):
         "metric": METRIC, "value": value, "unit": "Gvox/s", "impl": "reference", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded uniform 0..4095)",
-        "config": dict(CONFIG, parallelism="CPU, DIPlib OpenMP"),
+        "config": dict({k: v for k, v in CONFIG.items() if k != "graphs"}, parallelism="CPU, DIPlib OpenMP"),
         "cpu_baseline": {"value": value, "unit": "Gvox/s", "cores": cores, "kind": "reference",
                          "sample": f"full 256^3 step (both orders) x {args.steps}, {cores} threads"},
         "e2e": {"value": value, "unit": "Gvox/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},

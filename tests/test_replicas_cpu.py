@@ -60,3 +60,31 @@ def bench_single_process_max() -> float:
     import torch
     import bench
     return bench._max_over_ranks(3.0, torch.device("cpu"))
+
+
+def test_reference_arm_prints_the_contract_line():
+    """`bench.py --impl reference` times the compiled reference on the host cores and prints one
+    JSON line with the headline's metric, unit and workload, `impl`, a `cpu_baseline` describing
+    the run and an `e2e` with no host-device traffic (or an `unavailable` line without the
+    reference build)."""
+    import json
+    import subprocess
+    import sys
+
+    import oracle
+    from tests.conftest import ROOT
+    r = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--steps", "1", "--warmup", "0"],
+                       cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference"
+    if not oracle.ref_available():
+        assert "unavailable" in d
+        return
+    import bench
+    assert d["metric"] == bench.METRIC and d["unit"] == "Gvox/s" and d["higher_is_better"] is True
+    assert d["value"] > 0 and d["config"]["workload"] == bench.CONFIG["workload"]
+    assert d["cpu_baseline"]["kind"] == "reference" and d["cpu_baseline"]["cores"] >= 1
+    assert d["e2e"]["value"] == d["value"] and d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
