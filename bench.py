@@ -71,9 +71,23 @@ def cpu_reference_step(x, threads):
         oracle.ref_gauss(x, SIGMAS, o, BCS, TRUNC)
 
 
+def cpu_model() -> str:
+    """The host CPU's model name (/proc/cpuinfo), or the platform's processor string."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
 def cpu_baseline(x, budget_s=12.0, max_reps=40):
     """The reference's OpenMP CPU path (or the oracle port if the reference was not built) on
-    this host, timed on the full headline volume; min over repetitions, bounded by `budget_s`."""
+    this host, timed on the full headline volume; min over repetitions, bounded by `budget_s`.
+    Also one thread (min of 2 reps) and the CPU model."""
     import oracle
     nvox = 2 * x.size
     if oracle.ref_available():
@@ -85,10 +99,17 @@ def cpu_baseline(x, budget_s=12.0, max_reps=40):
             t0 = time.perf_counter()
             cpu_reference_step(x, 0)
             times.append(time.perf_counter() - t0)
+        t1 = []
+        for _ in range(2):
+            t0 = time.perf_counter()
+            cpu_reference_step(x, 1)
+            t1.append(time.perf_counter() - t0)
+        oracle.ref_set_threads(0)
         return {"value": nvox / min(times) / 1e9, "unit": "Gvox/s", "cores": cores, "kind": "reference",
                 "sample": f"full 256^3 step (both orders), min of {len(times)} reps, "
                           f"DIPlib sources built with -O3 -fopenmp, {cores} threads",
-                "ms_per_step": min(times) * 1e3}
+                "ms_per_step": min(times) * 1e3, "cpu_model": cpu_model(), "host_cpus": os.cpu_count(),
+                "value_1thread": nvox / min(t1) / 1e9, "ms_per_step_1thread": min(t1) * 1e3}
     # Oracle port: single thread on a z-slab sample of the volume.
     sl = x[:32]
     t0 = time.perf_counter()
@@ -187,7 +208,8 @@ def run_reference_arm(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded uniform 0..4095)",
         "config": dict({k: v for k, v in CONFIG.items() if k != "graphs"}, parallelism="CPU, DIPlib OpenMP"),
         "cpu_baseline": {"value": value, "unit": "Gvox/s", "cores": cores, "kind": "reference",
-                         "sample": f"full 256^3 step (both orders) x {args.steps}, {cores} threads"},
+                         "sample": f"full 256^3 step (both orders) x {args.steps}, {cores} threads",
+                         "cpu_model": cpu_model()},
         "e2e": {"value": value, "unit": "Gvox/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -294,12 +316,60 @@ def run_gpu_arm(args):
     }
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(host)
+    del xs, outs, d_in, d_out
+    torch.cuda.empty_cache()
+    if not args.headline_only:
+        line.update(other_workloads(args, achieved / peak))
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line))
     return 0
+
+
+def other_workloads(args, headline_frac):
+    """The rest of the metric, measured in the same run: the plain 2D image, the batched uneven
+    launch against the plain path, forward + backward against forward, and the structure tensor;
+    each with its own roofline fraction (of the same measured peak), plus the three targets."""
+    import argparse as _ap
+    import torch
+    sub = _ap.Namespace(**vars(args))
+    sub.steps = max(10, min(args.steps, 20))
+    out = {}
+    p2 = run_gauss2d(sub, embedded=True)
+    out["plain2d"] = {"workload": p2["config"]["workload"], "value": p2["value"], "unit": "Gvox/s",
+                      "ms_per_step": p2["ms_per_step"], "frac": p2["roofline"]["frac"],
+                      "kernel": p2["roofline"]["kernel"], "l2_flushed": p2["config"]["l2"],
+                      "l2_resident_value": p2["l2_resident"]["value"]}
+    torch.cuda.empty_cache()
+    b = run_batch(sub, embedded=True)
+    out["batched"] = {"workload": b["config"]["workload"], "value": b["value"], "unit": "Gvox/s",
+                      "ms_per_run": b["ms_per_step"], "frac": b["roofline"]["frac"],
+                      "vs_plain": b["vs_plain_large_image"]["ratio"],
+                      "plain_large_image_gvox_s": b["vs_plain_large_image"]["plain_gvox_s"],
+                      "plain_how": b["vs_plain_large_image"]["how"],
+                      "vs_per_combination": b["vs_single_image"]["ratio"],
+                      "per_combination_how": b["vs_single_image"]["how"],
+                      "kernels_per_run": b["config"]["plan"]["kernels_per_run"]}
+    torch.cuda.empty_cache()
+    d = run_fwdbwd(sub, embedded=True)
+    out["fwdbwd"] = {"workload": d["config"]["workload"], "fwd_ms": d["forward_only"]["ms_per_step"],
+                     "fwdbwd_ms": d["ms_per_step"], "ratio": d["forward_only"]["fwd_plus_bwd_over_fwd"],
+                     "value": d["value"], "unit": "Gvox/s", "frac": d["roofline"]["frac"],
+                     "fwd_frac": d["forward_only"]["roofline"]["frac"]}
+    torch.cuda.empty_cache()
+    st = run_structure_tensor(sub, embedded=True)
+    out["structure_tensor"] = {"workload": st["config"]["workload"], "value": st["value"], "unit": "Gvox/s",
+                               "ms_per_step": st["ms_per_step"], "frac": st["roofline"]["frac"],
+                               "fwd_plus_bwd_over_fwd": st["forward_only"]["fwd_plus_bwd_over_fwd"]}
+    torch.cuda.empty_cache()
+    out["targets"] = {
+        "forward_ge_70pct_hbm": {"value": headline_frac, "met": headline_frac >= 0.70},
+        "batched_ge_80pct_of_plain": {"value": out["batched"]["vs_plain"], "met": out["batched"]["vs_plain"] >= 0.80},
+        "fwdbwd_le_2p5x_fwd": {"value": out["fwdbwd"]["ratio"], "met": out["fwdbwd"]["ratio"] <= 2.5},
+    }
+    return out
 
 
 # ------------------------------------------------------------------------------------------------
@@ -316,7 +386,8 @@ def _device(args):
         import datetime
         import torch.distributed as dist
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        if not dist.is_initialized():
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     return world, rank, dev
@@ -442,7 +513,7 @@ G2_CONFIG = {"workload": "dip::Gauss FIR 2D 1024^2 sfloat, sigma (2,2), order (0
              "graphs": "one CUDA graph per rotation of 32 steps (remainder steps one graph each)"}
 
 
-def run_gauss2d(args):
+def run_gauss2d(args, embedded=False):
     import torch
     import diplib_b200 as dipcu
     world, rank, dev = _device(args)
@@ -474,6 +545,15 @@ def run_gauss2d(args):
                         "avg_kernel_ms": avg}
     line["clocks"] = clk
     line["gpu_launches"] = args.steps
+    # L2-resident: the same input and output every step (8 MB working set stays in the 126 MB L2).
+    same = _capture(lambda: [call(0) for _ in range(nsets)])
+    same.replay()
+    t_res, _ = _timed_steps(same, nsets, [graphs[0]] * nsets, args.steps, dev)
+    line["l2_resident"] = {"value": world * npx * args.steps / (t_res * 1e-3) / 1e9, "unit": "Gvox/s",
+                           "ms_per_step": t_res / args.steps,
+                           "how": "one input/output set replayed back to back (8 MB, stays in L2)"}
+    if embedded:
+        return line
     # e2e: pinned host image in, result out.
     h_in = torch.from_numpy(host).pin_memory()
     h_out = torch.empty(G2_SHAPE, dtype=torch.float32).pin_memory()
@@ -566,7 +646,7 @@ def make_batch_params(seed=0, n=512):
     return shapes, params
 
 
-def run_batch(args):
+def run_batch(args, embedded=False):
     import torch
     import diplib_b200 as dipcu
     from diplib_b200.batch import BatchPlan
@@ -624,6 +704,19 @@ def run_batch(args):
     line["vs_single_image"] = {"single_image_gvox_s": single_rate, "ratio": value / world / single_rate,
                                "how": "plain dipcu_gauss_fir on one 4096^2 image per (sigma, orders, boundary "
                                       "condition) combination, weighted by the batch's pixel shares", "rates": rates}
+    # The plain 2D tile kernel's large-image rate: one 4096^2 image, sigma 2, order (0,0), mirror.
+    gl = [[_capture(lambda i=i: dipcu.GaussFIR(bigs[i], [2.0, 2.0], [0, 0], ["mirror"], 3.0, out=bigo[i]))]
+          for i in range(2)]
+    for g in gl:
+        g[0].replay()
+    tt, _, _ = _timed(gl, 10, dev)
+    plain_rate = 4096 * 4096 * 10 / (tt * 1e-3) / 1e9
+    line["vs_plain_large_image"] = {"plain_gvox_s": plain_rate, "ratio": value / world / plain_rate,
+                                    "how": "plain dipcu_gauss_fir on one 4096^2 sfloat image, sigma 2, order (0,0), "
+                                           "mirror (the 2D tile kernel's large-image rate)"}
+    if embedded:
+        plan.close()
+        return line
     # e2e: every image in from pinned host memory, every result back; a second plan over a second
     # set of device buffers for the pipelined steps.
     h_in = [t.cpu().pin_memory() for t in ins]
@@ -670,7 +763,7 @@ D_CONFIG = {"workload": "differentiable dip::GaussFIR 2D 2048^2 sfloat, sigma 3,
             "l2": "4 rotating sets of input, upstream gradient, output and gradients (268 MB) > 126 MB L2"}
 
 
-def run_fwdbwd(args):
+def run_fwdbwd(args, embedded=False):
     import torch
     import diplib_b200 as dipcu
     from diplib_b200 import torch_ops
@@ -724,8 +817,13 @@ def run_fwdbwd(args):
                         "per pixel and order)", "bytes_per_voxel": 20, "avg_kernel_ms": t_fb / args.steps}
     line["forward_only"] = {"ms_per_step": t_f / args.steps, "gvox_s": world * npx * args.steps / (t_f * 1e-3) / 1e9,
                             "fwd_plus_bwd_over_fwd": t_fb / t_f}
+    ach_f = 8 * npx / (t_f / args.steps * 1e-3) / 1e9
+    line["forward_only"]["roofline"] = {"achieved": ach_f, "peak": peak, "unit": "GB/s", "frac": ach_f / peak,
+                                        "bytes_per_voxel": 8}
     line["clocks"] = clk
     line["gpu_launches"] = launches_per_step * args.steps
+    if embedded:
+        return line
     if rank == 0 and not args.no_cpu_baseline:
         import oracle
         if oracle.ref_available():
@@ -752,7 +850,7 @@ S_CONFIG = {"workload": "differentiable dip::StructureTensor, 8 sfloat volumes o
             "l2": "8 volumes with 6-component tensors and weights (2.9 GB) > 126 MB L2"}
 
 
-def run_structure_tensor(args):
+def run_structure_tensor(args, embedded=False):
     import torch
     from diplib_b200 import torch_ops
     world, rank, dev = _device(args)
@@ -801,6 +899,8 @@ def run_structure_tensor(args):
                             "fwd_plus_bwd_over_fwd": t_fb / t_f}
     line["clocks"] = clk
     line["gpu_launches"] = launches_per_step * steps
+    if embedded:
+        return line
     if rank == 0 and not args.no_cpu_baseline:
         import oracle
         if oracle.ref_available():
@@ -824,6 +924,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="dipcu", choices=["dipcu", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--headline-only", action="store_true",
+                    help="the headline workload alone, without the other configurations' summaries")
     ap.add_argument("--workload", default="gauss3d", choices=["gauss3d"] + sorted(WORKLOADS),
                     help="gauss3d: the headline 256^3 uint16 volume (default); the others are the further "
                          "configurations (plain 2D, batched uneven 2D, differentiable 2D, structure tensor)")

@@ -23,6 +23,11 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
           f"-I{os.path.join(ROOT, 'include')}", f"-I{CSRC}"]
 
 
+# Per-file flags.  k_weights.cu: no FMA contraction, so that the device weights follow the
+# reference's double operation order exactly (they must equal DIPlib's taps bit for bit).
+FILE_FLAGS = {"k_weights.cu": ["-fmad=false"]}
+
+
 def nvcc() -> str:
     path = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
     if not os.path.exists(path):
@@ -45,7 +50,7 @@ def _compile(src: str, verbose: bool) -> str:
     newest_dep = max(os.path.getmtime(p) for p in headers() + [src])
     if os.path.exists(obj) and os.path.getmtime(obj) >= newest_dep:
         return obj
-    cmd = [nvcc(), *ARCH, *COMMON, "-c", src, "-o", obj]
+    cmd = [nvcc(), *ARCH, *COMMON, *FILE_FLAGS.get(os.path.basename(src), []), "-c", src, "-o", obj]
     if src.endswith(".cu") and verbose:
         cmd += ["-Xptxas", "-v"]
     r = subprocess.run(cmd, capture_output=True, text=True)

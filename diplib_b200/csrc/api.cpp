@@ -222,13 +222,9 @@ std::vector< int > pass_order( dipcu_image_desc const* in, std::vector< AxisFilt
    return order;
 }
 
-int run_filters( dipcu_image_desc const* in, dipcu_image_desc const* out, std::vector< AxisFilter > const& f,
-                 bool compute_double, cudaStream_t stream ) {
+int run_convert( dipcu_image_desc const* in, dipcu_image_desc const* out, cudaStream_t stream ) {
    int const nd = in->ndims;
-   int32_t const buf_dt = compute_double ? DT_DFLOAT : DT_SFLOAT;
-   std::vector< int > order = pass_order( in, f );
-   if( order.empty() ) {
-      ConvertArgs c{};
+   ConvertArgs c{};
       c.src = in->data;
       c.dst = out->data;
       c.src_dt = in->dtype;
@@ -240,34 +236,24 @@ int run_filters( dipcu_image_desc const* in, dipcu_image_desc const* out, std::v
          c.sst[ d ] = in->strides[ d ];
          c.dstst[ d ] = out->strides[ d ];
       }
-      cudaError_t e = launch_convert( c, true, stream );
-      if( e != cudaSuccess ) { return cuda_fail( e, "convert_kernel" ); }
-      return DIPCU_OK;
-   }
+   cudaError_t e = launch_convert( c, true, stream );
+   if( e != cudaSuccess ) { return cuda_fail( e, "convert_kernel" ); }
+   return DIPCU_OK;
+}
 
-   cudaError_t ferr = cudaSuccess;
-   if( try_fused( in, out, f, order, compute_double, stream, &ferr )) {
-      if( ferr != cudaSuccess ) { return cuda_fail( ferr, "fused tile kernel" ); }
-      return DIPCU_OK;
-   }
+int line_pass_scratch_images( int passes, bool out_is_buf ) {
+   if( passes <= 1 ) { return 0; }
+   return ( out_is_buf || passes == 2 ) ? 1 : 2;
+}
 
-   // Line kernel passes.  No pass reads and writes the same buffer: the last pass writes `out`,
-   // earlier ones alternate between `out` (when it has the buffer type) and scratch images with
-   // normal strides.
+int run_line_passes( dipcu_image_desc const* in, dipcu_image_desc const* out, std::vector< AxisFilter > const& f,
+                     std::vector< int > const& order, bool compute_double, void* const scratch[ 2 ], cudaStream_t stream ) {
+   // No pass reads and writes the same buffer: the last pass writes `out`, earlier ones alternate
+   // between `out` (when it has the buffer type) and the scratch images (normal strides).
+   int const nd = in->ndims;
+   int32_t const buf_dt = compute_double ? DT_DFLOAT : DT_SFLOAT;
    int const P = static_cast< int >( order.size() );
-   int64_t const n = numel( in );
-   size_t const esz = compute_double ? 8 : 4;
    bool const out_is_buf = out->dtype == buf_dt;
-   void* scratch[ 2 ] = { nullptr, nullptr };
-   int nscratch = 0;
-   if( P > 1 ) { nscratch = ( out_is_buf || P == 2 ) ? 1 : 2; }
-   for( int i = 0; i < nscratch; ++i ) {
-      cudaError_t e = cudaMallocAsync( &scratch[ i ], static_cast< size_t >( n ) * esz, stream );
-      if( e != cudaSuccess ) {
-         for( int j = 0; j < i; ++j ) { cudaFreeAsync( scratch[ j ], stream ); }
-         return cuda_fail( e, "cudaMallocAsync (pass intermediate)" );
-      }
-   }
    int64_t normal[ DIPCU_MAX_DIMS ];
    {
       int64_t s = 1;
@@ -314,6 +300,33 @@ int run_filters( dipcu_image_desc const* in, dipcu_image_desc const* out, std::v
       src_dt = dst_dt;
       src_st = dst_st;
    }
+   return status;
+}
+
+int run_filters( dipcu_image_desc const* in, dipcu_image_desc const* out, std::vector< AxisFilter > const& f,
+                 bool compute_double, cudaStream_t stream ) {
+   std::vector< int > order = pass_order( in, f );
+   if( order.empty() ) { return run_convert( in, out, stream ); }
+
+   cudaError_t ferr = cudaSuccess;
+   if( try_fused( in, out, f, order, compute_double, stream, &ferr )) {
+      if( ferr != cudaSuccess ) { return cuda_fail( ferr, "fused tile kernel" ); }
+      return DIPCU_OK;
+   }
+
+   // Line kernel passes with their intermediates from the stream-ordered allocator.
+   int32_t const buf_dt = compute_double ? DT_DFLOAT : DT_SFLOAT;
+   int const nscratch = line_pass_scratch_images( static_cast< int >( order.size() ), out->dtype == buf_dt );
+   size_t const bytes = static_cast< size_t >( numel( in )) * ( compute_double ? 8 : 4 );
+   void* scratch[ 2 ] = { nullptr, nullptr };
+   for( int i = 0; i < nscratch; ++i ) {
+      cudaError_t e = cudaMallocAsync( &scratch[ i ], bytes, stream );
+      if( e != cudaSuccess ) {
+         for( int j = 0; j < i; ++j ) { cudaFreeAsync( scratch[ j ], stream ); }
+         return cuda_fail( e, "cudaMallocAsync (pass intermediate)" );
+      }
+   }
+   int status = run_line_passes( in, out, f, order, compute_double, scratch, stream );
    for( int i = 0; i < nscratch; ++i ) { cudaFreeAsync( scratch[ i ], stream ); }
    return status;
 }

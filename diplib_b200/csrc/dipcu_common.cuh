@@ -235,6 +235,98 @@ DIPCU_HD bool bc_is_index_map( int32_t bc ) {
 
 constexpr double kPi = 3.14159265358979323846264338327950288;
 
+// Round-to-nearest double operations that no compiler flag contracts or reorders (on the device
+// the explicit _rn intrinsics; on the host plain IEEE operations and the C library's fma).
+DIPCU_HD double rn_add( double a, double b ) {
+#ifdef __CUDA_ARCH__
+   return __dadd_rn( a, b );
+#else
+   return a + b;
+#endif
+}
+DIPCU_HD double rn_mul( double a, double b ) {
+#ifdef __CUDA_ARCH__
+   return __dmul_rn( a, b );
+#else
+   return a * b;
+#endif
+}
+DIPCU_HD double rn_fma( double a, double b, double c ) {
+#ifdef __CUDA_ARCH__
+   return __fma_rn( a, b, c );
+#else
+   return fma( a, b, c );
+#endif
+}
+
+// Double-double arithmetic (value = hi + lo, |lo| <= ulp(hi) / 2) with the error-free
+// transforms of Knuth (TwoSum), Dekker (FastTwoSum) and the fused-multiply-add product.
+struct DD { double hi, lo; };
+DIPCU_HD DD dd_fast_two_sum( double a, double b ) {   // |a| >= |b|
+   double s = rn_add( a, b );
+   return { s, rn_add( b, -rn_add( s, -a )) };
+}
+DIPCU_HD DD dd_two_sum( double a, double b ) {
+   double s = rn_add( a, b );
+   double bb = rn_add( s, -a );
+   return { s, rn_add( rn_add( a, -rn_add( s, -bb )), rn_add( b, -bb )) };
+}
+DIPCU_HD DD dd_mul( DD a, DD b ) {
+   double p = rn_mul( a.hi, b.hi );
+   double e = rn_fma( a.hi, b.hi, -p );
+   e = rn_add( e, rn_add( rn_mul( a.hi, b.lo ), rn_mul( a.lo, b.hi )));
+   return dd_fast_two_sum( p, e );
+}
+DIPCU_HD DD dd_div_small( DD a, double n ) {          // a / n, n a small positive integer
+   double q = a.hi / n;
+   double p = rn_mul( q, n );
+   double pe = rn_fma( q, n, -p );
+   double rem = rn_add( rn_add( rn_add( a.hi, -p ), -pe ), a.lo );
+   return dd_fast_two_sum( q, rem / n );
+}
+DIPCU_HD DD dd_add_one( DD a ) {                       // 1 + a, |a| < 1
+   DD s = dd_two_sum( 1.0, a.hi );
+   return dd_fast_two_sum( s.hi, rn_add( s.lo, a.lo ));
+}
+
+// exp(x) rounded to the nearest double for results in the normal range (x >= -708.39; the
+// double-double evaluation is good to ~1e-30 relative; below that the scaled high part can be one
+// subnormal unit off, a range the weights never reach).  Cody-Waite reduction x = k ln2 + r with |r| <= ln2 / 2 in
+// double-double (ln2 as a double-double constant), then the Taylor series of exp(r) to r^24 / 24!
+// (< 1e-33 truncation) by Horner's rule in double-double, then scaling by 2^k.  The device
+// weights use it where DIPlib calls the C library's exp (an IEEE-accurate function whose results
+// are the correctly rounded ones except for rare arguments), so that the device taps are the
+// reference's bit for bit after the cast to float.
+DIPCU_HD double exp_rn( double x ) {
+   if( x != x ) { return x; }
+   if( x > 709.782712893384 ) { return 1.0 / 0.0; }
+   if( x < -745.2 ) { return 0.0; }
+   constexpr double kLn2Hi = 6.93147180559945286227e-01;     // ln 2 rounded to double
+   constexpr double kLn2Lo = 2.31904681384629955842e-17;     // ln 2 - kLn2Hi
+   constexpr double kInvLn2 = 1.44269504088896338700e+00;
+   double const k = rint( rn_mul( x, kInvLn2 ));
+   double const p = rn_mul( k, kLn2Hi );
+   double const pe = rn_fma( k, kLn2Hi, -p );                 // k kLn2Hi = p + pe exactly
+   DD r = dd_two_sum( x, -p );
+   r = dd_fast_two_sum( r.hi, rn_add( rn_add( r.lo, -pe ), -rn_mul( k, kLn2Lo )));
+   DD t = { 1.0, 0.0 };
+   for( int n = 24; n >= 1; --n ) {
+      t = dd_add_one( dd_div_small( dd_mul( r, t ), static_cast< double >( n )));
+   }
+   return scalbn( t.hi, static_cast< int >( k ));
+}
+
+// The exp of the weights: the C library's on the host (the function DIPlib calls), exp_rn on the
+// device (and on the host when DIPCU_WEIGHT_EXP_RN is defined, which the CPU tests use to check
+// the device arithmetic against the reference).
+DIPCU_HD double weight_exp( double x ) {
+#if defined( __CUDA_ARCH__ ) || defined( DIPCU_WEIGHT_EXP_RN )
+   return exp_rn( x );
+#else
+   return exp( x );
+#endif
+}
+
 // maximum_gauss_truncation<T>() (include/diplib/library/numeric.h:69-76) for float / double.
 DIPCU_HD double max_gauss_truncation( bool dt_double ) {
    return dt_double ? 8.490424416849509 : 5.646660101844052; // sqrt( -2 ln eps )
@@ -274,7 +366,7 @@ DIPCU_HD void make_half_gaussian( double sigma, uint32_t order, int64_t len, T* 
          double norm = 0.0, dnorm = 0.0;
          for( int64_t r = 1; r <= r0; ++r ) {
             double rad = static_cast< double >( r );
-            double g = exp( factor * ( rad * rad ));
+            double g = weight_exp( factor * ( rad * rad ));
             norm += g;
             dnorm += g * rad * rad;
          }
@@ -283,7 +375,7 @@ DIPCU_HD void make_half_gaussian( double sigma, uint32_t order, int64_t len, T* 
          double dS = 2.0 * dnorm / ( s2 * sigma );       // dS/dsigma
          for( int64_t r = 0; r <= r0; ++r ) {
             double rad = static_cast< double >( r );
-            double g = ( r == 0 ) ? 1.0 : exp( factor * ( rad * rad ));
+            double g = ( r == 0 ) ? 1.0 : weight_exp( factor * ( rad * rad ));
             w[ r ] = static_cast< T >( g * inv );
             if( dw ) {
                double dg = g * rad * rad / ( s2 * sigma );
@@ -297,7 +389,7 @@ DIPCU_HD void make_half_gaussian( double sigma, uint32_t order, int64_t len, T* 
          double moment = 0.0, dmoment = 0.0;
          for( int64_t r = 1; r <= r0; ++r ) {
             double rad = static_cast< double >( r );
-            double g = rad * exp( factor * ( rad * rad ));
+            double g = rad * weight_exp( factor * ( rad * rad ));
             moment += rad * g;
             dmoment += rad * g * rad * rad / ( s2 * sigma );
          }
@@ -306,7 +398,7 @@ DIPCU_HD void make_half_gaussian( double sigma, uint32_t order, int64_t len, T* 
          if( dw ) { dw[ 0 ] = T( 0 ); }
          for( int64_t r = 1; r <= r0; ++r ) {
             double rad = static_cast< double >( r );
-            double g = rad * exp( factor * ( rad * rad ));
+            double g = rad * weight_exp( factor * ( rad * rad ));
             w[ r ] = static_cast< T >( g * inv );
             if( dw ) {
                double dg = g * rad * rad / ( s2 * sigma );
@@ -321,7 +413,7 @@ DIPCU_HD void make_half_gaussian( double sigma, uint32_t order, int64_t len, T* 
          for( int64_t r = 1; r <= r0; ++r ) {
             double rad = static_cast< double >( r );
             double sr2 = rad * rad / s2;
-            double e = exp( -0.5 * sr2 );
+            double e = weight_exp( -0.5 * sr2 );
             sum += ( sr2 - 1.0 ) * norm * e;
             dsum += e * sr2 * ( sr2 - 3.0 ) / sigma;     // d/dsigma of (sr2-1) e, unnormalised
          }
@@ -335,7 +427,7 @@ DIPCU_HD void make_half_gaussian( double sigma, uint32_t order, int64_t len, T* 
          for( int64_t r = 1; r <= r0; ++r ) {
             double rad = static_cast< double >( r );
             double sr2 = rad * rad / s2;
-            double e = exp( -0.5 * sr2 );
+            double e = weight_exp( -0.5 * sr2 );
             double f = ( sr2 - 1.0 ) * norm * e - mean;
             moment += rad * rad * f;
             double f1 = ( sr2 - 1.0 ) * e - mean1;
@@ -346,7 +438,7 @@ DIPCU_HD void make_half_gaussian( double sigma, uint32_t order, int64_t len, T* 
          for( int64_t r = 0; r <= r0; ++r ) {
             double rad = static_cast< double >( r );
             double sr2 = rad * rad / s2;
-            double e = exp( -0.5 * sr2 );
+            double e = weight_exp( -0.5 * sr2 );
             double g = ( r == 0 ) ? g0 : ( sr2 - 1.0 ) * norm * e;
             w[ r ] = static_cast< T >(( g - mean ) * inv );
             if( dw ) {
@@ -364,7 +456,7 @@ DIPCU_HD void make_half_gaussian( double sigma, uint32_t order, int64_t len, T* 
             double rad = static_cast< double >( r );
             double rr2 = rad * rad;
             double sr2 = rr2 / s2;
-            double e = exp( -0.5 * sr2 );
+            double e = weight_exp( -0.5 * sr2 );
             double g = norm * e * ( rad * ( 3.0 - sr2 ));
             moment += g * rr2 * rad;
             double g1 = e * ( rad * ( 3.0 - sr2 ));
@@ -378,7 +470,7 @@ DIPCU_HD void make_half_gaussian( double sigma, uint32_t order, int64_t len, T* 
             double rad = static_cast< double >( r );
             double rr2 = rad * rad;
             double sr2 = rr2 / s2;
-            double e = exp( -0.5 * sr2 );
+            double e = weight_exp( -0.5 * sr2 );
             double g = norm * e * ( rad * ( 3.0 - sr2 ));
             w[ r ] = static_cast< T >( g * inv );
             if( dw ) {

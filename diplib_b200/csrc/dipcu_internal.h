@@ -148,6 +148,18 @@ int build_filters( dipcu_image_desc const* in, double const* sigmas, uint32_t co
 // Framework::Separable's pass order: processed axes by input stride, stable.
 std::vector< int > pass_order( dipcu_image_desc const* in, std::vector< AxisFilter > const& f );
 
+// Copies `in` to `out` with the type conversion (no axis filtered).
+int run_convert( dipcu_image_desc const* in, dipcu_image_desc const* out, cudaStream_t stream );
+
+// Scratch images (each numel(in) samples of the compute type) run_line_passes needs for
+// `passes` line passes: 0 for one pass, 1 when `out` has the compute type or for two passes, else 2.
+int line_pass_scratch_images( int passes, bool out_is_buf );
+
+// The line-kernel pass chain of Framework::Separable (in -> out -> out ...) along `order`, with
+// the intermediates in the caller's scratch images (normal strides).
+int run_line_passes( dipcu_image_desc const* in, dipcu_image_desc const* out, std::vector< AxisFilter > const& f,
+                     std::vector< int > const& order, bool compute_double, void* const scratch[ 2 ], cudaStream_t stream );
+
 // Runs the separable filter `f` from `in` to `out` (fused tile kernel when possible, else the
 // line-kernel pass chain), computing in double when `compute_double`.
 int run_filters( dipcu_image_desc const* in, dipcu_image_desc const* out, std::vector< AxisFilter > const& f,

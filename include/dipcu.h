@@ -89,9 +89,10 @@ int dipcu_gauss_fir( dipcu_image_desc const* in, dipcu_image_desc const* out,
  * 4 Mi samples when the filter computes in float and 2 Mi samples when it computes in double
  * (32/64-bit integer or dfloat input); larger images return DIPCU_ERR_INVALID_ARG.  Runs the
  * line kernel pass by pass.  All calls share the array: calls whose work overlaps on the GPU race
- * and give wrong results, so order them on one stream.  The first call on a device looks up the
- * array's address; make it before any stream capture on that device.  Arguments and results
- * are those of dipcu_gauss_fir. */
+ * and give wrong results, so order them on one stream.  Every call outside stream capture looks up
+ * the array's address on its device; a call under capture reuses the one found by the device's
+ * last call outside capture, so make one call on a device (after any device reset) before
+ * capturing one.  Arguments, checks and results are those of dipcu_gauss_fir. */
 int dipcu_gauss_fir_noalloc( dipcu_image_desc const* in, dipcu_image_desc const* out,
                              double const* sigmas, uint32_t const* orders, int32_t const* bcs,
                              double truncation, void* stream );

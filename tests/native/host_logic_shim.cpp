@@ -25,4 +25,9 @@ void hl_make_half_gaussian( double sigma, uint32_t order, int64_t len, double* w
    dipcu::make_half_gaussian< double >( sigma, order, len, w, dw );
 }
 
+// exp rounded to the nearest double (the device weights' exp), evaluated on the host.
+double hl_exp_rn( double x ) {
+   return dipcu::exp_rn( x );
+}
+
 } // extern "C"

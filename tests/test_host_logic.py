@@ -64,8 +64,8 @@ def _hl():
     return l
 
 
-def host_half_gaussian(sigma, order, trunc, dt_double, with_derivative=False):
-    l = _hl()
+def host_half_gaussian(sigma, order, trunc, dt_double, with_derivative=False, lib=None):
+    l = lib or _hl()
     n = l.hl_half_gaussian_length(sigma, order, trunc, int(dt_double))
     w = np.zeros(n)
     dw = np.zeros(n)
@@ -82,9 +82,49 @@ def test_weights_match_oracle(dt_double):
                 ref = oracle.half_gaussian(sigma, order, trunc, dt_double)[::-1]  # centre first
                 got = host_half_gaussian(sigma, order, trunc, dt_double)
                 assert got.shape == ref.shape, (sigma, order, trunc)
-                np.testing.assert_array_max_ulp(got, ref, maxulp=2)
+                np.testing.assert_array_equal(got, ref)
                 assert _abi.lib().dipcu_half_gaussian_length(sigma, order, trunc, int(dt_double)) == ref.size
     assert _abi.lib().dipcu_half_gaussian_length(1.0, 4, 3.0, 0) == -1
+
+
+def test_exp_rn_is_correctly_rounded():
+    """exp_rn (the device weights' exp) against exp evaluated to 60 digits and rounded to double,
+    over the argument range the weights use and beyond (normal results)."""
+    from decimal import Decimal, getcontext
+    getcontext().prec = 60
+    l = ctypes.CDLL(HOSTLOGIC)
+    l.hl_exp_rn.restype = ctypes.c_double
+    l.hl_exp_rn.argtypes = [ctypes.c_double]
+    rng = np.random.default_rng(7)
+    xs = np.concatenate([rng.uniform(-60.0, 0.0, 4000), rng.uniform(-708.0, 709.0, 1000), -rng.random(500) * 1e-6,
+                         [0.0, -0.5, -1.0, -4.5, -18.0, -0.34657359027997264, 0.34657359027997264]])
+    for x in xs:
+        got = l.hl_exp_rn(float(x))
+        exact = Decimal(float(x)).exp()
+        # the nearest double: no double beside `got` is closer to the exact value
+        err = abs(Decimal(got) - exact)
+        for nb in (np.nextafter(got, np.inf), np.nextafter(got, -np.inf)):
+            assert err <= abs(Decimal(float(nb)) - exact), x
+
+
+def test_device_weight_arithmetic_matches_reference_in_float():
+    """The device weights (K0) compute with exp_rn instead of the C library's exp, which rounds a few
+    arguments differently in the last double bit.  After the cast to float the taps must be the
+    reference's bit for bit: the host build of the same arithmetic (libhostlogic_rn) against the
+    reference's MakeHalfGaussian over a grid of sigmas, all orders and truncations."""
+    lrn = ctypes.CDLL(HOSTLOGIC.replace("libhostlogic.so", "libhostlogic_rn.so"))
+    lrn.hl_half_gaussian_length.restype = ctypes.c_int64
+    lrn.hl_half_gaussian_length.argtypes = [ctypes.c_double, ctypes.c_uint32, ctypes.c_double, ctypes.c_int]
+    lrn.hl_make_half_gaussian.argtypes = [ctypes.c_double, ctypes.c_uint32, ctypes.c_int64, ctypes.c_void_p,
+                                          ctypes.c_void_p]
+    rng = np.random.default_rng(3)
+    sigmas = list(np.round(rng.uniform(0.3, 30.0, 300), 3)) + [0.8, 1.0, 1.5, 2.0, 3.0, 4.0, 8.0, 11.0]
+    for sigma in sigmas:
+        for order in range(4):
+            for trunc in (3.0, 4.5):
+                ref = oracle.half_gaussian(float(sigma), order, trunc, False)[::-1].astype(np.float32)
+                got = host_half_gaussian(float(sigma), order, trunc, False, lib=lrn).astype(np.float32)
+                np.testing.assert_array_equal(got, ref, err_msg=f"sigma {sigma} order {order} trunc {trunc}")
 
 
 @pytest.mark.parametrize("order", [0, 1, 2, 3])
