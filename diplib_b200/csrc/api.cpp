@@ -131,6 +131,8 @@ bool try_fused( dipcu_image_desc const* in, dipcu_image_desc const* out, std::ve
       a.db = 0;
    }
    if( np == 2 ) {
+      *err = launch_march2d( key, a, stream );
+      if( *err != cudaErrorNotSupported ) { return true; }
       *err = launch_fused2d_ws( key, a, stream );
       if( *err != cudaErrorNotSupported ) { return true; }
    }

@@ -103,6 +103,11 @@ cudaError_t launch_fused_adjoint2d( Adj2Params const& p, cudaStream_t stream );
 // conditions it handles); cudaErrorNotSupported when it does not apply.
 cudaError_t launch_fused2d_ws( FusedKey const& key, FusedArgs& args, cudaStream_t stream );
 
+// Row-march 2D kernel (march2d.cuh: half-widths up to 32 on both axes, float or uint16 input,
+// the index-mapping boundary conditions and "add zeros"); cudaErrorNotSupported when it does not
+// apply.
+cudaError_t launch_march2d( FusedKey const& key, FusedArgs& args, cudaStream_t stream );
+
 // Adjoint halo fold along one axis (k_backward.cu).
 struct FoldPass {
    void const* g;            // gradient w.r.t. the forward pass output (compute type)

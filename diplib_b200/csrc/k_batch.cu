@@ -37,6 +37,7 @@
 #include "dipcu_internal.h"
 #include "fused.cuh"
 #include "fused2d_ws.cuh"
+#include "march2d.cuh"
 
 namespace dipcu {
 
@@ -1009,6 +1010,16 @@ struct dipcu_batch_plan {
    cudaStream_t cap_stream = nullptr;
    cudaGraph_t graph = nullptr;
    cudaGraphExec_t exec = nullptr;
+   // Row-march path (march2d.cuh): every image it takes, in one persistent launch that pulls
+   // (image, strip, row run) items from a device work queue, most expensive items first.  The
+   // row-run length is chosen per class of y half-width (up to 8, 16, 24, 32) by the autotuner.
+   std::vector< char > march;              // per image: taken by the row-march path
+   std::vector< M2Image > mimg;
+   M2Image* d_mimg = nullptr;
+   M2Item* d_mitems = nullptr;
+   int32_t* d_mcounter = nullptr;
+   int m_nitems = 0;
+   int m_runlen[ 4 ] = { 384, 384, 384, 384 };
 };
 
 namespace {
@@ -1024,11 +1035,15 @@ int plan_fail( int code, std::string const& msg ) { return record_error( code, m
 // kernel gets no items of its own.
 int plan_groups( dipcu_batch_plan* p, int inject ) {
    p->gbucket.assign( static_cast< size_t >( p->count ), -1 );
+   for( int i = 0; i < p->count; ++i ) {
+      if( p->march[ static_cast< size_t >( i ) ] ) { p->gbucket[ static_cast< size_t >( i ) ] = 100; }   // row-march path
+   }
    bool const no_ws = getenv( "DIPCU_BATCH_NO_WS" ) != nullptr;
    std::vector< G2Image > gimg[ 4 ];
    std::vector< BatchItem > gitems[ 4 ];
    int rest = 0;
    for( int i = 0; i < p->count; ++i ) {
+      if( p->march[ static_cast< size_t >( i ) ] ) { continue; }
       BatchImage const& im = p->images[ static_cast< size_t >( i ) ];
       int const hm = std::max( im.h[ 0 ], im.h[ 1 ] );
       int const b = hm <= 4 ? 0 : hm <= 6 ? 1 : hm <= 9 ? 2 : hm <= 12 ? 3 : -1;
@@ -1172,6 +1187,132 @@ int plan_groups( dipcu_batch_plan* p, int inject ) {
    return DIPCU_OK;
 }
 
+// Images the row-march kernel takes (TMA-readable layout, its boundary conditions, half-widths up
+// to 32); their tables are uploaded once per plan.
+int plan_march( dipcu_batch_plan* p ) {
+   p->march.assign( static_cast< size_t >( p->count ), 0 );
+   p->mimg.clear();
+   if( getenv( "DIPCU_BATCH_NO_MARCH" )) { return DIPCU_OK; }
+   for( int i = 0; i < p->count; ++i ) {
+      BatchImage const& im = p->images[ static_cast< size_t >( i ) ];
+      M2Image m{};
+      if( !march2d_image< float >( m, im.src, im.n[ 0 ], im.n[ 1 ], im.ss[ 1 ], 1, 0, im.dst, im.ds[ 1 ], 0, im.bc, im.h, im.odd )) {
+         continue;
+      }
+      m.w[ 0 ] = p->d_bank + im.wofs[ 0 ];
+      m.w[ 1 ] = p->d_bank + im.wofs[ 1 ];
+      p->march[ static_cast< size_t >( i ) ] = 1;
+      p->mimg.push_back( m );
+   }
+   if( p->mimg.empty()) { return DIPCU_OK; }
+   if( cudaMalloc( &p->d_mimg, sizeof( M2Image ) * p->mimg.size()) != cudaSuccess ||
+       cudaMalloc( &p->d_mcounter, sizeof( int32_t )) != cudaSuccess ||
+       cudaMemcpy( p->d_mimg, p->mimg.data(), sizeof( M2Image ) * p->mimg.size(), cudaMemcpyHostToDevice ) != cudaSuccess ) {
+      return plan_fail( DIPCU_ERR_CUDA, "batch plan: row-march tables" );
+   }
+   return DIPCU_OK;
+}
+
+int march_class( int hy ) { return hy <= 8 ? 0 : hy <= 16 ? 1 : hy <= 24 ? 2 : 3; }
+
+// The row-march work items for the current row-run lengths: per image, strips of 128 columns times
+// runs of rows (the runs of an image equal in length), sorted by estimated cost (x-phase rows times
+// the x window plus output rows times the y tap blocks), most expensive first.  `inject` replaces
+// the middle item by an impossible one.
+int march_items( dipcu_batch_plan* p, int inject ) {
+   struct Costed { double cost; M2Item it; };
+   std::vector< Costed > items;
+   for( size_t k = 0; k < p->mimg.size(); ++k ) {
+      M2Image const& m = p->mimg[ k ];
+      int const L0 = p->m_runlen[ march_class( m.h[ 1 ] ) ];
+      int const runs = std::max( 1, ( m.ny + L0 - 1 ) / L0 );
+      int const L = ( m.ny + runs - 1 ) / runs;
+      int const strips = ( m.nx + kM2TX - 1 ) / kM2TX;
+      for( int y = 0; y < m.ny; y += L ) {
+         int const yb = std::min( m.ny, y + L );
+         double const cost = static_cast< double >( yb - y + 2 * m.h[ 1 ] ) * ( 4 + 2 * m.lead ) +
+                             static_cast< double >( yb - y ) * 8 * (( 2 * m.h[ 1 ] + 8 ) / 8 ) + 200.0;
+         for( int t = 0; t < strips; ++t ) { items.push_back( Costed{ cost, M2Item{ static_cast< int32_t >( k ), t * kM2TX, y, yb } } ); }
+      }
+   }
+   std::stable_sort( items.begin(), items.end(), []( Costed const& a, Costed const& b ) { return a.cost > b.cost; } );
+   std::vector< M2Item > list( items.size());
+   for( size_t k = 0; k < items.size(); ++k ) { list[ k ] = items[ k ].it; }
+   if( inject == 1 && !list.empty()) { list[ list.size() / 2 ].img = 1 << 20; }
+   if( inject == 2 && !list.empty()) { list[ list.size() / 2 ].x0 = 1 << 30; }
+   cudaFree( p->d_mitems );
+   p->d_mitems = nullptr;
+   p->m_nitems = static_cast< int >( list.size());
+   if( list.empty()) { return DIPCU_OK; }
+   if( cudaMalloc( &p->d_mitems, sizeof( M2Item ) * list.size()) != cudaSuccess ||
+       cudaMemcpy( p->d_mitems, list.data(), sizeof( M2Item ) * list.size(), cudaMemcpyHostToDevice ) != cudaSuccess ) {
+      return plan_fail( DIPCU_ERR_CUDA, "batch plan: row-march items" );
+   }
+   return DIPCU_OK;
+}
+
+cudaError_t march_launch( dipcu_batch_plan* p, cudaStream_t st ) {
+   if( p->m_nitems == 0 ) { return cudaSuccess; }
+   cudaError_t e = cudaMemsetAsync( p->d_mcounter, 0, sizeof( int32_t ), st );
+   if( e != cudaSuccess ) { return e; }
+   return launch_march2d_items( p->d_mimg, static_cast< int >( p->mimg.size()), p->d_mitems, p->m_nitems, p->d_mcounter, st );
+}
+
+// Autotuner of the row-march path: per class of y half-width present in the batch, the row-run
+// length (96 rows .. whole images) that times fastest on this batch -- a trade between the x phase
+// of the 2 hy halo rows every run repeats and the granularity of the work queue -- one class at a
+// time (coordinate descent), after the weights are built once.  Remembered per batch signature.
+std::mutex g_mtune_mu;
+std::map< std::string, std::vector< int >> g_mtune_cache;
+
+int march_tune( dipcu_batch_plan* p, std::string const& sig ) {
+   {
+      std::lock_guard< std::mutex > lock( g_mtune_mu );
+      auto it = g_mtune_cache.find( sig );
+      if( it != g_mtune_cache.end() ) {
+         for( int c = 0; c < 4; ++c ) { p->m_runlen[ c ] = it->second[ static_cast< size_t >( c ) ]; }
+         return DIPCU_OK;
+      }
+   }
+   bool present[ 4 ] = {};
+   for( auto const& m : p->mimg ) { present[ march_class( m.h[ 1 ] ) ] = true; }
+   if( launch_gauss_weights( p->d_sigmas, p->d_orders, 2 * p->count, p->truncation, p->d_bank, nullptr, nullptr, kBankStride,
+                             nullptr ) != cudaSuccess ) {
+      return plan_fail( DIPCU_ERR_CUDA, "batch autotune: weights" );
+   }
+   cudaEvent_t e0, e1;
+   cudaEventCreate( &e0 );
+   cudaEventCreate( &e1 );
+   auto time_it = [ & ]() -> float {
+      if( march_items( p, 0 ) != DIPCU_OK ) { return 1e30f; }
+      march_launch( p, nullptr );                           // warm-up
+      cudaEventRecord( e0, nullptr );
+      for( int r = 0; r < 3; ++r ) { march_launch( p, nullptr ); }
+      cudaEventRecord( e1, nullptr );
+      if( cudaEventSynchronize( e1 ) != cudaSuccess ) { return 1e30f; }
+      float ms = 0.0f;
+      cudaEventElapsedTime( &ms, e0, e1 );
+      return ms;
+   };
+   int const cand[] = { 96, 192, 384, 768, 1 << 20 };
+   for( int c = 0; c < 4; ++c ) {
+      if( !present[ c ] ) { continue; }
+      int best = p->m_runlen[ c ];
+      float best_ms = 1e30f;
+      for( int L : cand ) {
+         p->m_runlen[ c ] = L;
+         float const ms = time_it();
+         if( ms < best_ms ) { best_ms = ms; best = L; }
+      }
+      p->m_runlen[ c ] = best;
+   }
+   cudaEventDestroy( e0 );
+   cudaEventDestroy( e1 );
+   std::lock_guard< std::mutex > lock( g_mtune_mu );
+   g_mtune_cache[ sig ] = std::vector< int >( p->m_runlen, p->m_runlen + 4 );
+   return DIPCU_OK;
+}
+
 // Tile the images for shape `s` and upload the work items, most expensive first.
 int plan_items( dipcu_batch_plan* p, int s, int inject ) {
    TileShape const ts = kShapes[ s ];
@@ -1211,6 +1352,8 @@ int enqueue_run( dipcu_batch_plan* p, cudaStream_t st ) {
    cudaError_t e = launch_gauss_weights( p->d_sigmas, p->d_orders, 2 * p->count, p->truncation, p->d_bank, nullptr,
                                          nullptr, kBankStride, st );
    if( e != cudaSuccess ) { return plan_fail( DIPCU_ERR_CUDA, "gauss_weights_kernel" ); }
+   e = march_launch( p, st );
+   if( e != cudaSuccess ) { return plan_fail( DIPCU_ERR_CUDA, std::string( "march2d_kernel: " ) + cudaGetErrorString( e )); }
    if( cudaEventRecord( p->ev_fork, st ) != cudaSuccess ) { return plan_fail( DIPCU_ERR_CUDA, "batch fork" ); }
    if( p->nitems > 0 ) {
       BatchArgs a{};
@@ -1346,7 +1489,9 @@ int dipcu_batch_plan_create( dipcu_image_desc const* ins, dipcu_image_desc const
       dipcu_batch_plan_destroy( p );
       return plan_fail( DIPCU_ERR_CUDA, "device status word" );
    }
-   if( int st = plan_groups( p, inject )) { dipcu_batch_plan_destroy( p ); return st; }
+   if( int st = plan_march( p )) { dipcu_batch_plan_destroy( p ); return st; }
+   int const m_inject = p->mimg.empty() ? 0 : inject;       // planted on the row-march path when it has work
+   if( int st = plan_groups( p, m_inject ? 0 : inject )) { dipcu_batch_plan_destroy( p ); return st; }
    bool sok = cudaEventCreateWithFlags( &p->ev_fork, cudaEventDisableTiming ) == cudaSuccess;
    for( int b = 0; b < 4 && sok; ++b ) {
       sok = cudaStreamCreateWithFlags( &p->side[ b ], cudaStreamNonBlocking ) == cudaSuccess &&
@@ -1358,7 +1503,13 @@ int dipcu_batch_plan_create( dipcu_image_desc const* ins, dipcu_image_desc const
    // overwritten by the final runs), remembering the winner per batch signature.
    int shape = 0;
    if( char const* env = getenv( "DIPCU_BATCH_SHAPE" )) { shape = std::max( 0, std::min( 2, atoi( env ))); }
-   if( flags & DIPCU_BATCH_AUTOTUNE ) {
+   if(( flags & DIPCU_BATCH_AUTOTUNE ) && !p->mimg.empty()) {
+      if( int st = march_tune( p, sig )) { dipcu_batch_plan_destroy( p ); return st; }
+   }
+   if( int st = march_items( p, m_inject )) { dipcu_batch_plan_destroy( p ); return st; }
+   bool rest_persistent = false;     // images left for the persistent tile kernel
+   for( int i = 0; i < p->count; ++i ) { rest_persistent = rest_persistent || p->gbucket[ static_cast< size_t >( i ) ] < 0; }
+   if(( flags & DIPCU_BATCH_AUTOTUNE ) && rest_persistent ) {
       std::lock_guard< std::mutex > lock( g_tune_mu );
       auto it = g_tune_cache.find( sig );
       if( it != g_tune_cache.end() ) {
@@ -1384,7 +1535,7 @@ int dipcu_batch_plan_create( dipcu_image_desc const* ins, dipcu_image_desc const
          g_tune_cache[ sig ] = shape;
       }
    }
-   if( int st = plan_items( p, shape, inject )) { dipcu_batch_plan_destroy( p ); return st; }
+   if( int st = plan_items( p, shape, m_inject ? 0 : inject )) { dipcu_batch_plan_destroy( p ); return st; }
    if( flags & DIPCU_BATCH_GRAPH ) {
       if( cudaStreamCreateWithFlags( &p->cap_stream, cudaStreamNonBlocking ) != cudaSuccess ||
           cudaStreamBeginCapture( p->cap_stream, cudaStreamCaptureModeThreadLocal ) != cudaSuccess ) {
@@ -1416,7 +1567,7 @@ int dipcu_batch_plan_run( dipcu_batch_plan* plan, void* stream ) {
 int dipcu_batch_plan_info( dipcu_batch_plan const* plan, int* nitems, int* tile_x, int* tile_y, int* grid ) {
    if( !plan ) { return plan_fail( DIPCU_ERR_INVALID_ARG, "null plan" ); }
    if( nitems ) {
-      *nitems = plan->nitems;
+      *nitems = plan->nitems + plan->m_nitems;
       for( int b = 0; b < 4; ++b ) { *nitems += plan->g_nitems[ b ]; }
       for( int b = 0; b < kNBL; ++b ) { *nitems += plan->l_nx[ b ] + plan->l_ny[ b ]; }
    }
@@ -1428,7 +1579,7 @@ int dipcu_batch_plan_info( dipcu_batch_plan const* plan, int* nitems, int* tile_
 
 int dipcu_batch_plan_launches( dipcu_batch_plan const* plan, int* kernels, int* grouped_items ) {
    if( !plan ) { return plan_fail( DIPCU_ERR_INVALID_ARG, "null plan" ); }
-   int k = 1 + ( plan->nitems > 0 ? 1 : 0 ), g = 0;
+   int k = 1 + ( plan->nitems > 0 ? 1 : 0 ) + ( plan->m_nitems > 0 ? 1 : 0 ), g = plan->m_nitems;
    for( int b = 0; b < 4; ++b ) {
       k += plan->g_nitems[ b ] > 0 ? 1 : 0;
       g += plan->g_nitems[ b ];
@@ -1466,6 +1617,9 @@ int dipcu_batch_plan_destroy( dipcu_batch_plan* plan ) {
       cudaFree( plan->d_lyitems[ b ] );
    }
    cudaFree( plan->d_tmp );
+   cudaFree( plan->d_mimg );
+   cudaFree( plan->d_mitems );
+   cudaFree( plan->d_mcounter );
    for( int b = 0; b < 4; ++b ) {
       if( plan->side[ b ] ) { cudaStreamDestroy( plan->side[ b ] ); }
       if( plan->ev_join[ b ] ) { cudaEventDestroy( plan->ev_join[ b ] ); }

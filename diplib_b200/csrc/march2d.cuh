@@ -1,0 +1,471 @@
+// K1-2D, row march: the fused 2D Gaussian FIR kernel for sm_100a (single images and batches).
+//
+// Work item: a strip of TX = 128 output columns of one 2D image and a run of its rows [ya, yb).
+// A CTA takes items one after the other (from a static list, or from a device work queue) and
+// marches down the item's rows in steps of R = 24 input rows:
+//   * x phase: the step's R input rows (the strip plus LEAD columns of halo on each side) land in
+//     one of two shared-memory stages by TMA -- one box, or one box per row where rows lie outside
+//     the image (the boundary condition's source row, or TMA zero fill for "add zeros") -- and are
+//     filtered along x into a ring of x-filtered rows (each warp a row, each lane 4 outputs from
+//     aligned float4 windows, taps in tap quads broadcast from shared memory);
+//   * y phase: one step behind the rows it needs, the ring's rows are filtered along y into R output
+//     rows (each thread one column and R / 2 rows, taps in blocks of 8, R / 2 + 7 ring rows per block)
+//     and stored straight to global memory (each warp 32 consecutive columns: 128-byte rows).
+// One __syncthreads per step (x-phase results visible to the y phase); the ring holds (D + 2) R rows
+// (D = ceil(2 hy / R)), so that a step's x phase never overwrites rows an earlier step's y phase
+// may still read.  The next-but-one step's TMA goes out as soon as a stage is free.  Each input pixel
+// crosses HBM once (the x-halo columns of neighbouring strips hit L2) and each output pixel is
+// written once; the only recomputation is the x phase of the 2 hy rows of halo at the start of each
+// item's row run.
+//
+// Half-widths up to 32 on each axis, runtime taps (no compile-time buckets): the x filter is padded
+// to the TMA granule LEAD >= hx on both sides, the y filter to a multiple of 8 taps (the last block
+// cut at 2 hy, so that no row beyond the filter's support is read).  Boundary conditions in x:
+// every index-mapping one ("mirror", "asym mirror", "periodic", "asym periodic", "zero order") and
+// "add zeros": halo columns outside the image are rewritten in the stage from their source column
+// (a copy inside the box, or a load from the image where the source lies outside it), sign
+// included; in y the same conditions through the rows' source coordinates and a per-row sign.
+// These are the conditions whose extension of the x-filtered image equals the x-filtering of the
+// extended input, which is what lets the two passes fuse (DIPlib extends each intermediate line
+// itself, src/library/framework_separable.cpp:354-419).
+#pragma once
+
+#include <cuda.h>
+#include <stdint.h>
+
+#include <type_traits>
+
+#include "dipcu_common.cuh"
+#include "dipcu_internal.h"
+#include "tma.cuh"
+
+namespace dipcu {
+
+constexpr int kM2TX = 128;          // output columns per strip
+constexpr int kM2R = 24;            // rows per step (and per y-phase block)
+constexpr int kM2RT = kM2R / 2;     // output rows per thread in the y phase
+constexpr int kM2NT = 256;          // threads per CTA
+constexpr int kM2MaxH = 32;         // largest half-width along either axis
+constexpr int kM2MaxLead = 32;      // LEAD for hx = 32
+constexpr int kM2MaxBW = kM2TX + 2 * kM2MaxLead;
+constexpr int kM2MaxRing = ( 2 + ( 2 * kM2MaxH + kM2R - 1 ) / kM2R ) * kM2R;
+constexpr int kM2MaxFix = 2 * kM2MaxLead;
+constexpr int kM2WxLen = 4 + 2 * kM2MaxLead + 8;   // 4 leading zeros, 2 LEAD + 1 taps, zero tail
+constexpr int kM2WyLen = 2 * kM2MaxH + 8;
+
+// One image of a launch.  `tmap` boxes are (bw, R) for the interior steps, `tmap1` (bw, 1) for
+// rows at the image's edges; both 4D (x, y, 1, b).
+struct alignas( 64 ) M2Image {
+   CUtensorMap tmap;
+   CUtensorMap tmap1;
+   void const* src;           // the source (for gathers of x-halo columns whose source lies outside the box)
+   int64_t ss1, ssb;          // source row and batch strides (samples)
+   float* dst;
+   int64_t ds1, dsb;          // destination row and batch strides
+   int32_t nx, ny;
+   int32_t bc[ 2 ];
+   int32_t h[ 2 ];
+   int32_t odd[ 2 ];
+   int32_t lead;              // box columns before the strip (multiple of the TMA granule, >= h[0])
+   int32_t bw;                // box width = 128 + 2 lead
+   float const* w[ 2 ];       // half kernels (centre first, h + 1 taps) in device memory; null: M2Args::w0
+};
+
+struct M2Item {
+   int32_t img;               // image index (or batch index for a single image)
+   int32_t x0;                // first output column of the strip
+   int32_t ya, yb;            // output rows
+};
+
+struct M2Args {
+   M2Image img0;              // the image of a single-image launch (images == nullptr)
+   M2Image const* images;     // per-image table of a batch launch
+   M2Item const* items;       // item list (batch); null: items from the single image's geometry
+   int32_t nitems;
+   int32_t nimages;           // entries of `images`
+   int32_t* queue;            // device work counter (batch; zero before the launch); null: static
+   int32_t* status;
+   // single-image geometry: items = nb x strips x chunks, chunk = `lchunk` rows
+   int32_t nb, strips, chunks, lchunk;
+   float w0[ 2 ][ kM2MaxH + 1 ];   // single-image half kernels (x, y), centre first
+};
+
+struct M2Smem {
+   static constexpr int STAGE_BYTES = kM2R * kM2MaxBW * 4;                       // float stage (u16 uses half)
+   static constexpr int OFF_STAGE = 0;
+   static constexpr int OFF_RING = OFF_STAGE + 2 * STAGE_BYTES;
+   static constexpr int OFF_WX = OFF_RING + kM2MaxRing * kM2TX * 4;
+   static constexpr int OFF_WY = OFF_WX + kM2WxLen * 4;
+   static constexpr int OFF_ROWS = OFF_WY + kM2WyLen * 4;                        // [2][R] source row, [2][R] sign
+   static constexpr int OFF_FIX = OFF_ROWS + 4 * kM2R * 4;                       // [kM2MaxFix] fix entries
+   static constexpr int OFF_MISC = OFF_FIX + kM2MaxFix * 8;                      // 16 ints
+   static constexpr int OFF_BAR = ( OFF_MISC + 64 + 15 ) / 16 * 16;
+   static constexpr int BYTES = OFF_BAR + 2 * 8;
+   static_assert( OFF_RING % 128 == 0 && STAGE_BYTES % 128 == 0, "TMA destinations 128-byte aligned" );
+   static_assert( OFF_WX % 16 == 0 && OFF_WY % 16 == 0, "float4 weight reads" );
+   static_assert( BYTES <= 113 * 1024, "two CTAs per SM" );
+};
+
+// Column fix entry: destination box column, source (box column, or image column for a gather),
+// flags.
+struct M2Fix {
+   int16_t dst;
+   int16_t flags;             // bit 0: negate; bit 1: source is an image column (gather); bit 2: zero
+   int32_t src;
+};
+
+template< typename TIn >
+__device__ __forceinline__ float4 m2_load4( unsigned char const* stage, int rs, int row, int col ) {
+   if constexpr( std::is_same< TIn, float >::value ) {
+      return *reinterpret_cast< float4 const* >( stage + ( static_cast< size_t >( row ) * rs + col ) * 4 );
+   } else {
+      uint2 const u = *reinterpret_cast< uint2 const* >( stage + ( static_cast< size_t >( row ) * rs + col ) * 2 );
+      // uint16 -> float exactly: the sample placed in the low mantissa bits of 2^23, minus 2^23.
+      float4 r;
+      r.x = __uint_as_float( __byte_perm( u.x, 0x4B000000u, 0x7610 )) - 8388608.0f;
+      r.y = __uint_as_float( __byte_perm( u.x, 0x4B000000u, 0x7632 )) - 8388608.0f;
+      r.z = __uint_as_float( __byte_perm( u.y, 0x4B000000u, 0x7610 )) - 8388608.0f;
+      r.w = __uint_as_float( __byte_perm( u.y, 0x4B000000u, 0x7632 )) - 8388608.0f;
+      return r;
+   }
+}
+
+template< typename TIn >
+__device__ __forceinline__ float m2_get( unsigned char const* stage, int rs, int row, int col ) {
+   if constexpr( std::is_same< TIn, float >::value ) {
+      return reinterpret_cast< float const* >( stage )[ static_cast< size_t >( row ) * rs + col ];
+   } else {
+      return static_cast< float >( reinterpret_cast< uint16_t const* >( stage )[ static_cast< size_t >( row ) * rs + col ] );
+   }
+}
+
+template< typename TIn >
+__device__ __forceinline__ void m2_put( unsigned char* stage, int rs, int row, int col, float v ) {
+   if constexpr( std::is_same< TIn, float >::value ) {
+      reinterpret_cast< float* >( stage )[ static_cast< size_t >( row ) * rs + col ] = v;
+   } else {
+      reinterpret_cast< uint16_t* >( stage )[ static_cast< size_t >( row ) * rs + col ] = static_cast< uint16_t >( v );
+   }
+}
+
+template< typename TIn >
+__device__ __forceinline__ float m2_src_sample( M2Image const& im, int b, int row, int col ) {
+   TIn const* p = static_cast< TIn const* >( im.src ) + static_cast< int64_t >( b ) * im.ssb +
+                  static_cast< int64_t >( row ) * im.ss1 + col;
+   return static_cast< float >( *p );
+}
+
+template< typename TIn >
+__global__ void __launch_bounds__( kM2NT, 2 ) march2d_kernel( M2Args const __grid_constant__ a ) {
+   constexpr int R = kM2R, TX = kM2TX, NT = kM2NT;
+   extern __shared__ __align__( 128 ) unsigned char smem[];
+   unsigned char* const stages = smem + M2Smem::OFF_STAGE;
+   float* const ring = reinterpret_cast< float* >( smem + M2Smem::OFF_RING );
+   float* const wx = reinterpret_cast< float* >( smem + M2Smem::OFF_WX );
+   float* const wy = reinterpret_cast< float* >( smem + M2Smem::OFF_WY );
+   int32_t* const rsrc = reinterpret_cast< int32_t* >( smem + M2Smem::OFF_ROWS );   // [2][R]
+   float* const rsgn = reinterpret_cast< float* >( rsrc + 2 * R );                   // [2][R]
+   M2Fix* const fix = reinterpret_cast< M2Fix* >( smem + M2Smem::OFF_FIX );
+   // misc: [0] item, [1] fixes, [2] abort, [4..5] stage row strides
+   int32_t* const misc = reinterpret_cast< int32_t* >( smem + M2Smem::OFF_MISC );
+   uint64_t* const full = reinterpret_cast< uint64_t* >( smem + M2Smem::OFF_BAR );
+   int const tid = static_cast< int >( threadIdx.x );
+   int const warp = tid >> 5, lane = tid & 31;
+
+   // Stages and ring start as zeros (never uninitialised bits), then the barriers.
+   for( int i = tid; i < M2Smem::OFF_WX / 16; i += NT ) { reinterpret_cast< float4* >( smem )[ i ] = make_float4( 0.f, 0.f, 0.f, 0.f ); }
+   if( tid == 0 ) {
+      mbar_init( &full[ 0 ], 1 );
+      mbar_init( &full[ 1 ], 1 );
+      misc[ 2 ] = 0;
+      fence_mbar_init();
+   }
+   __syncthreads();
+   uint32_t uses[ 2 ] = { 0, 0 };       // completed phases per stage (uniform over the CTA)
+   int volatile* const abort_flag = misc + 2;
+
+   int32_t const total = a.items ? a.nitems : a.nb * a.strips * a.chunks;
+   int32_t next = static_cast< int32_t >( blockIdx.x );
+   for( ;; ) {
+      // ---- next item
+      int32_t it;
+      if( a.queue ) {
+         if( tid == 0 ) { misc[ 0 ] = atomicAdd( a.queue, 1 ); }
+         __syncthreads();
+         it = misc[ 0 ];
+      } else {
+         it = next;
+         next += static_cast< int32_t >( gridDim.x );
+      }
+      if( it >= total || *abort_flag ) { break; }
+      M2Item item;
+      if( a.items ) {
+         item = a.items[ it ];
+         // An impossible item (a corrupted list) is skipped and reported, never followed.
+         bool bad = item.img < 0 || item.img >= a.nimages;
+         if( !bad ) {
+            M2Image const& ib = a.images[ item.img ];
+            bad = item.x0 < 0 || item.x0 >= ib.nx || item.x0 % TX != 0 || item.ya < 0 || item.yb > ib.ny || item.ya >= item.yb;
+         }
+         if( bad ) {
+            if( tid == 0 ) { atomicExch( a.status, DIPCU_ERR_INVALID_ARG ); }
+            __syncthreads();                          // every thread has read this item's index
+            continue;
+         }
+      } else {
+         int32_t const c = it % a.chunks;
+         int32_t const t = it / a.chunks;
+         item.x0 = ( t % a.strips ) * TX;
+         item.img = t / a.strips;
+         item.ya = c * a.lchunk;
+         item.yb = min( item.ya + a.lchunk, a.img0.ny );
+      }
+      M2Image const& im = a.images ? a.images[ item.img ] : a.img0;
+      int const b = a.images ? 0 : item.img;          // batch coordinate of a single-image launch
+      int const nx = im.nx, ny = im.ny;
+      int const hx = im.h[ 0 ], hy = im.h[ 1 ];
+      int const lead = im.lead, bw = im.bw;
+      int const x0 = item.x0, ya = item.ya, yb = item.yb;
+      int const D = ( 2 * hy + R - 1 ) / R;
+      int const NR = ( D + 2 ) * R;
+      int const qtot = yb - ya + 2 * hy;               // input rows of the item
+      int const S = ( qtot + R - 1 ) / R;              // x steps
+      int const J = ( yb - ya + R - 1 ) / R;           // y blocks
+      int const nyb = ( 2 * hy + 1 + 7 ) / 8;          // y tap blocks of 8
+      int const nxq = 1 + lead / 2;                    // x window float4s per lane (4 + 2 lead samples)
+      bool const xedge = x0 - lead < 0 || x0 + TX + lead > nx;
+      float const sx = im.odd[ 0 ] ? -1.f : 1.f, sy = im.odd[ 1 ] ? -1.f : 1.f;
+
+      // ---- set-up: weights, column fixes (edge strips)
+      {
+         float const* hwx = im.w[ 0 ] ? im.w[ 0 ] : a.w0[ 0 ];
+         float const* hwy = im.w[ 1 ] ? im.w[ 1 ] : a.w0[ 1 ];
+         // wx[4 + i], i in [0, 2 lead]: tap d = i - lead (zero beyond hx); wx[0..3] = 0; zero tail.
+         for( int i = tid; i < kM2WxLen; i += NT ) {
+            int const d = i - 4 - lead;
+            float v = 0.f;
+            if( i >= 4 && d >= -hx && d <= hx ) { v = d >= 0 ? hwx[ d ] : sx * hwx[ -d ]; }
+            wx[ i ] = v;
+         }
+         // wy[k], k in [0, 8 nyb): tap d = k - hy (zero beyond hy).
+         for( int k = tid; k < kM2WyLen; k += NT ) {
+            int const d = k - hy;
+            float v = 0.f;
+            if( d >= -hy && d <= hy ) { v = d >= 0 ? hwy[ d ] : sy * hwy[ -d ]; }
+            wy[ k ] = v;
+         }
+         if( xedge && warp == 0 ) {
+            int n = 0;
+            for( int cc = 0; cc < bw; cc += 32 ) {
+               int const c = cc + lane;
+               int const xx = x0 - lead + c;
+               // columns the stored outputs read (outputs beyond the image are never stored)
+               bool want = c < bw && ( xx < 0 || xx >= nx ) && xx >= x0 - hx && xx < min( x0 + TX, nx ) + hx;
+               M2Fix f{};
+               if( want ) {
+                  f.dst = static_cast< int16_t >( c );
+                  if( im.bc[ 0 ] == BC_ADD_ZEROS ) {
+                     f.flags = 4;
+                  } else {
+                     bool neg;
+                     int const sc = static_cast< int >( bc_map_index( xx, nx, im.bc[ 0 ], &neg ));
+                     int const sb = sc - ( x0 - lead );
+                     bool const inbox = sb >= 0 && sb < bw && ( x0 - lead + sb ) >= 0 && ( x0 - lead + sb ) < nx;
+                     f.flags = static_cast< int16_t >(( neg ? 1 : 0 ) | ( inbox ? 0 : 2 ));
+                     f.src = inbox ? sb : sc;
+                  }
+               }
+               uint32_t const m = __ballot_sync( 0xffffffffu, want );
+               int const slot = n + __popc( m & (( 1u << lane ) - 1u ));
+               if( want && slot < kM2MaxFix ) { fix[ slot ] = f; }
+               n += __popc( m );
+            }
+            if( lane == 0 ) { misc[ 1 ] = n < kM2MaxFix ? n : kM2MaxFix; }
+         }
+      }
+      __syncthreads();
+      int const nfix = xedge ? misc[ 1 ] : 0;
+
+      // Issues the TMA load(s) of step s into stage s & 1 and records its rows' sources and signs
+      // and the stage's row stride: bw for one box of R rows, bw rounded up to 128 bytes for one
+      // box per row (each TMA destination 128-byte aligned).
+      auto issue = [ & ]( int s ) {
+         int const st = s & 1;
+         int const r0 = ya - hy + s * R;                 // absolute row of the step's first row
+         unsigned char* const dst = stages + st * M2Smem::STAGE_BYTES;
+         uint32_t const row_bytes = static_cast< uint32_t >( bw ) * sizeof( TIn );
+         if( r0 >= 0 && r0 + R <= ny ) {
+            for( int r = 0; r < R; ++r ) { rsrc[ st * R + r ] = r0 + r; rsgn[ st * R + r ] = 1.f; }
+            misc[ 4 + st ] = bw;
+            mbar_arrive_expect_tx( &full[ st ], R * row_bytes );
+            tma_load_4d( dst, &im.tmap, &full[ st ], x0 - lead, r0, 0, b );
+         } else {
+            uint32_t const pitch = ( row_bytes + 127u ) / 128u * 128u;
+            misc[ 4 + st ] = static_cast< int32_t >( pitch / sizeof( TIn ));
+            mbar_arrive_expect_tx( &full[ st ], R * row_bytes );
+            for( int r = 0; r < R; ++r ) {
+               int yy = r0 + r;
+               float sg = 1.f;
+               if( yy < 0 || yy >= ny ) {
+                  if( im.bc[ 1 ] == BC_ADD_ZEROS ) {
+                     yy = -1;                           // TMA zero fill
+                  } else {
+                     bool neg;
+                     yy = static_cast< int >( bc_map_index( yy, ny, im.bc[ 1 ], &neg ));
+                     sg = neg ? -1.f : 1.f;
+                  }
+               }
+               rsrc[ st * R + r ] = yy;
+               rsgn[ st * R + r ] = sg;
+               tma_load_4d( dst + static_cast< size_t >( r ) * pitch, &im.tmap1, &full[ st ], x0 - lead, yy, 0, b );
+            }
+         }
+      };
+
+      if( tid == 0 ) {
+         fence_proxy_async();                         // earlier generic writes to the stages first
+         issue( 0 );
+         if( S > 1 ) { issue( 1 ); }
+      }
+
+      int const nsteps = max( S, J + D );
+      for( int s = 0; s < nsteps; ++s ) {
+         int const st = s & 1;
+         unsigned char* const stage = stages + st * M2Smem::STAGE_BYTES;
+         if( s < S ) {
+            // ---- wait for the step's rows (a give-up is reported and ends the CTA's work at the
+            // next barrier; no later copy is issued)
+            if( !*abort_flag && !mbar_wait( &full[ st ], uses[ st ] & 1u )) {
+               *abort_flag = 1;
+               atomicExch( a.status, DIPCU_ERR_TIMEOUT );
+            }
+            ++uses[ st ];
+            int const rs = misc[ 4 + st ];             // the stage's row stride (samples)
+            if( nfix > 0 ) {
+               // Halo columns outside the image: their source column's sample (sign included).
+               for( int e = tid; e < nfix * R; e += NT ) {
+                  M2Fix const f = fix[ e % nfix ];
+                  int const r = e / nfix;
+                  float v = 0.f;
+                  if( !( f.flags & 4 )) {
+                     if( f.flags & 2 ) {
+                        int const yy = rsrc[ st * R + r ];
+                        v = yy >= 0 ? m2_src_sample< TIn >( im, b, yy, f.src ) : 0.f;
+                     } else {
+                        v = m2_get< TIn >( stage, rs, r, f.src );
+                     }
+                     if( f.flags & 1 ) { v = -v; }
+                  }
+                  // In-box sources are interior columns, never rewritten here, so the order of the
+                  // rewrites does not matter.
+                  m2_put< TIn >( stage, rs, r, f.dst, v );
+               }
+               __syncthreads();
+            }
+            // ---- x phase: warp w takes rows w, w + 8, ...; lane -> outputs 4 lane .. 4 lane + 3
+            {
+               constexpr int RW = R / 8;                 // rows per warp
+               float acc[ RW ][ 4 ];
+#pragma unroll
+               for( int i = 0; i < RW; ++i ) {
+#pragma unroll
+                  for( int t = 0; t < 4; ++t ) { acc[ i ][ t ] = 0.f; }
+               }
+               int const cb = 4 * lane;                  // box column of the window start (aligned)
+               for( int m = 0; m < nxq; ++m ) {
+                  // taps for window quad m: wx[4m .. 4m + 7]
+                  float4 const wl = *reinterpret_cast< float4 const* >( wx + 4 * m );
+                  float4 const wh = *reinterpret_cast< float4 const* >( wx + 4 * m + 4 );
+                  float const wv[ 8 ] = { wl.x, wl.y, wl.z, wl.w, wh.x, wh.y, wh.z, wh.w };
+#pragma unroll
+                  for( int i = 0; i < RW; ++i ) {
+                     float4 const q = m2_load4< TIn >( stage, rs, warp + 8 * i, cb + 4 * m );
+                     float const qv[ 4 ] = { q.x, q.y, q.z, q.w };
+#pragma unroll
+                     for( int e = 0; e < 4; ++e ) {
+#pragma unroll
+                        for( int t = 0; t < 4; ++t ) {
+                           // sample at box column cb + 4m + e feeds output cb + t with tap
+                           // d = 4m + e - t - lead, i.e. wx[4 + 4m + e - t] = wv[4 + e - t]
+                           acc[ i ][ t ] = fmaf( wv[ 4 + e - t ], qv[ e ], acc[ i ][ t ] );
+                        }
+                     }
+                  }
+               }
+#pragma unroll
+               for( int i = 0; i < RW; ++i ) {
+                  int const r = warp + 8 * i;
+                  int const q = s * R + r;                 // item input row
+                  if( q < qtot ) {
+                     float const sg = rsgn[ st * R + r ];
+                     float4 o = make_float4( sg * acc[ i ][ 0 ], sg * acc[ i ][ 1 ], sg * acc[ i ][ 2 ], sg * acc[ i ][ 3 ] );
+                     *reinterpret_cast< float4* >( ring + static_cast< size_t >( q % NR ) * TX + cb ) = o;
+                  }
+               }
+            }
+         }
+         __syncthreads();
+         if( *abort_flag ) { break; }
+         // ---- stage st is free: stream step s + 2 into it
+         if( tid == 0 && s + 2 < S ) {
+            fence_proxy_async();                      // the column fixes' writes before the copy's
+            issue( s + 2 );
+         }
+         // ---- y phase: block j = s - D (output rows ya + jR ..), thread -> column, RT rows
+         int const j = s - D;
+         if( j >= 0 && j < J ) {
+            constexpr int RT = kM2RT;
+            int const c = tid & ( TX - 1 );
+            int const g = tid >> 7;                      // row half
+            int const t0 = j * R + RT * g;               // item output row offset of the thread's first row
+            float acc[ RT ];
+#pragma unroll
+            for( int t = 0; t < RT; ++t ) { acc[ t ] = 0.f; }
+            // Output row t0 + t needs item input rows t0 + t + k, k in [0, 2 hy]: blocks of 8 taps,
+            // the last one cut at 2 hy (no read beyond the rows the filter covers).
+            int const last = 2 * hy + 1 - 8 * ( nyb - 1 );   // taps in the last block, 1..8
+            for( int kb = 0; kb < nyb; ++kb ) {
+               float4 const w0 = *reinterpret_cast< float4 const* >( wy + 8 * kb );
+               float4 const w1 = *reinterpret_cast< float4 const* >( wy + 8 * kb + 4 );
+               float const wv[ 8 ] = { w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w };
+               int const qb = t0 + 8 * kb;
+               int const nk = kb + 1 < nyb ? 8 : last;
+#pragma unroll
+               for( int u = 0; u < RT + 7; ++u ) {
+                  if( u >= RT - 1 + nk ) { break; }
+                  float const v = ring[ static_cast< size_t >(( qb + u ) % NR ) * TX + c ];
+#pragma unroll
+                  for( int t = 0; t < RT; ++t ) {
+                     int const k = u - t;
+                     if( k >= 0 && k < 8 && k < nk ) { acc[ t ] = fmaf( wv[ k ], v, acc[ t ] ); }
+                  }
+               }
+            }
+            int const xo = x0 + c;
+            if( xo < nx ) {
+               float* p = im.dst + static_cast< int64_t >( b ) * im.dsb + static_cast< int64_t >( ya + t0 ) * im.ds1 + xo;
+#pragma unroll
+               for( int t = 0; t < RT; ++t ) {
+                  if( ya + t0 + t < yb ) { p[ 0 ] = acc[ t ]; }
+                  p += im.ds1;
+               }
+            }
+         }
+      }
+      __syncthreads();   // the item's ring, stages and tables are done with
+   }
+}
+
+// Host side (k_march2d.cu).  Fills one image's TMA maps and geometry; false when the kernel
+// cannot take the image (layout, boundary conditions, half-widths).
+template< typename TIn >
+bool march2d_image( M2Image& im, void const* src, int64_t nx, int64_t ny, int64_t ss1, int64_t nb, int64_t ssb,
+                    float* dst, int64_t ds1, int64_t dsb, int32_t const bc[ 2 ], int32_t const h[ 2 ], int32_t const odd[ 2 ] );
+// Persistent CTAs the kernel runs with (two per SM).
+int march2d_slots();
+// One launch over a device item list pulled through the device counter `counter` (zero before the
+// launch).
+cudaError_t launch_march2d_items( M2Image const* d_images, int nimages, M2Item const* d_items, int nitems, int32_t* counter,
+                                  cudaStream_t stream );
+
+} // namespace dipcu

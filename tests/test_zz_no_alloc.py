@@ -36,11 +36,12 @@ def _call(fn_name, x, out, sig, ords, bcs):
 def _pool_high_water_reset():
     """Resets the high-water mark of the device's default stream-ordered memory pool (the pool
     dipcu_gauss_fir's cudaMallocAsync draws from) and returns a reader of it."""
+    from cuda.bindings import driver as drv
     from cuda.bindings import runtime as rt
     err, pool = rt.cudaDeviceGetDefaultMemPool(0)
     assert err == rt.cudaError_t.cudaSuccess
     attr = rt.cudaMemPoolAttr.cudaMemPoolAttrUsedMemHigh
-    (err,) = rt.cudaMemPoolSetAttribute(pool, attr, rt.cuuint64_t(0))
+    (err,) = rt.cudaMemPoolSetAttribute(pool, attr, drv.cuuint64_t(0))
     assert err == rt.cudaError_t.cudaSuccess
 
     def read() -> int:
