@@ -13,12 +13,14 @@ import torch
 from . import _abi
 from .filtering import BoundaryConditionFromString, ParameterError, _array_use_parameter, check, image_desc
 
-__all__ = ["BatchPlan", "device_status", "GRAPH", "AUTOTUNE", "INJECT_INVALID_IMAGE", "INJECT_INVALID_TILE"]
+__all__ = ["BatchPlan", "device_status", "GRAPH", "AUTOTUNE", "INJECT_INVALID_IMAGE", "INJECT_INVALID_TILE",
+           "INJECT_STALLED_COPY"]
 
 GRAPH = 1
 AUTOTUNE = 2
 INJECT_INVALID_IMAGE = 256
 INJECT_INVALID_TILE = 512
+INJECT_STALLED_COPY = 1024
 
 
 def device_status(clear: bool = True) -> int:

@@ -1020,6 +1020,7 @@ struct dipcu_batch_plan {
    int32_t* d_mcounter = nullptr;
    int m_nitems = 0;
    int m_runlen[ 4 ] = { 384, 384, 384, 384 };
+   int m_stall = 0;                        // DIPCU_BATCH_INJECT_STALLED_COPY
 };
 
 namespace {
@@ -1255,7 +1256,8 @@ cudaError_t march_launch( dipcu_batch_plan* p, cudaStream_t st ) {
    if( p->m_nitems == 0 ) { return cudaSuccess; }
    cudaError_t e = cudaMemsetAsync( p->d_mcounter, 0, sizeof( int32_t ), st );
    if( e != cudaSuccess ) { return e; }
-   return launch_march2d_items( p->d_mimg, static_cast< int >( p->mimg.size()), p->d_mitems, p->m_nitems, p->d_mcounter, st );
+   return launch_march2d_items( p->d_mimg, static_cast< int >( p->mimg.size()), p->d_mitems, p->m_nitems, p->d_mcounter,
+                                p->m_stall, st );
 }
 
 // Autotuner of the row-march path: per class of y half-width present in the batch, the row-run
@@ -1503,7 +1505,8 @@ int dipcu_batch_plan_create( dipcu_image_desc const* ins, dipcu_image_desc const
    // overwritten by the final runs), remembering the winner per batch signature.
    int shape = 0;
    if( char const* env = getenv( "DIPCU_BATCH_SHAPE" )) { shape = std::max( 0, std::min( 2, atoi( env ))); }
-   if(( flags & DIPCU_BATCH_AUTOTUNE ) && !p->mimg.empty()) {
+   p->m_stall = ( flags & DIPCU_BATCH_INJECT_STALLED_COPY ) ? 1 : 0;
+   if(( flags & DIPCU_BATCH_AUTOTUNE ) && !p->mimg.empty() && !p->m_stall ) {
       if( int st = march_tune( p, sig )) { dipcu_batch_plan_destroy( p ); return st; }
    }
    if( int st = march_items( p, m_inject )) { dipcu_batch_plan_destroy( p ); return st; }

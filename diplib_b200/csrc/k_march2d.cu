@@ -152,7 +152,7 @@ cudaError_t run_march2d( FusedArgs const& f, int32_t const h[ 2 ], int32_t const
 } // namespace
 
 cudaError_t launch_march2d_items( M2Image const* d_images, int nimages, M2Item const* d_items, int nitems, int32_t* counter,
-                                  cudaStream_t stream ) {
+                                  int stall, cudaStream_t stream ) {
    if( nitems <= 0 ) { return cudaSuccess; }
    if( !march2d_ready< float >()) { return cudaErrorNotSupported; }
    M2Args a{};
@@ -161,6 +161,8 @@ cudaError_t launch_march2d_items( M2Image const* d_images, int nimages, M2Item c
    a.items = d_items;
    a.nitems = nitems;
    a.queue = counter;
+   a.stall_copies = stall ? 1 : 0;
+   a.wait_limit = stall ? 20000u : 0u;       // a stalled copy is given up on after ~10 ms, not seconds
    a.status = device_status_ptr();
    if( !a.status ) { return cudaErrorUnknown; }
    int const slots = march2d_slots();

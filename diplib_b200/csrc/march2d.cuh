@@ -9,18 +9,20 @@
 //     filtered along x into a ring of x-filtered rows (each warp a row, each lane 4 outputs from
 //     aligned float4 windows, taps in tap quads broadcast from shared memory);
 //   * y phase: one step behind the rows it needs, the ring's rows are filtered along y into R output
-//     rows (each thread one column and R / 2 rows, taps in blocks of 8, R / 2 + 7 ring rows per block)
+//     rows (each thread one column and R / 2 rows, taps in blocks of 8, R / 2 + 7 ring rows per block,
+//     loaded ahead of the block's FMAs)
 //     and stored straight to global memory (each warp 32 consecutive columns: 128-byte rows).
-// One __syncthreads per step (x-phase results visible to the y phase); the ring holds (D + 2) R rows
-// (D = ceil(2 hy / R)), so that a step's x phase never overwrites rows an earlier step's y phase
-// may still read.  The next-but-one step's TMA goes out as soon as a stage is free.  Each input pixel
+// One __syncthreads per step (x-phase results visible to the y phase); the ring of 128 rows holds
+// at least (D + 2) R (D = ceil(2 hy / R)), so that a step's x phase never overwrites rows an earlier
+// step's y phase may still read.  The next-but-one step's TMA goes out as soon as a stage is free.  Each input pixel
 // crosses HBM once (the x-halo columns of neighbouring strips hit L2) and each output pixel is
 // written once; the only recomputation is the x phase of the 2 hy rows of halo at the start of each
 // item's row run.
 //
-// Half-widths up to 32 on each axis, runtime taps (no compile-time buckets): the x filter is padded
-// to the TMA granule LEAD >= hx on both sides, the y filter to a multiple of 8 taps (the last block
-// cut at 2 hy, so that no row beyond the filter's support is read).  Boundary conditions in x:
+// Half-widths up to 32 on each axis, runtime taps: the x filter is padded to the TMA granule
+// LEAD >= hx on both sides (the x phase compiled per LEAD), the y filter to a multiple of 8 taps
+// (the y phase compiled per number of tap blocks; the last block cut at 2 hy, so that no row beyond
+// the filter's support is read).  Boundary conditions in x:
 // every index-mapping one ("mirror", "asym mirror", "periodic", "asym periodic", "zero order") and
 // "add zeros": halo columns outside the image are rewritten in the stage from their source column
 // (a copy inside the box, or a load from the image where the source lies outside it), sign
@@ -48,7 +50,8 @@ constexpr int kM2NT = 256;          // threads per CTA
 constexpr int kM2MaxH = 32;         // largest half-width along either axis
 constexpr int kM2MaxLead = 32;      // LEAD for hx = 32
 constexpr int kM2MaxBW = kM2TX + 2 * kM2MaxLead;
-constexpr int kM2MaxRing = ( 2 + ( 2 * kM2MaxH + kM2R - 1 ) / kM2R ) * kM2R;
+constexpr int kM2Ring = 128;        // ring rows (a power of two >= (D + 2) R for every hy <= 32)
+static_assert(( 2 + ( 2 * kM2MaxH + kM2R - 1 ) / kM2R ) * kM2R <= kM2Ring, "ring holds (D + 2) R rows" );
 constexpr int kM2MaxFix = 2 * kM2MaxLead;
 constexpr int kM2WxLen = 4 + 2 * kM2MaxLead + 8;   // 4 leading zeros, 2 LEAD + 1 taps, zero tail
 constexpr int kM2WyLen = 2 * kM2MaxH + 8;
@@ -85,6 +88,9 @@ struct M2Args {
    int32_t nimages;           // entries of `images`
    int32_t* queue;            // device work counter (batch; zero before the launch); null: static
    int32_t* status;
+   uint32_t wait_limit;       // polls before a wait for a copy gives up (0: kWaitLimit)
+   int32_t stall_copies;      // test hook: the copies are announced but never issued, so every wait
+                              // for one gives up (nothing is ever in flight)
    // single-image geometry: items = nb x strips x chunks, chunk = `lchunk` rows
    int32_t nb, strips, chunks, lchunk;
    float w0[ 2 ][ kM2MaxH + 1 ];   // single-image half kernels (x, y), centre first
@@ -94,7 +100,7 @@ struct M2Smem {
    static constexpr int STAGE_BYTES = kM2R * kM2MaxBW * 4;                       // float stage (u16 uses half)
    static constexpr int OFF_STAGE = 0;
    static constexpr int OFF_RING = OFF_STAGE + 2 * STAGE_BYTES;
-   static constexpr int OFF_WX = OFF_RING + kM2MaxRing * kM2TX * 4;
+   static constexpr int OFF_WX = OFF_RING + kM2Ring * kM2TX * 4;
    static constexpr int OFF_WY = OFF_WX + kM2WxLen * 4;
    static constexpr int OFF_ROWS = OFF_WY + kM2WyLen * 4;                        // [2][R] source row, [2][R] sign
    static constexpr int OFF_FIX = OFF_ROWS + 4 * kM2R * 4;                       // [kM2MaxFix] fix entries
@@ -155,6 +161,75 @@ __device__ __forceinline__ float m2_src_sample( M2Image const& im, int b, int ro
    return static_cast< float >( *p );
 }
 
+// x phase of one step for LEAD = 4 LQ: warp w filters stage rows w, w + 8, w + 16; lane l the
+// outputs 4 l .. 4 l + 3 from the aligned window of 4 + 2 LEAD samples (1 + 2 LQ float4s).  The
+// sample at window offset 4 m + e feeds output t with tap d = 4 m + e - t - LEAD; pairs with
+// |d| > LEAD (the window's corners) are skipped at compile time, so each output takes 2 LEAD + 1
+// FMAs (taps beyond hx are zero).
+template< typename TIn, int LQ >
+__device__ __forceinline__ void m2_xphase( unsigned char const* stage, int rs, int warp, int lane, float const* wx,
+                                           float ( &acc )[ kM2R / 8 ][ 4 ] ) {
+   constexpr int RW = kM2R / 8, NQ = 1 + 2 * LQ, LEAD = 4 * LQ;
+   int const cb = 4 * lane;
+#pragma unroll
+   for( int m = 0; m < NQ; ++m ) {
+      float4 const wl = *reinterpret_cast< float4 const* >( wx + 4 * m );
+      float4 const wh = *reinterpret_cast< float4 const* >( wx + 4 * m + 4 );
+      float const wv[ 8 ] = { wl.x, wl.y, wl.z, wl.w, wh.x, wh.y, wh.z, wh.w };
+#pragma unroll
+      for( int i = 0; i < RW; ++i ) {
+         float4 const q = m2_load4< TIn >( stage, rs, warp + 8 * i, cb + 4 * m );
+         float const qv[ 4 ] = { q.x, q.y, q.z, q.w };
+#pragma unroll
+         for( int e = 0; e < 4; ++e ) {
+#pragma unroll
+            for( int t = 0; t < 4; ++t ) {
+               int const d = 4 * m + e - t - LEAD;
+               if( d < -LEAD || d > LEAD ) { continue; }
+               acc[ i ][ t ] = fmaf( wv[ 4 + e - t ], qv[ e ], acc[ i ][ t ] );   // wx[4 + 4m + e - t]
+            }
+         }
+      }
+   }
+}
+
+// y phase of one block for NYB tap blocks of 8: the thread's column c, output rows t0 .. t0 + RT - 1
+// (item offsets), from ring rows t0 + k, k in [0, 8 NYB); the last block reads only the rows up to
+// t0 + RT - 1 + 2 hy (zeros beyond: `nlast` rows), so no row outside the filter's support is read.
+// Ring rows are slots modulo kM2Ring; a block whose rows do not wrap reads them at immediate offsets.
+template< int NYB >
+__device__ __forceinline__ void m2_yphase( float const* ring, float const* wy, int c, int t0, int nlast,
+                                           float ( &acc )[ kM2RT ] ) {
+   constexpr int RT = kM2RT, NU = RT + 7, TX = kM2TX;
+#pragma unroll
+   for( int kb = 0; kb < NYB; ++kb ) {
+      float4 const w0 = *reinterpret_cast< float4 const* >( wy + 8 * kb );
+      float4 const w1 = *reinterpret_cast< float4 const* >( wy + 8 * kb + 4 );
+      float const wv[ 8 ] = { w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w };
+      int const sb = ( t0 + 8 * kb ) & ( kM2Ring - 1 );
+      float v[ NU ];
+      bool const last = kb == NYB - 1;
+      if( sb + NU <= kM2Ring ) {
+         float const* p = ring + sb * TX + c;
+#pragma unroll
+         for( int u = 0; u < NU; ++u ) { v[ u ] = ( !last || u < nlast ) ? p[ u * TX ] : 0.f; }
+      } else {
+#pragma unroll
+         for( int u = 0; u < NU; ++u ) {
+            v[ u ] = ( !last || u < nlast ) ? ring[ (( sb + u ) & ( kM2Ring - 1 )) * TX + c ] : 0.f;
+         }
+      }
+#pragma unroll
+      for( int u = 0; u < NU; ++u ) {
+#pragma unroll
+         for( int t = 0; t < RT; ++t ) {
+            int const k = u - t;
+            if( k >= 0 && k < 8 ) { acc[ t ] = fmaf( wv[ k ], v[ u ], acc[ t ] ); }
+         }
+      }
+   }
+}
+
 template< typename TIn >
 __global__ void __launch_bounds__( kM2NT, 2 ) march2d_kernel( M2Args const __grid_constant__ a ) {
    constexpr int R = kM2R, TX = kM2TX, NT = kM2NT;
@@ -166,7 +241,7 @@ __global__ void __launch_bounds__( kM2NT, 2 ) march2d_kernel( M2Args const __gri
    int32_t* const rsrc = reinterpret_cast< int32_t* >( smem + M2Smem::OFF_ROWS );   // [2][R]
    float* const rsgn = reinterpret_cast< float* >( rsrc + 2 * R );                   // [2][R]
    M2Fix* const fix = reinterpret_cast< M2Fix* >( smem + M2Smem::OFF_FIX );
-   // misc: [0] item, [1] fixes, [2] abort, [4..5] stage row strides
+   // misc: [0] item, [1] fixes, [2] abort, [4..5] stage row strides, [6..7] stage interior, [8..9] stage first row
    int32_t* const misc = reinterpret_cast< int32_t* >( smem + M2Smem::OFF_MISC );
    uint64_t* const full = reinterpret_cast< uint64_t* >( smem + M2Smem::OFF_BAR );
    int const tid = static_cast< int >( threadIdx.x );
@@ -182,6 +257,8 @@ __global__ void __launch_bounds__( kM2NT, 2 ) march2d_kernel( M2Args const __gri
    }
    __syncthreads();
    uint32_t uses[ 2 ] = { 0, 0 };       // completed phases per stage (uniform over the CTA)
+   uint32_t issued[ 2 ] = { 0, 0 };     // phases announced per stage (thread 0)
+   uint32_t const wait_limit = a.wait_limit ? a.wait_limit : kWaitLimit;
    int volatile* const abort_flag = misc + 2;
 
    int32_t const total = a.items ? a.nitems : a.nb * a.strips * a.chunks;
@@ -227,12 +304,10 @@ __global__ void __launch_bounds__( kM2NT, 2 ) march2d_kernel( M2Args const __gri
       int const lead = im.lead, bw = im.bw;
       int const x0 = item.x0, ya = item.ya, yb = item.yb;
       int const D = ( 2 * hy + R - 1 ) / R;
-      int const NR = ( D + 2 ) * R;
       int const qtot = yb - ya + 2 * hy;               // input rows of the item
       int const S = ( qtot + R - 1 ) / R;              // x steps
       int const J = ( yb - ya + R - 1 ) / R;           // y blocks
       int const nyb = ( 2 * hy + 1 + 7 ) / 8;          // y tap blocks of 8
-      int const nxq = 1 + lead / 2;                    // x window float4s per lane (4 + 2 lead samples)
       bool const xedge = x0 - lead < 0 || x0 + TX + lead > nx;
       float const sx = im.odd[ 0 ] ? -1.f : 1.f, sy = im.odd[ 1 ] ? -1.f : 1.f;
 
@@ -294,13 +369,16 @@ __global__ void __launch_bounds__( kM2NT, 2 ) march2d_kernel( M2Args const __gri
          int const r0 = ya - hy + s * R;                 // absolute row of the step's first row
          unsigned char* const dst = stages + st * M2Smem::STAGE_BYTES;
          uint32_t const row_bytes = static_cast< uint32_t >( bw ) * sizeof( TIn );
+         ++issued[ st ];
+         misc[ 8 + st ] = r0;
          if( r0 >= 0 && r0 + R <= ny ) {
-            for( int r = 0; r < R; ++r ) { rsrc[ st * R + r ] = r0 + r; rsgn[ st * R + r ] = 1.f; }
+            misc[ 6 + st ] = 1;                          // interior: rows r0 .. r0 + R - 1, signs +1
             misc[ 4 + st ] = bw;
             mbar_arrive_expect_tx( &full[ st ], R * row_bytes );
-            tma_load_4d( dst, &im.tmap, &full[ st ], x0 - lead, r0, 0, b );
+            if( !a.stall_copies ) { tma_load_4d( dst, &im.tmap, &full[ st ], x0 - lead, r0, 0, b ); }
          } else {
             uint32_t const pitch = ( row_bytes + 127u ) / 128u * 128u;
+            misc[ 6 + st ] = 0;
             misc[ 4 + st ] = static_cast< int32_t >( pitch / sizeof( TIn ));
             mbar_arrive_expect_tx( &full[ st ], R * row_bytes );
             for( int r = 0; r < R; ++r ) {
@@ -317,7 +395,9 @@ __global__ void __launch_bounds__( kM2NT, 2 ) march2d_kernel( M2Args const __gri
                }
                rsrc[ st * R + r ] = yy;
                rsgn[ st * R + r ] = sg;
-               tma_load_4d( dst + static_cast< size_t >( r ) * pitch, &im.tmap1, &full[ st ], x0 - lead, yy, 0, b );
+               if( !a.stall_copies ) {
+                  tma_load_4d( dst + static_cast< size_t >( r ) * pitch, &im.tmap1, &full[ st ], x0 - lead, yy, 0, b );
+               }
             }
          }
       };
@@ -335,12 +415,14 @@ __global__ void __launch_bounds__( kM2NT, 2 ) march2d_kernel( M2Args const __gri
          if( s < S ) {
             // ---- wait for the step's rows (a give-up is reported and ends the CTA's work at the
             // next barrier; no later copy is issued)
-            if( !*abort_flag && !mbar_wait( &full[ st ], uses[ st ] & 1u )) {
+            if( !*abort_flag && !mbar_wait( &full[ st ], uses[ st ] & 1u, wait_limit )) {
                *abort_flag = 1;
                atomicExch( a.status, DIPCU_ERR_TIMEOUT );
             }
             ++uses[ st ];
             int const rs = misc[ 4 + st ];             // the stage's row stride (samples)
+            bool const interior = misc[ 6 + st ] != 0;
+            int const r0s = misc[ 8 + st ];
             if( nfix > 0 ) {
                // Halo columns outside the image: their source column's sample (sign included).
                for( int e = tid; e < nfix * R; e += NT ) {
@@ -349,7 +431,7 @@ __global__ void __launch_bounds__( kM2NT, 2 ) march2d_kernel( M2Args const __gri
                   float v = 0.f;
                   if( !( f.flags & 4 )) {
                      if( f.flags & 2 ) {
-                        int const yy = rsrc[ st * R + r ];
+                        int const yy = interior ? r0s + r : rsrc[ st * R + r ];
                         v = yy >= 0 ? m2_src_sample< TIn >( im, b, yy, f.src ) : 0.f;
                      } else {
                         v = m2_get< TIn >( stage, rs, r, f.src );
@@ -362,44 +444,37 @@ __global__ void __launch_bounds__( kM2NT, 2 ) march2d_kernel( M2Args const __gri
                }
                __syncthreads();
             }
-            // ---- x phase: warp w takes rows w, w + 8, ...; lane -> outputs 4 lane .. 4 lane + 3
+            // ---- x phase: warp w takes rows w, w + 8, w + 16; lane -> outputs 4 lane .. 4 lane + 3
             {
-               constexpr int RW = R / 8;                 // rows per warp
+               constexpr int RW = R / 8;
                float acc[ RW ][ 4 ];
 #pragma unroll
                for( int i = 0; i < RW; ++i ) {
 #pragma unroll
                   for( int t = 0; t < 4; ++t ) { acc[ i ][ t ] = 0.f; }
                }
-               int const cb = 4 * lane;                  // box column of the window start (aligned)
-               for( int m = 0; m < nxq; ++m ) {
-                  // taps for window quad m: wx[4m .. 4m + 7]
-                  float4 const wl = *reinterpret_cast< float4 const* >( wx + 4 * m );
-                  float4 const wh = *reinterpret_cast< float4 const* >( wx + 4 * m + 4 );
-                  float const wv[ 8 ] = { wl.x, wl.y, wl.z, wl.w, wh.x, wh.y, wh.z, wh.w };
-#pragma unroll
-                  for( int i = 0; i < RW; ++i ) {
-                     float4 const q = m2_load4< TIn >( stage, rs, warp + 8 * i, cb + 4 * m );
-                     float const qv[ 4 ] = { q.x, q.y, q.z, q.w };
-#pragma unroll
-                     for( int e = 0; e < 4; ++e ) {
-#pragma unroll
-                        for( int t = 0; t < 4; ++t ) {
-                           // sample at box column cb + 4m + e feeds output cb + t with tap
-                           // d = 4m + e - t - lead, i.e. wx[4 + 4m + e - t] = wv[4 + e - t]
-                           acc[ i ][ t ] = fmaf( wv[ 4 + e - t ], qv[ e ], acc[ i ][ t ] );
-                        }
-                     }
-                  }
+               switch( lead / 4 ) {
+                  case 1: m2_xphase< TIn, 1 >( stage, rs, warp, lane, wx, acc ); break;
+                  case 2: m2_xphase< TIn, 2 >( stage, rs, warp, lane, wx, acc ); break;
+                  case 3: m2_xphase< TIn, 3 >( stage, rs, warp, lane, wx, acc ); break;
+                  case 4: m2_xphase< TIn, 4 >( stage, rs, warp, lane, wx, acc ); break;
+                  case 5: m2_xphase< TIn, 5 >( stage, rs, warp, lane, wx, acc ); break;
+                  case 6: m2_xphase< TIn, 6 >( stage, rs, warp, lane, wx, acc ); break;
+                  case 7: m2_xphase< TIn, 7 >( stage, rs, warp, lane, wx, acc ); break;
+                  default: m2_xphase< TIn, 8 >( stage, rs, warp, lane, wx, acc ); break;
                }
+               int const cb = 4 * lane;
 #pragma unroll
                for( int i = 0; i < RW; ++i ) {
                   int const r = warp + 8 * i;
                   int const q = s * R + r;                 // item input row
                   if( q < qtot ) {
-                     float const sg = rsgn[ st * R + r ];
-                     float4 o = make_float4( sg * acc[ i ][ 0 ], sg * acc[ i ][ 1 ], sg * acc[ i ][ 2 ], sg * acc[ i ][ 3 ] );
-                     *reinterpret_cast< float4* >( ring + static_cast< size_t >( q % NR ) * TX + cb ) = o;
+                     float4 o = make_float4( acc[ i ][ 0 ], acc[ i ][ 1 ], acc[ i ][ 2 ], acc[ i ][ 3 ] );
+                     if( !interior ) {
+                        float const sg = rsgn[ st * R + r ];
+                        o = make_float4( sg * o.x, sg * o.y, sg * o.z, sg * o.w );
+                     }
+                     *reinterpret_cast< float4* >( ring + ( q & ( kM2Ring - 1 )) * TX + cb ) = o;
                   }
                }
             }
@@ -421,25 +496,18 @@ __global__ void __launch_bounds__( kM2NT, 2 ) march2d_kernel( M2Args const __gri
             float acc[ RT ];
 #pragma unroll
             for( int t = 0; t < RT; ++t ) { acc[ t ] = 0.f; }
-            // Output row t0 + t needs item input rows t0 + t + k, k in [0, 2 hy]: blocks of 8 taps,
-            // the last one cut at 2 hy (no read beyond the rows the filter covers).
-            int const last = 2 * hy + 1 - 8 * ( nyb - 1 );   // taps in the last block, 1..8
-            for( int kb = 0; kb < nyb; ++kb ) {
-               float4 const w0 = *reinterpret_cast< float4 const* >( wy + 8 * kb );
-               float4 const w1 = *reinterpret_cast< float4 const* >( wy + 8 * kb + 4 );
-               float const wv[ 8 ] = { w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w };
-               int const qb = t0 + 8 * kb;
-               int const nk = kb + 1 < nyb ? 8 : last;
-#pragma unroll
-               for( int u = 0; u < RT + 7; ++u ) {
-                  if( u >= RT - 1 + nk ) { break; }
-                  float const v = ring[ static_cast< size_t >(( qb + u ) % NR ) * TX + c ];
-#pragma unroll
-                  for( int t = 0; t < RT; ++t ) {
-                     int const k = u - t;
-                     if( k >= 0 && k < 8 && k < nk ) { acc[ t ] = fmaf( wv[ k ], v, acc[ t ] ); }
-                  }
-               }
+            // Output row t0 + t needs item input rows t0 + t + k, k in [0, 2 hy].
+            int const nlast = RT - 1 + ( 2 * hy + 1 - 8 * ( nyb - 1 ));   // rows the last tap block reads
+            switch( nyb ) {
+               case 1: m2_yphase< 1 >( ring, wy, c, t0, nlast, acc ); break;
+               case 2: m2_yphase< 2 >( ring, wy, c, t0, nlast, acc ); break;
+               case 3: m2_yphase< 3 >( ring, wy, c, t0, nlast, acc ); break;
+               case 4: m2_yphase< 4 >( ring, wy, c, t0, nlast, acc ); break;
+               case 5: m2_yphase< 5 >( ring, wy, c, t0, nlast, acc ); break;
+               case 6: m2_yphase< 6 >( ring, wy, c, t0, nlast, acc ); break;
+               case 7: m2_yphase< 7 >( ring, wy, c, t0, nlast, acc ); break;
+               case 8: m2_yphase< 8 >( ring, wy, c, t0, nlast, acc ); break;
+               default: m2_yphase< 9 >( ring, wy, c, t0, nlast, acc ); break;
             }
             int const xo = x0 + c;
             if( xo < nx ) {
@@ -451,6 +519,17 @@ __global__ void __launch_bounds__( kM2NT, 2 ) march2d_kernel( M2Args const __gri
                }
             }
          }
+      }
+      if( *abort_flag ) {
+         // Before the CTA ends: the copies it announced and did not consume land first (bounded
+         // waits again; a copy that never comes is given up on like the first).
+         if( tid == 0 ) {
+            for( int st = 0; st < 2; ++st ) {
+               for( ; uses[ st ] < issued[ st ]; ++uses[ st ] ) { mbar_wait( &full[ st ], uses[ st ] & 1u, wait_limit ); }
+            }
+         }
+         __syncthreads();
+         break;
       }
       __syncthreads();   // the item's ring, stages and tables are done with
    }
@@ -464,8 +543,9 @@ bool march2d_image( M2Image& im, void const* src, int64_t nx, int64_t ny, int64_
 // Persistent CTAs the kernel runs with (two per SM).
 int march2d_slots();
 // One launch over a device item list pulled through the device counter `counter` (zero before the
-// launch).
+// launch).  `stall` (a test hook): the copies are announced but never issued and every wait gives
+// up after a short limit, so the kernel reports DIPCU_ERR_TIMEOUT with nothing in flight.
 cudaError_t launch_march2d_items( M2Image const* d_images, int nimages, M2Item const* d_items, int nitems, int32_t* counter,
-                                  cudaStream_t stream );
+                                  int stall, cudaStream_t stream );
 
 } // namespace dipcu

@@ -45,10 +45,11 @@ __device__ __forceinline__ void named_bar_arrive( int id, int threads ) {
    asm volatile( "bar.arrive %0, %1;" :: "r"( id ), "r"( threads ) : "memory" );
 }
 
-// Bounded wait for the phase with parity `parity` to complete.  Returns false on timeout.
-__device__ __forceinline__ bool mbar_wait( uint64_t* bar, uint32_t parity ) {
+// Bounded wait for the phase with parity `parity` to complete (at most `limit` polls).  Returns
+// false on timeout.
+__device__ __forceinline__ bool mbar_wait( uint64_t* bar, uint32_t parity, uint32_t limit = kWaitLimit ) {
    uint32_t addr = smem_u32( bar );
-   for( uint32_t it = 0; it < kWaitLimit; ++it ) {
+   for( uint32_t it = 0; it < limit; ++it ) {
       uint32_t done;
       asm volatile(
             "{\n\t.reg .pred p;\n\t"

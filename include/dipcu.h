@@ -23,7 +23,9 @@ extern "C" {
 
 #define DIPCU_MAX_DIMS 8
 
-/* Sample types: the real dip::DataType values (include/diplib/library/datatype.h). */
+/* Sample types: DIPlib's real types (include/diplib/library/datatype.h).  The codes are this
+ * library's own (dip::DataType's internal enumerator order differs); a DIPlib caller converts with a
+ * switch, as DipTypeToDipcu in INTEGRATION.md does. */
 typedef enum {
    DIPCU_BIN = 0, DIPCU_UINT8 = 1, DIPCU_UINT16 = 2, DIPCU_UINT32 = 3, DIPCU_UINT64 = 4,
    DIPCU_SINT8 = 5, DIPCU_SINT16 = 6, DIPCU_SINT32 = 7, DIPCU_SINT64 = 8,
@@ -152,8 +154,11 @@ int dipcu_structure_tensor_backward( dipcu_image_desc const* grad_out, dipcu_ima
  * Flags: DIPCU_BATCH_GRAPH captures the run (queue reset, on-device weights, all launches)
  * into a CUDA graph so that dipcu_batch_plan_run is one graph launch; DIPCU_BATCH_AUTOTUNE times
  * the persistent kernel's candidate tile shapes on this batch at creation (overwriting the outputs) and keeps the
- * fastest, remembered per batch signature.  The two INJECT flags are test hooks that plant one
- * impossible work item, which the kernels skip and report through dipcu_device_status.
+ * fastest, remembered per batch signature.  The INJECT flags are test hooks: INVALID_IMAGE and
+ * INVALID_TILE plant one impossible work item, which the kernels skip and report through
+ * dipcu_device_status; STALLED_COPY makes the row-march launch announce its TMA copies without
+ * issuing them, so that its bounded waits give up (after ~10 ms) and it reports DIPCU_ERR_TIMEOUT
+ * with no copy in flight -- the context stays usable.
  * The plan allocates its tables and the line-pass intermediate at creation; runs allocate nothing.  The images must stay alive
  * while the plan is used.  The sigma table (dipcu_batch_plan_sigmas, device, 2 * count doubles)
  * may be rewritten between runs, as long as no kernel length changes. */
@@ -162,6 +167,7 @@ typedef struct dipcu_batch_plan dipcu_batch_plan;
 #define DIPCU_BATCH_AUTOTUNE 2
 #define DIPCU_BATCH_INJECT_INVALID_IMAGE 256
 #define DIPCU_BATCH_INJECT_INVALID_TILE 512
+#define DIPCU_BATCH_INJECT_STALLED_COPY 1024
 int dipcu_batch_plan_create( dipcu_image_desc const* ins, dipcu_image_desc const* outs, int count,
                              double const* sigmas, uint32_t const* orders, int32_t const* bcs, double truncation,
                              int flags, dipcu_batch_plan** plan );

@@ -133,3 +133,24 @@ def test_batch_tile_path_periodic_edges(cuda):
         err = np.abs(outs[i].cpu().numpy() - ref).max()
         assert err <= 1e-5 * max(1.0, float(a.max() - a.min())), (i, a.shape, s, o, bc, err)
     plan.close()
+
+
+def test_batch_stalled_copy_times_out_and_the_context_stays_usable(cuda):
+    """A copy that never lands: with INJECT_STALLED_COPY the row-march launch announces its TMA copies
+    without issuing them, so its bounded waits give up after a short limit; the launch reports
+    DIPCU_ERR_TIMEOUT through the device status word with nothing in flight, and the same context
+    then runs a normal plan correctly (no GPU fault, no hang)."""
+    from diplib_b200 import _abi
+    from diplib_b200.batch import INJECT_STALLED_COPY, device_status
+    device_status(clear=True)
+    rng = np.random.default_rng(12)
+    imgs = [rng.random(s, dtype=np.float32) for s in [(100, 128), (77, 260), (200, 64)]]   # rows TMA can address
+    params = [(2.0, [0, 1], "mirror"), (4.0, [1, 0], "periodic"), (1.0, [2, 2], "add zeros")]
+    plan, ins, outs = run_plan(imgs, params, graph=False, autotune=False, flags=INJECT_STALLED_COPY)
+    assert plan.info()["kernels_per_run"] == 2                    # weights and the row-march launch
+    assert device_status(clear=True) == _abi.ERR_TIMEOUT
+    plan.close()
+    plan, ins, outs = run_plan(imgs, params, graph=True, autotune=False)
+    check_all(imgs, params, outs)
+    assert device_status(clear=True) == 0
+    plan.close()

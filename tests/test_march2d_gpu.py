@@ -51,6 +51,6 @@ def test_shapes_types_and_boundaries(cuda, shape, dt, sig, ords, bcs):
 def test_batch_axis(cuda):
     rng = np.random.default_rng(4)
     x = rng.random((3, 90, 260), dtype=np.float32)
-    ref = oracle.gauss_fir(x, [6.0, 4.0, 0.0], [2, 1, 0], ["periodic", "mirror"], 3.0)
-    got = dip().GaussFIR(x, [6.0, 4.0, 0.0], [2, 1, 0], ["periodic", "mirror"], 3.0)
+    ref = oracle.gauss_fir(x, [6.0, 4.0, 0.0], [2, 1, 0], ["periodic", "mirror", "mirror"], 3.0)
+    got = dip().GaussFIR(x, [6.0, 4.0, 0.0], [2, 1, 0], ["periodic", "mirror", "mirror"], 3.0)
     assert_close(got, ref, x, "batch axis")
