@@ -5,10 +5,11 @@ The Python API mirrors PyDIP's (``Gauss``, ``GaussFIR``, ``Derivative`` ...); al
 runs in libdipcu.so's CUDA kernels through the C-ABI declared in include/dipcu.h.
 """
 from .filtering import (BestGaussMethod, BoundaryConditionFromString, Derivative, Error, Gauss, GaussFIR,
-                        ParameterError, RunTimeError, flex_dtype, image_desc)
+                        OneDimensionalFilter, ParameterError, RunTimeError, SeparableConvolution, Uniform, flex_dtype,
+                        image_desc)
 from .analysis import StructureTensor
 from .derivatives import Gradient, GradientMagnitude, Hessian, Laplace
 
 __all__ = ["BestGaussMethod", "BoundaryConditionFromString", "Derivative", "Error", "Gauss", "GaussFIR", "Gradient",
-           "GradientMagnitude", "Hessian", "Laplace", "ParameterError", "StructureTensor", "RunTimeError",
-           "flex_dtype", "image_desc"]
+           "GradientMagnitude", "Hessian", "Laplace", "OneDimensionalFilter", "ParameterError", "SeparableConvolution",
+           "StructureTensor", "RunTimeError", "Uniform", "flex_dtype", "image_desc"]

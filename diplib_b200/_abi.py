@@ -38,6 +38,19 @@ class ImageDesc(ctypes.Structure):
     ]
 
 
+class Filter1D(ctypes.Structure):
+    """dipcu_filter_1d: a real 1D filter (dip::OneDimensionalFilter)."""
+    _fields_ = [
+        ("weights", ctypes.POINTER(ctypes.c_double)),
+        ("size", ctypes.c_int64),
+        ("origin", ctypes.c_int64),
+        ("symmetry", ctypes.c_int32),
+    ]
+
+
+# dipcu_symmetry codes, by dip::OneDimensionalFilter::symmetry string (real filters: "conj" is "even").
+SYMMETRY = {"": 0, "general": 0, "even": 1, "odd": 2, "conj": 1, "d-even": 3, "d-odd": 4, "d-conj": 3}
+
 _lib = None
 _lock = threading.Lock()
 
@@ -49,6 +62,10 @@ SIGNATURES = {
     "dipcu_gauss_fir_noalloc": (ctypes.c_int, [_P(ImageDesc), _P(ImageDesc), _P(ctypes.c_double),
                                                _P(ctypes.c_uint32), _P(ctypes.c_int32), ctypes.c_double,
                                                ctypes.c_void_p]),
+    "dipcu_separable_convolution": (ctypes.c_int, [_P(ImageDesc), _P(ImageDesc), _P(Filter1D), ctypes.c_int,
+                                                   _P(ctypes.c_int32), _P(ctypes.c_uint8), ctypes.c_void_p]),
+    "dipcu_uniform": (ctypes.c_int, [_P(ImageDesc), _P(ImageDesc), _P(ctypes.c_double), _P(ctypes.c_int32),
+                                     ctypes.c_void_p]),
     "dipcu_gauss_fir_backward": (ctypes.c_int, [_P(ImageDesc), _P(ImageDesc), _P(ImageDesc), ctypes.c_void_p,
                                                 _P(ctypes.c_double), _P(ctypes.c_uint32), _P(ctypes.c_int32),
                                                 ctypes.c_double, ctypes.c_void_p]),

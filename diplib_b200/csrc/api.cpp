@@ -131,9 +131,11 @@ bool try_fused( dipcu_image_desc const* in, dipcu_image_desc const* out, std::ve
       a.db = 0;
    }
    if( np == 2 ) {
-      *err = launch_march2d( key, a, stream );
-      if( *err != cudaErrorNotSupported ) { return true; }
+      // Half-widths up to 12: the warp-per-tile kernel (packed FMAs, no block barrier) is the
+      // faster one; beyond, and for the layouts and conditions it hands back, the row march.
       *err = launch_fused2d_ws( key, a, stream );
+      if( *err != cudaErrorNotSupported ) { return true; }
+      *err = launch_march2d( key, a, stream );
       if( *err != cudaErrorNotSupported ) { return true; }
    }
    if( !fused_available( key )) { return false; }
@@ -296,6 +298,11 @@ int run_line_passes( dipcu_image_desc const* in, dipcu_image_desc const* out, st
       lp.bc = af.bc;
       lp.compute_double = compute_double;
       lp.taps = af.taps.data();
+      lp.mode = af.mode;
+      lp.lo = af.lo;
+      lp.hi = af.hi;
+      lp.usize = af.usize;
+      lp.full = af.full.data();
       cudaError_t e = launch_line_pass( lp, stream );
       if( e != cudaSuccess ) { status = cuda_fail( e, "line_pass_kernel" ); break; }
       src = dst;

@@ -32,11 +32,19 @@ struct LinePass {
    int64_t sizes[ DIPCU_MAX_DIMS ];
    int64_t src_strides[ DIPCU_MAX_DIMS ];
    int64_t dst_strides[ DIPCU_MAX_DIMS ];
-   int64_t h;
+   int64_t h;           // border: the boundary extension on both sides (the half-width in mode 0)
    int32_t odd, bc;
    bool compute_double;
-   double const* taps;  // h + 1 host values, centre first
+   double const* taps;  // mode 0: h + 1 host values, centre first
+   // mode 0: symmetric or antisymmetric taps (the Gaussian); mode 1: a general filter,
+   // out[i] = sum_{j=-lo}^{hi} full[j + lo] x[i + j] (lo + hi + 1 <= kGeneralMaxTaps host values);
+   // mode 2: the rectangular uniform filter of `usize` samples, window [i - usize/2, i + (usize+1)/2),
+   // as a running sum in the order of dip::Uniform's line filter (src/linear/uniform.cpp:41-62).
+   int32_t mode = 0;
+   int64_t lo = 0, hi = 0, usize = 0;
+   double const* full = nullptr;
 };
+constexpr int kGeneralMaxTaps = 256;
 cudaError_t launch_line_pass( LinePass const& p, cudaStream_t stream );
 
 struct ConvertArgs {
@@ -133,13 +141,17 @@ int record_error( int code, char const* msg );
 // once, at capture).  Every launch site calls it right after its <<< >>> statement.
 void count_launch();
 
-// Per-axis filter as dip::GaussFIR builds it (src/linear/gauss.cpp:255-284).
+// Per-axis filter as dip::GaussFIR builds it (src/linear/gauss.cpp:255-284); modes 1 and 2 (a
+// general filter, the rectangular uniform filter) as LinePass describes them.
 struct AxisFilter {
    bool process = false;
    int64_t h = 0;
    int32_t odd = 0;
    int32_t bc = 0;
    std::vector< double > taps;  // centre first, rounded to the compute precision
+   int32_t mode = 0;
+   int64_t lo = 0, hi = 0, usize = 0;
+   std::vector< double > full;  // mode 1: lo + hi + 1 taps, rounded to the compute precision
 };
 
 // Checks an (in, out) image pair: forged, same sizes, valid types, non-overlapping.

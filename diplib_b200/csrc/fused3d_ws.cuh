@@ -292,6 +292,12 @@ __global__ void __launch_bounds__( W5Geom< TIn, HX, HY, HZ >::NT, W5Geom< TIn, H
       if( warp < NWI ) {
          // ---- in-plane warps: per plane pair, y pass, x-edge fix, x pass -> ring
          float4* const b2 = reinterpret_cast< float4* >( smem + G::OFF_B2 + warp * G::B2_BYTES );   // [TY/2][BW/2]
+         // The taps as register pairs (packed FMAs take register operands).
+         float2 wyr[ HY + 1 ], wxr[ HX + 1 ];
+#pragma unroll
+         for( int k = 0; k <= HY; ++k ) { wyr[ k ] = a.w[ 1 ][ k ]; }
+#pragma unroll
+         for( int k = 0; k <= HX; ++k ) { wxr[ k ] = a.w[ 0 ][ k ]; }
          int pq = pfirst;
          for( int j = 0; j < nblocks; ++j ) {
             uint32_t const blk = gblock + static_cast< uint32_t >( j );
@@ -325,11 +331,11 @@ __global__ void __launch_bounds__( W5Geom< TIn, HX, HY, HZ >::NT, W5Geom< TIn, H
                         float2 o[ TY ];
 #pragma unroll
                         for( int t = 0; t < TY; ++t ) {
-                           float2 acc = OY ? make_float2( 0.f, 0.f ) : fmul2( a.w[ 1 ][ 0 ], v[ t + HY ] );
+                           float2 acc = OY ? make_float2( 0.f, 0.f ) : fmul2( wyr[ 0 ], v[ t + HY ] );
 #pragma unroll
                            for( int k = 1; k <= HY; ++k ) {
                               float2 const ps = OY ? fsub2( v[ t + HY + k ], v[ t + HY - k ] ) : fadd2( v[ t + HY + k ], v[ t + HY - k ] );
-                              acc = ffma2( a.w[ 1 ][ k ], ps, acc );
+                              acc = ffma2( wyr[ k ], ps, acc );
                            }
                            o[ t ] = acc;
                         }
@@ -384,11 +390,11 @@ __global__ void __launch_bounds__( W5Geom< TIn, HX, HY, HZ >::NT, W5Geom< TIn, H
 #pragma unroll
                      for( int c = 0; c < 2; ++c ) {
                         constexpr int C0 = HX + E;
-                        float2 acc = OX ? make_float2( 0.f, 0.f ) : fmul2( a.w[ 0 ][ 0 ], vx[ C0 + c ] );
+                        float2 acc = OX ? make_float2( 0.f, 0.f ) : fmul2( wxr[ 0 ], vx[ C0 + c ] );
 #pragma unroll
                         for( int k = 1; k <= HX; ++k ) {
                            float2 const ps = OX ? fsub2( vx[ C0 + c + k ], vx[ C0 + c - k ] ) : fadd2( vx[ C0 + c + k ], vx[ C0 + c - k ] );
-                           acc = ffma2( a.w[ 0 ][ k ], ps, acc );
+                           acc = ffma2( wxr[ k ], ps, acc );
                         }
                         out[ c ] = zneg ? make_float2( -acc.x, -acc.y ) : acc;
                      }
@@ -405,6 +411,13 @@ __global__ void __launch_bounds__( W5Geom< TIn, HX, HY, HZ >::NT, W5Geom< TIn, H
       } else {
          // ---- z warps: per block, accumulate RZ outputs per column pair from the ring
          int const zt = tid - NWI * 32;
+         // The full z kernel as register pairs (index k + HZ for tap k; odd kernels negated below 0).
+         float2 wzr[ 2 * HZ + 1 ];
+#pragma unroll
+         for( int k = -HZ; k <= HZ; ++k ) {
+            float2 const w = a.w[ 2 ][ k >= 0 ? k : -k ];
+            wzr[ k + HZ ] = ( OZ && k < 0 ) ? make_float2( -w.x, -w.y ) : w;
+         }
          for( int j = 0; j < nblocks; ++j ) {
             uint32_t const blk = gblock + static_cast< uint32_t >( j );
             named_bar_sync( kBarReady + ( blk & 1u ), NWC * 32 );
@@ -425,8 +438,7 @@ __global__ void __launch_bounds__( W5Geom< TIn, HX, HY, HZ >::NT, W5Geom< TIn, H
                      int const k = i - t - HZ;
                      if( k < -HZ || k > HZ ) { continue; }
                      if( OZ && k == 0 ) { continue; }
-                     float2 const wk = k >= 0 ? a.w[ 2 ][ k ] : ( OZ ? make_float2( -a.w[ 2 ][ -k ].x, -a.w[ 2 ][ -k ].y ) : a.w[ 2 ][ -k ] );
-                     acc[ t ] = ffma2( wk, v, acc[ t ] );
+                     acc[ t ] = ffma2( wzr[ k + HZ ], v, acc[ t ] );
                   }
                }
                int const xo = x0 + 2 * cp, yo = y0 + y;

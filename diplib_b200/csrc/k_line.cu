@@ -32,6 +32,7 @@ struct LineArgs {
    int32_t ndims, axis, comp;   // comp: the axis the L lines of a tile run along, or -1
    int32_t L, T_out, W;         // lines per tile, outputs per tile, staged samples per line
    int32_t h, odd, bc, across;  // across: threads run along `comp` when staging
+   int32_t general, lo, hi;     // general: taps[0 .. lo + hi] is a full filter over offsets -lo .. hi
    int64_t n, ncomp, nouter;    // line length, size along comp, number of tile rows
    int64_t sizes[ DIPCU_MAX_DIMS ];
    int64_t sst[ DIPCU_MAX_DIMS ], dstst[ DIPCU_MAX_DIMS ];
@@ -97,6 +98,12 @@ __global__ void __launch_bounds__( 256 ) line_pass_kernel( LineArgs< T, MAXH1 > 
          int64_t i = a0 + t;
          if( line >= a.ncomp || i >= a.n ) { continue; }
          T const* c = tile + l * a.W + t + a.h;
+         if( a.general ) {
+            T sum = T( 0 );
+            for( int j = 0; j <= a.lo + a.hi; ++j ) { sum = fma( a.taps[ j ], c[ j - a.lo ], sum ); }
+            store_from< T >( a.dst, a.dst_dt, dbase + line * ( a.comp >= 0 ? a.dstst[ a.comp ] : 0 ) + i * a.dstst[ a.axis ], sum );
+            continue;
+         }
          T sum = a.taps[ 0 ] * c[ 0 ];
          if( a.odd ) {
             for( int k = 1; k <= a.h; ++k ) { sum = fma( a.taps[ k ], c[ k ] - c[ -k ], sum ); }
@@ -425,7 +432,14 @@ cudaError_t launch_line( LinePass const& p, cudaStream_t stream ) {
       a.sst[ d ] = p.src_strides[ d ];
       a.dstst[ d ] = p.dst_strides[ d ];
    }
-   for( int k = 0; k <= p.h; ++k ) { a.taps[ k ] = static_cast< T >( p.taps[ k ] ); }
+   if( p.mode == 1 ) {
+      a.general = 1;
+      a.lo = static_cast< int32_t >( p.lo );
+      a.hi = static_cast< int32_t >( p.hi );
+      for( int64_t k = 0; k <= p.lo + p.hi; ++k ) { a.taps[ k ] = static_cast< T >( p.full[ k ] ); }
+   } else {
+      for( int k = 0; k <= p.h; ++k ) { a.taps[ k ] = static_cast< T >( p.taps[ k ] ); }
+   }
 
    // Companion axis: the smallest source stride among the other axes of size > 1.
    int comp = -1;
@@ -476,8 +490,91 @@ cudaError_t launch_line( LinePass const& p, cudaStream_t stream ) {
 
 } // namespace
 
+// The rectangular uniform filter along one axis: one thread per line keeps the running sum of
+// RectangularUniformLineFilter::Filter (src/linear/uniform.cpp:41-62 in DIPlib) in the same
+// operation order, over the line extended by `border` samples with the boundary condition.
+struct UniformArgs {
+   void const* src;
+   void* dst;
+   int32_t src_dt, dst_dt, ndims, axis, bc;
+   int64_t n, nlines, usize, border;
+   int64_t sizes[ DIPCU_MAX_DIMS ];
+   int64_t sst[ DIPCU_MAX_DIMS ], dstst[ DIPCU_MAX_DIMS ];
+};
+
+// Additions and the product in the reference's order, never contracted into FMAs.
+__device__ __forceinline__ float uadd( float a, float b ) { return __fadd_rn( a, b ); }
+__device__ __forceinline__ double uadd( double a, double b ) { return __dadd_rn( a, b ); }
+__device__ __forceinline__ float usub( float a, float b ) { return __fsub_rn( a, b ); }
+__device__ __forceinline__ double usub( double a, double b ) { return __dsub_rn( a, b ); }
+__device__ __forceinline__ float umul( float a, float b ) { return __fmul_rn( a, b ); }
+__device__ __forceinline__ double umul( double a, double b ) { return __dmul_rn( a, b ); }
+
+template< typename T >
+__global__ void __launch_bounds__( 128 ) uniform_line_kernel( UniformArgs const __grid_constant__ a ) {
+   int64_t const line = static_cast< int64_t >( blockIdx.x ) * blockDim.x + threadIdx.x;
+   if( line >= a.nlines ) { return; }
+   int64_t rem = line, sbase = 0, dbase = 0;
+   for( int d = 0; d < a.ndims; ++d ) {
+      if( d == a.axis ) { continue; }
+      int64_t const c = rem % a.sizes[ d ];
+      rem /= a.sizes[ d ];
+      sbase += c * a.sst[ d ];
+      dbase += c * a.dstst[ d ];
+   }
+   int64_t const sa = a.sst[ a.axis ], da = a.dstst[ a.axis ], n = a.n;
+   auto ld = [ & ]( int64_t i ) { return load_as< T >( a.src, a.src_dt, sbase + i * sa ); };
+   auto x = [ & ]( int64_t j ) { return ( j >= 0 && j < n ) ? ld( j ) : bc_extend< T >( j, n, a.bc, a.border, ld ); };
+   T const norm = T( 1 ) / static_cast< T >( a.usize );
+   int64_t left = -( a.usize / 2 ), right = ( a.usize + 1 ) / 2;
+   T sum = T( 0 );
+   for( int64_t j = left; j < right; ++j ) { sum = uadd( sum, x( j )); }
+   store_from< T >( a.dst, a.dst_dt, dbase, umul( sum, norm ));
+   for( int64_t ii = 1; ii < n; ++ii ) {
+      sum = usub( sum, x( left ));
+      sum = uadd( sum, x( right ));
+      ++left;
+      ++right;
+      store_from< T >( a.dst, a.dst_dt, dbase + ii * da, umul( sum, norm ));
+   }
+}
+
+template< typename T >
+cudaError_t launch_uniform( LinePass const& p, cudaStream_t stream ) {
+   UniformArgs a{};
+   a.src = p.src;
+   a.dst = p.dst;
+   a.src_dt = p.src_dt;
+   a.dst_dt = p.dst_dt;
+   a.ndims = p.ndims;
+   a.axis = p.axis;
+   a.bc = p.bc;
+   a.n = p.sizes[ p.axis ];
+   a.usize = p.usize;
+   a.border = p.h;
+   int64_t total = 1;
+   for( int d = 0; d < p.ndims; ++d ) {
+      a.sizes[ d ] = p.sizes[ d ];
+      a.sst[ d ] = p.src_strides[ d ];
+      a.dstst[ d ] = p.dst_strides[ d ];
+      total *= p.sizes[ d ];
+   }
+   a.nlines = total / a.n;
+   int64_t const blocks = ( a.nlines + 127 ) / 128;
+   if( blocks > 0x7fffffff ) { return cudaErrorInvalidValue; }
+   uniform_line_kernel< T ><<< static_cast< unsigned >( blocks ), 128, 0, stream >>>( a ); count_launch();
+   return cudaGetLastError();
+}
+
 cudaError_t launch_line_pass( LinePass const& p, cudaStream_t stream ) {
    if( p.h < 0 || p.h > kLineMaxHalf ) { return cudaErrorInvalidValue; }
+   if( p.mode == 2 ) {
+      return p.compute_double ? launch_uniform< double >( p, stream ) : launch_uniform< float >( p, stream );
+   }
+   if( p.mode == 1 ) {
+      if( p.lo < 0 || p.hi < 0 || p.lo + p.hi + 1 > kGeneralMaxTaps ) { return cudaErrorInvalidValue; }
+      return p.compute_double ? launch_line< double, kGeneralMaxTaps >( p, stream ) : launch_line< float, kGeneralMaxTaps >( p, stream );
+   }
    {
       cudaError_t const e = launch_line_fast( p, stream );
       if( e != cudaErrorNotSupported ) { return e; }

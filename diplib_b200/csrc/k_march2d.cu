@@ -82,10 +82,14 @@ bool march2d_image( M2Image& im, void const* src, int64_t nx, int64_t ny, int64_
    if( h[ 0 ] > kM2MaxH || h[ 1 ] > kM2MaxH || h[ 0 ] < 0 || h[ 1 ] < 0 ) { return false; }
    if( nx < 1 || ny < 1 || nx > 0x7fffffff || ny > 0x7fffffff || nb < 1 || nb > 0x7fffffff ) { return false; }
    if( ss1 <= 0 || ( nb > 1 && ssb <= 0 )) { return false; }
-   if(( reinterpret_cast< uintptr_t >( src ) & 15 ) != 0 || ( ss1 * esz ) % 16 || ( nb > 1 && ( ssb * esz ) % 16 )) { return false; }
    bool const is_float = std::is_same< TIn, float >::value;
+   bool const tma_ok = ( reinterpret_cast< uintptr_t >( src ) & 15 ) == 0 && ( ss1 * esz ) % 16 == 0 &&
+                       ( nb <= 1 || ( ssb * esz ) % 16 == 0 );
+   // Rows TMA cannot address: float images take the per-thread copy path.
+   if( !tma_ok && !( is_float && ( reinterpret_cast< uintptr_t >( src ) & 3 ) == 0 )) { return false; }
    if( !bc_marchable( bc[ 0 ], is_float ) || !bc_marchable( bc[ 1 ], is_float )) { return false; }
    im = M2Image{};
+   im.tma = tma_ok ? 1 : 0;
    im.lead = ( h[ 0 ] + A - 1 ) / A * A;
    if( im.lead < A ) { im.lead = A; }
    im.bw = kM2TX + 2 * im.lead;
@@ -96,15 +100,18 @@ bool march2d_image( M2Image& im, void const* src, int64_t nx, int64_t ny, int64_
    cuuint64_t strides[ 3 ] = { static_cast< cuuint64_t >( ss1 * esz ), static_cast< cuuint64_t >( ss1 * esz * ny ),
                                static_cast< cuuint64_t >(( nb > 1 ? ssb : ss1 * ny ) * esz ) };
    cuuint32_t box[ 4 ] = { static_cast< cuuint32_t >( im.bw ), static_cast< cuuint32_t >( kM2R ), 1, 1 };
-   if( encode_source_map( &im.tmap, dt, src, dims, strides, box ) != CUDA_SUCCESS ) { return false; }
-   box[ 1 ] = 1;
-   if( encode_source_map( &im.tmap1, dt, src, dims, strides, box ) != CUDA_SUCCESS ) { return false; }
+   if( im.tma ) {
+      if( encode_source_map( &im.tmap, dt, src, dims, strides, box ) != CUDA_SUCCESS ) { return false; }
+      box[ 1 ] = 1;
+      if( encode_source_map( &im.tmap1, dt, src, dims, strides, box ) != CUDA_SUCCESS ) { return false; }
+   }
    im.src = src;
    im.ss1 = ss1;
    im.ssb = ssb;
    im.dst = dst;
    im.ds1 = ds1;
    im.dsb = dsb;
+   im.vec_out = (( reinterpret_cast< uintptr_t >( dst ) & 7 ) == 0 && ds1 % 2 == 0 && ( nb <= 1 || dsb % 2 == 0 )) ? 1 : 0;
    im.nx = static_cast< int32_t >( nx );
    im.ny = static_cast< int32_t >( ny );
    for( int i = 0; i < 2; ++i ) {

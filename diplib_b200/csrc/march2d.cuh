@@ -9,9 +9,9 @@
 //     filtered along x into a ring of x-filtered rows (each warp a row, each lane 4 outputs from
 //     aligned float4 windows, taps in tap quads broadcast from shared memory);
 //   * y phase: one step behind the rows it needs, the ring's rows are filtered along y into R output
-//     rows (each thread one column and R / 2 rows, taps in blocks of 8, R / 2 + 7 ring rows per block,
-//     loaded ahead of the block's FMAs)
-//     and stored straight to global memory (each warp 32 consecutive columns: 128-byte rows).
+//     rows (each thread a column pair and R / 4 rows with packed f32x2 FMAs, taps in blocks of 8,
+//     R / 4 + 7 ring rows per block loaded ahead of the block's FMAs)
+//     and stored straight to global memory (each warp 64 consecutive columns: 256-byte rows).
 // One __syncthreads per step (x-phase results visible to the y phase); the ring of 128 rows holds
 // at least (D + 2) R (D = ceil(2 hy / R)), so that a step's x phase never overwrites rows an earlier
 // step's y phase may still read.  The next-but-one step's TMA goes out as soon as a stage is free.  Each input pixel
@@ -45,7 +45,7 @@ namespace dipcu {
 
 constexpr int kM2TX = 128;          // output columns per strip
 constexpr int kM2R = 24;            // rows per step (and per y-phase block)
-constexpr int kM2RT = kM2R / 2;     // output rows per thread in the y phase
+constexpr int kM2RT = kM2R / 4;     // output rows per thread in the y phase (a column pair per thread)
 constexpr int kM2NT = 256;          // threads per CTA
 constexpr int kM2MaxH = 32;         // largest half-width along either axis
 constexpr int kM2MaxLead = 32;      // LEAD for hx = 32
@@ -54,7 +54,7 @@ constexpr int kM2Ring = 128;        // ring rows (a power of two >= (D + 2) R fo
 static_assert(( 2 + ( 2 * kM2MaxH + kM2R - 1 ) / kM2R ) * kM2R <= kM2Ring, "ring holds (D + 2) R rows" );
 constexpr int kM2MaxFix = 2 * kM2MaxLead;
 constexpr int kM2WxLen = 4 + 2 * kM2MaxLead + 8;   // 4 leading zeros, 2 LEAD + 1 taps, zero tail
-constexpr int kM2WyLen = 2 * kM2MaxH + 8;
+constexpr int kM2WyLen = 9 * 8;      // 9 blocks of 8 taps (2 hy + 1 <= 65), as duplicated pairs
 
 // One image of a launch.  `tmap` boxes are (bw, R) for the interior steps, `tmap1` (bw, 1) for
 // rows at the image's edges; both 4D (x, y, 1, b).
@@ -71,6 +71,9 @@ struct alignas( 64 ) M2Image {
    int32_t odd[ 2 ];
    int32_t lead;              // box columns before the strip (multiple of the TMA granule, >= h[0])
    int32_t bw;                // box width = 128 + 2 lead
+   int32_t vec_out;           // destination rows take float2 stores (8-byte aligned origin, even row stride)
+   int32_t tma;               // 1: stages filled by TMA; 0 (float images whose rows TMA cannot address):
+                              // by per-thread 4-byte asynchronous copies
    float const* w[ 2 ];       // half kernels (centre first, h + 1 taps) in device memory; null: M2Args::w0
 };
 
@@ -102,11 +105,11 @@ struct M2Smem {
    static constexpr int OFF_RING = OFF_STAGE + 2 * STAGE_BYTES;
    static constexpr int OFF_WX = OFF_RING + kM2Ring * kM2TX * 4;
    static constexpr int OFF_WY = OFF_WX + kM2WxLen * 4;
-   static constexpr int OFF_ROWS = OFF_WY + kM2WyLen * 4;                        // [2][R] source row, [2][R] sign
+   static constexpr int OFF_ROWS = OFF_WY + kM2WyLen * 8;                        // [2][R] source row, [2][R] sign
    static constexpr int OFF_FIX = OFF_ROWS + 4 * kM2R * 4;                       // [kM2MaxFix] fix entries
    static constexpr int OFF_MISC = OFF_FIX + kM2MaxFix * 8;                      // 16 ints
    static constexpr int OFF_BAR = ( OFF_MISC + 64 + 15 ) / 16 * 16;
-   static constexpr int BYTES = OFF_BAR + 2 * 8;
+   static constexpr int BYTES = OFF_BAR + 4 * 8;                                // TMA and copy barriers per stage
    static_assert( OFF_RING % 128 == 0 && STAGE_BYTES % 128 == 0, "TMA destinations 128-byte aligned" );
    static_assert( OFF_WX % 16 == 0 && OFF_WY % 16 == 0, "float4 weight reads" );
    static_assert( BYTES <= 113 * 1024, "two CTAs per SM" );
@@ -154,6 +157,17 @@ __device__ __forceinline__ void m2_put( unsigned char* stage, int rs, int row, i
    }
 }
 
+// 4-byte asynchronous copy global -> shared; `bytes` 0 writes a zero (the source is not read).
+__device__ __forceinline__ void m2_cp4( void* dst, void const* src, int bytes ) {
+   asm volatile( "cp.async.ca.shared.global [%0], [%1], 4, %2;" :: "r"( smem_u32( dst )), "l"( src ), "r"( bytes ) : "memory" );
+}
+
+// The mbarrier's pending count drops when all of this thread's earlier asynchronous copies have
+// landed (the barrier's arrival count includes this arrival).
+__device__ __forceinline__ void m2_cp_arrive( uint64_t* bar ) {
+   asm volatile( "cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" :: "r"( smem_u32( bar )) : "memory" );
+}
+
 template< typename TIn >
 __device__ __forceinline__ float m2_src_sample( M2Image const& im, int b, int row, int col ) {
    TIn const* p = static_cast< TIn const* >( im.src ) + static_cast< int64_t >( b ) * im.ssb +
@@ -193,30 +207,37 @@ __device__ __forceinline__ void m2_xphase( unsigned char const* stage, int rs, i
    }
 }
 
-// y phase of one block for NYB tap blocks of 8: the thread's column c, output rows t0 .. t0 + RT - 1
-// (item offsets), from ring rows t0 + k, k in [0, 8 NYB); the last block reads only the rows up to
-// t0 + RT - 1 + 2 hy (zeros beyond: `nlast` rows), so no row outside the filter's support is read.
-// Ring rows are slots modulo kM2Ring; a block whose rows do not wrap reads them at immediate offsets.
+// y phase of one block for NYB tap blocks of 8, on column pairs with packed f32x2 FMAs: the
+// thread's columns 2 cp, 2 cp + 1, output rows t0 .. t0 + RT - 1 (item offsets), from ring rows
+// t0 + k, k in [0, 8 NYB); the last block reads only the rows up to t0 + RT - 1 + 2 hy (zeros
+// beyond: `nlast` rows), so no row outside the filter's support is read.  Taps are duplicated pairs
+// (w, w).  Ring rows are slots modulo kM2Ring; a block whose rows do not wrap reads them at immediate
+// offsets.
 template< int NYB >
-__device__ __forceinline__ void m2_yphase( float const* ring, float const* wy, int c, int t0, int nlast,
-                                           float ( &acc )[ kM2RT ] ) {
+__device__ __forceinline__ void m2_yphase( float const* ring, float2 const* wy2, int cp, int t0, int nlast,
+                                           float2 ( &acc )[ kM2RT ] ) {
    constexpr int RT = kM2RT, NU = RT + 7, TX = kM2TX;
 #pragma unroll
    for( int kb = 0; kb < NYB; ++kb ) {
-      float4 const w0 = *reinterpret_cast< float4 const* >( wy + 8 * kb );
-      float4 const w1 = *reinterpret_cast< float4 const* >( wy + 8 * kb + 4 );
-      float const wv[ 8 ] = { w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w };
+      float2 wv[ 8 ];
+#pragma unroll
+      for( int h = 0; h < 4; ++h ) {
+         float4 const w4 = *reinterpret_cast< float4 const* >( wy2 + 8 * kb + 2 * h );
+         wv[ 2 * h ] = make_float2( w4.x, w4.y );
+         wv[ 2 * h + 1 ] = make_float2( w4.z, w4.w );
+      }
       int const sb = ( t0 + 8 * kb ) & ( kM2Ring - 1 );
-      float v[ NU ];
+      float2 v[ NU ];
       bool const last = kb == NYB - 1;
       if( sb + NU <= kM2Ring ) {
-         float const* p = ring + sb * TX + c;
+         float2 const* p = reinterpret_cast< float2 const* >( ring + sb * TX ) + cp;
 #pragma unroll
-         for( int u = 0; u < NU; ++u ) { v[ u ] = ( !last || u < nlast ) ? p[ u * TX ] : 0.f; }
+         for( int u = 0; u < NU; ++u ) { v[ u ] = ( !last || u < nlast ) ? p[ u * ( TX / 2 ) ] : make_float2( 0.f, 0.f ); }
       } else {
 #pragma unroll
          for( int u = 0; u < NU; ++u ) {
-            v[ u ] = ( !last || u < nlast ) ? ring[ (( sb + u ) & ( kM2Ring - 1 )) * TX + c ] : 0.f;
+            v[ u ] = ( !last || u < nlast ) ? reinterpret_cast< float2 const* >( ring + (( sb + u ) & ( kM2Ring - 1 )) * TX )[ cp ]
+                                            : make_float2( 0.f, 0.f );
          }
       }
 #pragma unroll
@@ -224,7 +245,7 @@ __device__ __forceinline__ void m2_yphase( float const* ring, float const* wy, i
 #pragma unroll
          for( int t = 0; t < RT; ++t ) {
             int const k = u - t;
-            if( k >= 0 && k < 8 ) { acc[ t ] = fmaf( wv[ k ], v[ u ], acc[ t ] ); }
+            if( k >= 0 && k < 8 ) { acc[ t ] = __ffma2_rn( wv[ k ], v[ u ], acc[ t ] ); }
          }
       }
    }
@@ -237,13 +258,13 @@ __global__ void __launch_bounds__( kM2NT, 2 ) march2d_kernel( M2Args const __gri
    unsigned char* const stages = smem + M2Smem::OFF_STAGE;
    float* const ring = reinterpret_cast< float* >( smem + M2Smem::OFF_RING );
    float* const wx = reinterpret_cast< float* >( smem + M2Smem::OFF_WX );
-   float* const wy = reinterpret_cast< float* >( smem + M2Smem::OFF_WY );
+   float2* const wy2 = reinterpret_cast< float2* >( smem + M2Smem::OFF_WY );
    int32_t* const rsrc = reinterpret_cast< int32_t* >( smem + M2Smem::OFF_ROWS );   // [2][R]
    float* const rsgn = reinterpret_cast< float* >( rsrc + 2 * R );                   // [2][R]
    M2Fix* const fix = reinterpret_cast< M2Fix* >( smem + M2Smem::OFF_FIX );
    // misc: [0] item, [1] fixes, [2] abort, [4..5] stage row strides, [6..7] stage interior, [8..9] stage first row
    int32_t* const misc = reinterpret_cast< int32_t* >( smem + M2Smem::OFF_MISC );
-   uint64_t* const full = reinterpret_cast< uint64_t* >( smem + M2Smem::OFF_BAR );
+   uint64_t* const full = reinterpret_cast< uint64_t* >( smem + M2Smem::OFF_BAR );   // [2] TMA, [2] copies
    int const tid = static_cast< int >( threadIdx.x );
    int const warp = tid >> 5, lane = tid & 31;
 
@@ -252,12 +273,15 @@ __global__ void __launch_bounds__( kM2NT, 2 ) march2d_kernel( M2Args const __gri
    if( tid == 0 ) {
       mbar_init( &full[ 0 ], 1 );
       mbar_init( &full[ 1 ], 1 );
+      mbar_init( &full[ 2 ], NT );               // every thread's copies of a stage
+      mbar_init( &full[ 3 ], NT );
       misc[ 2 ] = 0;
       fence_mbar_init();
    }
    __syncthreads();
-   uint32_t uses[ 2 ] = { 0, 0 };       // completed phases per stage (uniform over the CTA)
-   uint32_t issued[ 2 ] = { 0, 0 };     // phases announced per stage (thread 0)
+   uint32_t uses0 = 0, uses1 = 0;       // completed phases per stage (uniform over the CTA)
+   uint32_t cuses0 = 0, cuses1 = 0;     // the same for the copy barriers
+   uint32_t issued0 = 0, issued1 = 0;   // phases announced per stage (thread 0)
    uint32_t const wait_limit = a.wait_limit ? a.wait_limit : kWaitLimit;
    int volatile* const abort_flag = misc + 2;
 
@@ -322,12 +346,12 @@ __global__ void __launch_bounds__( kM2NT, 2 ) march2d_kernel( M2Args const __gri
             if( i >= 4 && d >= -hx && d <= hx ) { v = d >= 0 ? hwx[ d ] : sx * hwx[ -d ]; }
             wx[ i ] = v;
          }
-         // wy[k], k in [0, 8 nyb): tap d = k - hy (zero beyond hy).
+         // wy2[k] = (w, w), k in [0, 72): tap d = k - hy (zero beyond hy).
          for( int k = tid; k < kM2WyLen; k += NT ) {
             int const d = k - hy;
             float v = 0.f;
             if( d >= -hy && d <= hy ) { v = d >= 0 ? hwy[ d ] : sy * hwy[ -d ]; }
-            wy[ k ] = v;
+            wy2[ k ] = make_float2( v, v );
          }
          if( xedge && warp == 0 ) {
             int n = 0;
@@ -369,7 +393,7 @@ __global__ void __launch_bounds__( kM2NT, 2 ) march2d_kernel( M2Args const __gri
          int const r0 = ya - hy + s * R;                 // absolute row of the step's first row
          unsigned char* const dst = stages + st * M2Smem::STAGE_BYTES;
          uint32_t const row_bytes = static_cast< uint32_t >( bw ) * sizeof( TIn );
-         ++issued[ st ];
+         if( st ) { ++issued1; } else { ++issued0; }
          misc[ 8 + st ] = r0;
          if( r0 >= 0 && r0 + R <= ny ) {
             misc[ 6 + st ] = 1;                          // interior: rows r0 .. r0 + R - 1, signs +1
@@ -402,10 +426,49 @@ __global__ void __launch_bounds__( kM2NT, 2 ) march2d_kernel( M2Args const __gri
          }
       };
 
-      if( tid == 0 ) {
-         fence_proxy_async();                         // earlier generic writes to the stages first
-         issue( 0 );
-         if( S > 1 ) { issue( 1 ); }
+      // The per-thread copy path: warp w copies rows w, w + 8, w + 16 of step s (lane 0 records each
+      // row's source and sign), its lanes the row's columns; columns and "add zeros" rows outside the
+      // image become zeros (the column fixes then rewrite the boundary columns).
+      bool const tma = im.tma != 0;
+      auto copy = [ & ]( int s ) {
+         int const st = s & 1;
+         int const r0 = ya - hy + s * R;
+         float* const dstf = reinterpret_cast< float* >( stages + st * M2Smem::STAGE_BYTES );
+         float const* const base = static_cast< float const* >( im.src ) + static_cast< int64_t >( b ) * im.ssb;
+#pragma unroll
+         for( int i = 0; i < R / 8; ++i ) {
+            int const r = warp + 8 * i;
+            int yy = r0 + r;
+            float sg = 1.f;
+            if( yy < 0 || yy >= ny ) {
+               if( im.bc[ 1 ] == BC_ADD_ZEROS ) {
+                  yy = -1;
+               } else {
+                  bool neg;
+                  yy = static_cast< int >( bc_map_index( yy, ny, im.bc[ 1 ], &neg ));
+                  sg = neg ? -1.f : 1.f;
+               }
+            }
+            if( lane == 0 ) { rsrc[ st * R + r ] = yy; rsgn[ st * R + r ] = sg; }
+            float const* const srow = base + static_cast< int64_t >( yy < 0 ? 0 : yy ) * im.ss1;
+            for( int c = lane; c < bw; c += 32 ) {
+               int const xx = x0 - lead + c;
+               bool const ok = yy >= 0 && xx >= 0 && xx < nx;
+               m2_cp4( dstf + r * bw + c, ok ? srow + xx : base, ok ? 4 : 0 );
+            }
+         }
+         m2_cp_arrive( &full[ 2 + st ] );
+      };
+
+      if( tma ) {
+         if( tid == 0 ) {
+            fence_proxy_async();                      // earlier generic writes to the stages first
+            issue( 0 );
+            if( S > 1 ) { issue( 1 ); }
+         }
+      } else {
+         copy( 0 );
+         if( S > 1 ) { copy( 1 ); }
       }
 
       int const nsteps = max( S, J + D );
@@ -415,15 +478,21 @@ __global__ void __launch_bounds__( kM2NT, 2 ) march2d_kernel( M2Args const __gri
          if( s < S ) {
             // ---- wait for the step's rows (a give-up is reported and ends the CTA's work at the
             // next barrier; no later copy is issued)
-            if( !*abort_flag && !mbar_wait( &full[ st ], uses[ st ] & 1u, wait_limit )) {
+            uint32_t const use = tma ? ( st ? uses1 : uses0 ) : ( st ? cuses1 : cuses0 );
+            if( !*abort_flag && !mbar_wait( &full[ tma ? st : 2 + st ], use & 1u, wait_limit )) {
                *abort_flag = 1;
                atomicExch( a.status, DIPCU_ERR_TIMEOUT );
             }
-            ++uses[ st ];
-            int const rs = misc[ 4 + st ];             // the stage's row stride (samples)
-            bool const interior = misc[ 6 + st ] != 0;
+            if( tma ) {
+               if( st ) { ++uses1; } else { ++uses0; }
+            } else {
+               if( st ) { ++cuses1; } else { ++cuses0; }
+            }
+            int const rs = tma ? misc[ 4 + st ] : bw;     // the stage's row stride (samples)
+            bool const interior = tma && misc[ 6 + st ] != 0;
             int const r0s = misc[ 8 + st ];
             if( nfix > 0 ) {
+               if( !tma ) { __syncthreads(); }          // every warp's row table of this stage
                // Halo columns outside the image: their source column's sample (sign included).
                for( int e = tid; e < nfix * R; e += NT ) {
                   M2Fix const f = fix[ e % nfix ];
@@ -482,39 +551,51 @@ __global__ void __launch_bounds__( kM2NT, 2 ) march2d_kernel( M2Args const __gri
          __syncthreads();
          if( *abort_flag ) { break; }
          // ---- stage st is free: stream step s + 2 into it
-         if( tid == 0 && s + 2 < S ) {
-            fence_proxy_async();                      // the column fixes' writes before the copy's
-            issue( s + 2 );
+         if( s + 2 < S ) {
+            if( !tma ) {
+               copy( s + 2 );
+            } else if( tid == 0 ) {
+               fence_proxy_async();                   // the column fixes' writes before the copy's
+               issue( s + 2 );
+            }
          }
          // ---- y phase: block j = s - D (output rows ya + jR ..), thread -> column, RT rows
          int const j = s - D;
          if( j >= 0 && j < J ) {
             constexpr int RT = kM2RT;
-            int const c = tid & ( TX - 1 );
-            int const g = tid >> 7;                      // row half
+            int const cp = tid & ( TX / 2 - 1 );          // column pair
+            int const g = tid >> 6;                      // row group
             int const t0 = j * R + RT * g;               // item output row offset of the thread's first row
-            float acc[ RT ];
+            float2 acc[ RT ];
 #pragma unroll
-            for( int t = 0; t < RT; ++t ) { acc[ t ] = 0.f; }
+            for( int t = 0; t < RT; ++t ) { acc[ t ] = make_float2( 0.f, 0.f ); }
             // Output row t0 + t needs item input rows t0 + t + k, k in [0, 2 hy].
             int const nlast = RT - 1 + ( 2 * hy + 1 - 8 * ( nyb - 1 ));   // rows the last tap block reads
             switch( nyb ) {
-               case 1: m2_yphase< 1 >( ring, wy, c, t0, nlast, acc ); break;
-               case 2: m2_yphase< 2 >( ring, wy, c, t0, nlast, acc ); break;
-               case 3: m2_yphase< 3 >( ring, wy, c, t0, nlast, acc ); break;
-               case 4: m2_yphase< 4 >( ring, wy, c, t0, nlast, acc ); break;
-               case 5: m2_yphase< 5 >( ring, wy, c, t0, nlast, acc ); break;
-               case 6: m2_yphase< 6 >( ring, wy, c, t0, nlast, acc ); break;
-               case 7: m2_yphase< 7 >( ring, wy, c, t0, nlast, acc ); break;
-               case 8: m2_yphase< 8 >( ring, wy, c, t0, nlast, acc ); break;
-               default: m2_yphase< 9 >( ring, wy, c, t0, nlast, acc ); break;
+               case 1: m2_yphase< 1 >( ring, wy2, cp, t0, nlast, acc ); break;
+               case 2: m2_yphase< 2 >( ring, wy2, cp, t0, nlast, acc ); break;
+               case 3: m2_yphase< 3 >( ring, wy2, cp, t0, nlast, acc ); break;
+               case 4: m2_yphase< 4 >( ring, wy2, cp, t0, nlast, acc ); break;
+               case 5: m2_yphase< 5 >( ring, wy2, cp, t0, nlast, acc ); break;
+               case 6: m2_yphase< 6 >( ring, wy2, cp, t0, nlast, acc ); break;
+               case 7: m2_yphase< 7 >( ring, wy2, cp, t0, nlast, acc ); break;
+               case 8: m2_yphase< 8 >( ring, wy2, cp, t0, nlast, acc ); break;
+               default: m2_yphase< 9 >( ring, wy2, cp, t0, nlast, acc ); break;
             }
-            int const xo = x0 + c;
+            int const xo = x0 + 2 * cp;
             if( xo < nx ) {
+               bool const both = xo + 1 < nx;
                float* p = im.dst + static_cast< int64_t >( b ) * im.dsb + static_cast< int64_t >( ya + t0 ) * im.ds1 + xo;
 #pragma unroll
                for( int t = 0; t < RT; ++t ) {
-                  if( ya + t0 + t < yb ) { p[ 0 ] = acc[ t ]; }
+                  if( ya + t0 + t < yb ) {
+                     if( both && im.vec_out ) {
+                        *reinterpret_cast< float2* >( p ) = acc[ t ];
+                     } else {
+                        p[ 0 ] = acc[ t ].x;
+                        if( both ) { p[ 1 ] = acc[ t ].y; }
+                     }
+                  }
                   p += im.ds1;
                }
             }
@@ -523,10 +604,10 @@ __global__ void __launch_bounds__( kM2NT, 2 ) march2d_kernel( M2Args const __gri
       if( *abort_flag ) {
          // Before the CTA ends: the copies it announced and did not consume land first (bounded
          // waits again; a copy that never comes is given up on like the first).
+         asm volatile( "cp.async.wait_all;" ::: "memory" );
          if( tid == 0 ) {
-            for( int st = 0; st < 2; ++st ) {
-               for( ; uses[ st ] < issued[ st ]; ++uses[ st ] ) { mbar_wait( &full[ st ], uses[ st ] & 1u, wait_limit ); }
-            }
+            for( ; uses0 < issued0; ++uses0 ) { mbar_wait( &full[ 0 ], uses0 & 1u, wait_limit ); }
+            for( ; uses1 < issued1; ++uses1 ) { mbar_wait( &full[ 1 ], uses1 & 1u, wait_limit ); }
          }
          __syncthreads();
          break;

@@ -19,6 +19,7 @@ import torch
 from . import _abi
 
 __all__ = ["Error", "ParameterError", "RunTimeError", "Gauss", "GaussFIR", "Derivative", "BestGaussMethod",
+           "SeparableConvolution", "Uniform", "OneDimensionalFilter",
            "BoundaryConditionFromString", "image_desc", "flex_dtype"]
 
 
@@ -201,6 +202,96 @@ def GaussFIR(in_, sigmas: Iterable[float] | float = (1.0,), derivativeOrder: Ite
     else:
         with torch.cuda.device(x.device):
             check(_abi.lib().dipcu_gauss_fir(*args, ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+    if target is not None:
+        target.copy_(res)
+        res = target
+    return _to_host(res) if was_numpy else res
+
+
+def _prepare_out(x: torch.Tensor, out):
+    """(result tensor, tensor to copy it into afterwards or None) for an optional `out`, with
+    DIPlib's rules: the output's type is kept when given (protected output), and an output sharing
+    memory with the input gets a fresh buffer first."""
+    if out is None:
+        return torch.empty(x.shape, dtype=flex_dtype(x.dtype), device=x.device), None
+    if not isinstance(out, torch.Tensor) or out.device != x.device:
+        raise ParameterError("out must be a tensor on the input's device")
+    if tuple(out.shape) != tuple(x.shape):
+        raise ParameterError("Sizes don't match")
+    if _shares_memory(out, x):
+        return torch.empty(out.shape, dtype=out.dtype, device=out.device), out
+    return out, None
+
+
+def _run(x: torch.Tensor, fn, *args) -> None:
+    if x.device.index == torch.cuda.current_device():
+        check(fn(*args, ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+    else:
+        with torch.cuda.device(x.device):
+            check(fn(*args, ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+
+
+class OneDimensionalFilter:
+    """dip::OneDimensionalFilter (include/diplib/linear.h:84-92): real `filter` weights, `origin`
+    (-1: the centre) and `symmetry` ("general", "even", "odd", "conj", "d-even", "d-odd", "d-conj")."""
+
+    def __init__(self, filter=(), origin: int = -1, symmetry: str = "general", isComplex: bool = False):
+        self.filter = [float(v) for v in filter]
+        self.origin = int(origin)
+        self.symmetry = symmetry
+        self.isComplex = bool(isComplex)
+
+
+def SeparableConvolution(in_, filter, boundaryCondition=(), process=(), *, out=None):
+    """dip::SeparableConvolution (include/diplib/linear.h:114-129, src/linear/convolution.cpp:319-421)
+    for real filters: `filter` is one OneDimensionalFilter (or a dict with the same keys) used along
+    every axis, or one per axis (DIPlib order, x first); `process` (optional) one flag per axis."""
+    x, was_numpy = _to_device(in_)
+    nd = max(1, x.dim())
+    filters = filter if isinstance(filter, (list, tuple)) else [filter]
+    filters = [OneDimensionalFilter(**f) if isinstance(f, dict) else f for f in filters]
+    if len(filters) not in (1, nd):
+        raise ParameterError("Array parameter has the wrong number of elements")
+    if any(f.isComplex for f in filters):
+        raise NotImplementedError("complex filters are outside the B200 real-valued path")
+    syms = []
+    for f in filters:
+        if f.symmetry not in _abi.SYMMETRY:
+            raise ParameterError("Symmetry string not recognized: " + f.symmetry)
+        syms.append(_abi.SYMMETRY[f.symmetry])
+    bcs = [BoundaryConditionFromString(b) for b in _array_use_parameter(boundaryCondition, nd, "")]
+    proc = list(process) if process else []
+    if proc and len(proc) != nd:
+        raise ParameterError("Array parameter has the wrong number of elements")
+    weights = [(ctypes.c_double * max(1, len(f.filter)))(*f.filter) for f in filters]
+    descs = (_abi.Filter1D * len(filters))(*[
+        _abi.Filter1D(ctypes.cast(w, ctypes.POINTER(ctypes.c_double)), len(f.filter), f.origin, sy)
+        for w, f, sy in zip(weights, filters, syms)])
+    res, target = _prepare_out(x, out)
+    din, dout = image_desc(x), image_desc(res)
+    pr = (ctypes.c_uint8 * nd)(*[1 if p_ else 0 for p_ in proc]) if proc else None
+    _run(x, _abi.lib().dipcu_separable_convolution, ctypes.byref(din), ctypes.byref(dout), descs, len(filters),
+         (ctypes.c_int32 * nd)(*bcs), pr)
+    if target is not None:
+        target.copy_(res)
+        res = target
+    return _to_host(res) if was_numpy else res
+
+
+def Uniform(in_, kernel=7, boundaryCondition=(), *, shape: str = "rectangular", out=None):
+    """dip::Uniform (include/diplib/linear.h:262-275, src/linear/uniform.cpp:147-163) with a
+    rectangular kernel: `kernel` holds the per-axis sizes (a scalar broadcasts; DIPlib order).  Other
+    kernel shapes (the pixel-table path) are outside this implementation."""
+    if shape != "rectangular":
+        raise NotImplementedError("only rectangular uniform kernels are implemented on the B200 path")
+    x, was_numpy = _to_device(in_)
+    nd = max(1, x.dim())
+    sizes = [float(v) for v in _array_use_parameter(kernel, nd, 7.0)]
+    bcs = [BoundaryConditionFromString(b) for b in _array_use_parameter(boundaryCondition, nd, "")]
+    res, target = _prepare_out(x, out)
+    din, dout = image_desc(x), image_desc(res)
+    _run(x, _abi.lib().dipcu_uniform, ctypes.byref(din), ctypes.byref(dout), (ctypes.c_double * nd)(*sizes),
+         (ctypes.c_int32 * nd)(*bcs))
     if target is not None:
         target.copy_(res)
         res = target

@@ -99,6 +99,42 @@ int dipcu_gauss_fir_noalloc( dipcu_image_desc const* in, dipcu_image_desc const*
                              double const* sigmas, uint32_t const* orders, int32_t const* bcs,
                              double truncation, void* stream );
 
+/* ---- Other separable filters -------------------------------------------------------------- */
+
+/* A real 1D filter as dip::OneDimensionalFilter holds it (include/diplib/linear.h:84-92 in DIPlib):
+ * `size` weights (HOST memory), the origin (-1: the centre), and the symmetry: DIPCU_SYM_GENERAL
+ * ("general" or ""), _EVEN ("even", and "conj" for a real filter: `weights` is the left half
+ * with the centre last), _ODD ("odd"), _D_EVEN ("d-even", "d-conj"), _D_ODD ("d-odd"). */
+typedef enum {
+   DIPCU_SYM_GENERAL = 0, DIPCU_SYM_EVEN = 1, DIPCU_SYM_ODD = 2, DIPCU_SYM_D_EVEN = 3, DIPCU_SYM_D_ODD = 4
+} dipcu_symmetry;
+
+typedef struct {
+   double const* weights;
+   int64_t size;
+   int64_t origin;
+   int32_t symmetry;                  /* dipcu_symmetry */
+} dipcu_filter_1d;
+
+/* dip::SeparableConvolution for real filters (src/linear/convolution.cpp:319-421 in DIPlib):
+ * `nfilters` is 1 (the filter is used along every axis) or in->ndims; `bcs` has ndims entries;
+ * `process` (optional, ndims flags) selects the axes.  Output and computation types as
+ * dipcu_gauss_fir (dip::DataType::SuggestFlex; another `out` type is the protected-output path).
+ * An axis of size 1, or whose filter is empty or a single unit weight, is not filtered.  Filters up
+ * to 256 weights after the symmetry's expansion (DIPCU_ERR_KERNEL_TOO_LARGE beyond).  Errors:
+ * "Symmetry string not recognized" and "Origin outside of filter" (DIPCU_ERR_INVALID_ARG), as the
+ * reference.  Intermediates of the pass chain are stream-ordered allocations. */
+int dipcu_separable_convolution( dipcu_image_desc const* in, dipcu_image_desc const* out, dipcu_filter_1d const* filters,
+                                 int nfilters, int32_t const* bcs, uint8_t const* process, void* stream );
+
+/* dip::Uniform with a rectangular kernel (src/linear/uniform.cpp:68-86, 147-163 in DIPlib): `sizes`
+ * holds the kernel's per-axis sizes (ndims values; a size above 1 is truncated to an integer, as
+ * dip::Kernel::Sizes does, others leave the axis unfiltered); the mean over the window
+ * [i - size/2, i + (size+1)/2) of the boundary-extended line, computed as the reference's running
+ * sum (same operation order).  Types as dipcu_gauss_fir. */
+int dipcu_uniform( dipcu_image_desc const* in, dipcu_image_desc const* out, double const* sizes, int32_t const* bcs,
+                   void* stream );
+
 /* ---- Backward (adjoint) ------------------------------------------------------------------- */
 
 /* Gradients of dipcu_gauss_fir (no DIPlib counterpart; DIPlib has no derivatives of its filters).

@@ -182,6 +182,62 @@ def gauss_fir(x: np.ndarray, sigmas: Sequence[float] = (1.0,), orders: Sequence[
     return out
 
 
+SYMMETRIES = {"": 0, "general": 0, "even": 1, "odd": 2, "conj": 1, "d-even": 3, "d-odd": 4, "d-conj": 3}
+
+
+def _filter_arrays(filters):
+    """(data pointers, lens, origins, symmetry codes, symmetry strings, keep-alive) of filters given as
+    dicts {"filter": values, "origin": int (-1 centre), "symmetry": str} (dip::OneDimensionalFilter)."""
+    n = len(filters)
+    arrs = [np.ascontiguousarray(np.asarray(f["filter"], dtype=np.float64)) for f in filters]
+    data = (ctypes.c_void_p * n)(*[a.ctypes.data for a in arrs])
+    lens = (ctypes.c_int * n)(*[a.size for a in arrs])
+    origins = (ctypes.c_long * n)(*[int(f.get("origin", -1)) for f in filters])
+    syms = [str(f.get("symmetry", "general")) for f in filters]
+    codes = (ctypes.c_int * n)(*[SYMMETRIES[s_] for s_ in syms])
+    return data, lens, origins, codes, syms, arrs
+
+
+def separable_convolution(x: np.ndarray, filters, bcs: Sequence[str] = (), process=None, out_dtype=None) -> np.ndarray:
+    """The restated dip::SeparableConvolution (real filters) on a numpy array."""
+    nd = x.ndim
+    if len(filters) not in (1, nd):
+        raise ValueError("Array parameter has the wrong number of elements")
+    bcl = _broadcast(bcs, nd, "mirror")
+    out_dt = suggest_flex(x.dtype) if out_dtype is None else np.dtype(out_dtype)
+    out = np.zeros(x.shape, out_dt)
+    sizes, in_strides = _dip_geometry(x)
+    _, out_strides = _dip_geometry(out)
+    data, lens, origins, codes, _, keep = _filter_arrays(filters)
+    proc = None if process is None else (ctypes.c_int * nd)(*[int(bool(p)) for p in process])
+    lib = oracle_lib()
+    st = lib.or_separable_convolution(
+        ctypes.c_void_p(x.ctypes.data), DTYPE_CODES[x.dtype], nd, sizes, in_strides,
+        ctypes.c_void_p(out.ctypes.data), DTYPE_CODES[out_dt], out_strides, len(filters), data, lens, origins, codes,
+        (ctypes.c_int * nd)(*[bc_code(b) for b in bcl]), proc)
+    if st != 0:
+        raise RuntimeError(f"or_separable_convolution failed ({st})")
+    return out
+
+
+def uniform(x: np.ndarray, sizes, bcs: Sequence[str] = (), out_dtype=None) -> np.ndarray:
+    """The restated dip::Uniform with a rectangular kernel of per-axis `sizes` (DIPlib order)."""
+    nd = x.ndim
+    fs = _broadcast(sizes, nd, 7)
+    bcl = _broadcast(bcs, nd, "mirror")
+    out_dt = suggest_flex(x.dtype) if out_dtype is None else np.dtype(out_dtype)
+    out = np.zeros(x.shape, out_dt)
+    isz, in_strides = _dip_geometry(x)
+    _, out_strides = _dip_geometry(out)
+    st = oracle_lib().or_uniform_rect(
+        ctypes.c_void_p(x.ctypes.data), DTYPE_CODES[x.dtype], nd, isz, in_strides,
+        ctypes.c_void_p(out.ctypes.data), DTYPE_CODES[out_dt], out_strides,
+        (ctypes.c_int64 * nd)(*[int(f) for f in fs]), (ctypes.c_int * nd)(*[bc_code(b) for b in bcl]))
+    if st != 0:
+        raise RuntimeError(f"or_uniform_rect failed ({st})")
+    return out
+
+
 def separable_fir(x: np.ndarray, taps, odd, bcs, out_dtype=None) -> np.ndarray:
     """The restated dip::SeparableConvolution with given EVEN/ODD half kernels, centre tap first
     (per axis, DIPlib order; None leaves an axis unfiltered)."""
@@ -334,6 +390,41 @@ def ref_gauss(x: np.ndarray, sigmas: Sequence[float] = (1.0,), orders: Sequence[
         raise RuntimeError(errbuf.value.decode())
     if not protect and code.value != DTYPE_CODES[res_dt]:
         raise RuntimeError(f"unexpected output type code {code.value}")
+    return out
+
+
+def ref_separable_convolution(x: np.ndarray, filters, bcs: Sequence[str] | None = None, process=None) -> np.ndarray:
+    """dip::SeparableConvolution of the reference (real filters given as dicts, see
+    separable_convolution)."""
+    nd = x.ndim
+    sizes, st = _dip_geometry(x)
+    out = np.zeros(x.shape, suggest_flex(x.dtype))
+    code = ctypes.c_int(0)
+    errbuf = ctypes.create_string_buffer(512)
+    data, lens, origins, _, syms, keep = _filter_arrays(filters)
+    proc = None if process is None else (ctypes.c_int * nd)(*[int(bool(p)) for p in process])
+    rc = ref_lib().dipref_separable_convolution(
+        ctypes.c_void_p(x.ctypes.data), DTYPE_CODES[x.dtype], nd, sizes, st, len(filters), data, lens, origins,
+        "\n".join(syms).encode(), "\n".join(bcs or []).encode(), int(bool(bcs)), proc, ctypes.c_void_p(out.ctypes.data),
+        ctypes.byref(code), errbuf, 512)
+    if rc != 0:
+        raise RuntimeError(errbuf.value.decode())
+    return out
+
+
+def ref_uniform(x: np.ndarray, sizes, bcs: Sequence[str] | None = None) -> np.ndarray:
+    """dip::Uniform of the reference with a rectangular kernel of per-axis `sizes`."""
+    nd = x.ndim
+    isz, st = _dip_geometry(x)
+    out = np.zeros(x.shape, suggest_flex(x.dtype))
+    code = ctypes.c_int(0)
+    errbuf = ctypes.create_string_buffer(512)
+    fs = _broadcast(sizes, nd, 7)
+    rc = ref_lib().dipref_uniform(
+        ctypes.c_void_p(x.ctypes.data), DTYPE_CODES[x.dtype], nd, isz, st, (ctypes.c_double * nd)(*[float(f) for f in fs]),
+        "\n".join(bcs or []).encode(), int(bool(bcs)), ctypes.c_void_p(out.ctypes.data), ctypes.byref(code), errbuf, 512)
+    if rc != 0:
+        raise RuntimeError(errbuf.value.decode())
     return out
 
 

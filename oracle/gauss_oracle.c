@@ -434,6 +434,7 @@ static void line_filter_f64( double const* in, double* out, size_t length, doubl
 /* ------------------------------------------------------------------------------------------ */
 
 #define OR_MAX_DIMS 16
+#define OR_MAX_FILTER 4096
 
 /* dip::SeparableConvolution (src/linear/convolution.cpp:319-421) for real EVEN / ODD filters given as
  * half kernels with the centre FIRST (the reversed storage of InternOneDimensionalFilter), driven by
@@ -587,4 +588,250 @@ int or_gauss_fir( void const* in, int in_dtype, int ndims, int64_t const* sizes,
 done:
    for( int d = 0; d < ndims; ++d ) { free( taps[ d ] ); }
    return status;
+}
+
+
+/* ------------------------------------------------------------------------------------------ */
+/* General real filters and the rectangular uniform filter (next to the Gaussian path):        */
+/* dip::SeparableConvolution with dip::OneDimensionalFilter of any symmetry                    */
+/* (src/linear/convolution.cpp:67-162 interning, :175-302 line filter, :319-421 driver) and    */
+/* dip::Uniform with a rectangular kernel (src/linear/uniform.cpp:33-86).                      */
+/* ------------------------------------------------------------------------------------------ */
+
+/* One real filter as InternOneDimensionalFilter keeps it: f = the data reversed, `size` the full
+ * length (symmetry expanded), `origin` the reversed origin. */
+typedef struct {
+   double f[ OR_MAX_FILTER ];
+   size_t dataSize, size, origin;
+   int symmetry;
+} or_ifilter;
+
+static int intern_filter( double const* data, size_t n, long origin, int symmetry, or_ifilter* out ) {
+   if( n > OR_MAX_FILTER ) { return OR_ERR_ARG; }
+   out->dataSize = n;
+   out->size = n;
+   out->symmetry = symmetry;
+   if( n == 0 ) { out->origin = 0; return OR_OK; }
+   switch( symmetry ) {
+      case OR_SYM_GENERAL: break;
+      case OR_SYM_EVEN: case OR_SYM_ODD: out->size = 2 * n - 1; break;
+      case OR_SYM_D_EVEN: case OR_SYM_D_ODD: out->size = 2 * n; break;
+      default: return OR_ERR_ARG;
+   }
+   size_t o = origin < 0 ? out->size / 2 : (size_t)origin;
+   if( o >= out->size ) { return OR_ERR_ARG; }
+   for( size_t i = 0; i < n; ++i ) { out->f[ i ] = data[ n - 1 - i ]; }    /* CopyReverseData */
+   out->origin = out->size - o - 1;
+   return OR_OK;
+}
+
+/* The line filter of convolution.cpp:184-302 for real data; `in` is the first sample of the line
+ * (the buffer is extended by the border on both sides). */
+#define DEFINE_GENERAL_LINE( SUFFIX, T )                                                              \
+static void general_line_##SUFFIX( T const* in, T* out, size_t length, or_ifilter const* F, T const* f ) { \
+   size_t const ds = F->dataSize;                                                                        \
+   in -= F->origin;                                                                                      \
+   switch( F->symmetry ) {                                                                               \
+      case OR_SYM_GENERAL:                                                                               \
+         for( size_t ii = 0; ii < length; ++ii, ++in ) {                                                 \
+            T sum = 0;                                                                                   \
+            for( size_t k = 0; k < ds; ++k ) { sum += f[ k ] * in[ k ]; }                                \
+            out[ ii ] = sum;                                                                             \
+         }                                                                                               \
+         break;                                                                                          \
+      case OR_SYM_EVEN: case OR_SYM_ODD: {                                                               \
+         int const odd = F->symmetry == OR_SYM_ODD;                                                      \
+         T const* c = in + ds - 1;                                                                       \
+         for( size_t ii = 0; ii < length; ++ii, ++c ) {                                                  \
+            T sum = f[ 0 ] * c[ 0 ];                                                                     \
+            for( size_t k = 1; k < ds; ++k ) {                                                           \
+               sum += f[ k ] * ( odd ? ( c[ k ] - c[ -(ptrdiff_t)k ] ) : ( c[ k ] + c[ -(ptrdiff_t)k ] )); \
+            }                                                                                            \
+            out[ ii ] = sum;                                                                             \
+         }                                                                                               \
+         break;                                                                                          \
+      }                                                                                                  \
+      default: {   /* D_EVEN, D_ODD */                                                                   \
+         int const odd = F->symmetry == OR_SYM_D_ODD;                                                    \
+         T const* r = in + ds - 1;                                                                       \
+         for( size_t ii = 0; ii < length; ++ii, ++r ) {                                                  \
+            T sum = 0;                                                                                   \
+            for( size_t k = 0; k < ds; ++k ) {                                                           \
+               sum += f[ k ] * ( odd ? ( r[ k ] - r[ -1 - (ptrdiff_t)k ] ) : ( r[ k ] + r[ -1 - (ptrdiff_t)k ] )); \
+            }                                                                                            \
+            out[ ii ] = sum;                                                                             \
+         }                                                                                               \
+         break;                                                                                          \
+      }                                                                                                  \
+   }                                                                                                     \
+}                                                                                                        \
+/* RectangularUniformLineFilter::Filter (uniform.cpp:41-62): a running sum. */                          \
+static void uniform_line_##SUFFIX( T const* in, T* out, size_t length, size_t filterSize ) {             \
+   T const norm = (T)1 / (T)filterSize;                                                                  \
+   T const* left = in - (ptrdiff_t)( filterSize / 2 );                                                   \
+   T const* right = in + (ptrdiff_t)(( filterSize + 1 ) / 2 );                                           \
+   T sum = 0;                                                                                            \
+   for( T const* p = left; p != right; ++p ) { sum += *p; }                                              \
+   out[ 0 ] = sum * norm;                                                                                \
+   for( size_t ii = 1; ii < length; ++ii ) {                                                             \
+      sum -= *left;                                                                                      \
+      sum += *right;                                                                                     \
+      ++left;                                                                                            \
+      ++right;                                                                                           \
+      out[ ii ] = sum * norm;                                                                            \
+   }                                                                                                     \
+}
+
+DEFINE_GENERAL_LINE( f32, float )
+DEFINE_GENERAL_LINE( f64, double )
+
+/* Framework::Separable (framework_separable.cpp:35-431) around a per-axis line filter: kind 0 the
+ * interned filters `F`, kind 1 the rectangular uniform filter of `usize[d]` samples. */
+static int separable_driver( void const* in, int in_dtype, int ndims, int64_t const* sizes, int64_t const* in_strides,
+                             void* out, int out_dtype, int64_t const* out_strides, int const* process_in,
+                             size_t const* border, int const* bcs, int kind, or_ifilter const* const* F,
+                             size_t const* usize ) {
+   if( ndims < 1 || ndims > OR_MAX_DIMS || dtype_size( in_dtype ) == 0 || dtype_size( out_dtype ) == 0 ) {
+      return OR_ERR_ARG;
+   }
+   int buf_type = or_suggest_flex( in_dtype );
+   int buf_double = ( buf_type == OR_DFLOAT );
+   int process[ OR_MAX_DIMS ];
+   size_t npix = 1;
+   for( int d = 0; d < ndims; ++d ) {
+      npix *= (size_t)sizes[ d ];
+      process[ d ] = process_in[ d ] && sizes[ d ] > 1;
+      if( process[ d ] && ( bcs[ d ] < 0 || bcs[ d ] >= OR_BC_ALREADY_EXPANDED )) { return OR_ERR_BC; }
+   }
+   int order[ OR_MAX_DIMS ];
+   int nproc = 0;
+   for( int d = 0; d < ndims; ++d ) {
+      if( process[ d ] ) { order[ nproc++ ] = d; }
+   }
+   for( int ii = 1; ii < nproc; ++ii ) {
+      int elem = order[ ii ];
+      int jj = ii;
+      while( jj > 0 && in_strides[ order[ jj - 1 ] ] > in_strides[ elem ] ) {
+         order[ jj ] = order[ jj - 1 ];
+         --jj;
+      }
+      order[ jj ] = elem;
+   }
+   if( nproc == 0 ) {
+      int64_t coord[ OR_MAX_DIMS ] = { 0 };
+      for( size_t p = 0; p < npix; ++p ) {
+         ptrdiff_t io = 0, oo = 0;
+         for( int d = 0; d < ndims; ++d ) { io += coord[ d ] * in_strides[ d ]; oo += coord[ d ] * out_strides[ d ]; }
+         put_sample( out, out_dtype, oo, get_sample( in, in_dtype, io ));
+         for( int d = 0; d < ndims; ++d ) { if( ++coord[ d ] < sizes[ d ] ) { break; } coord[ d ] = 0; }
+      }
+      return OR_OK;
+   }
+   int use_intermediate = ( out_dtype != buf_type );
+   void* inter = NULL;
+   int64_t inter_strides[ OR_MAX_DIMS ];
+   if( use_intermediate ) {
+      inter = malloc( npix * dtype_size( buf_type ));
+      int64_t s = 1;
+      for( int d = 0; d < ndims; ++d ) { inter_strides[ d ] = s; s *= sizes[ d ]; }
+   }
+   size_t maxlen = 0, maxb = 0;
+   for( int ii = 0; ii < nproc; ++ii ) {
+      if( (size_t)sizes[ order[ ii ] ] > maxlen ) { maxlen = (size_t)sizes[ order[ ii ] ]; }
+      if( border[ order[ ii ] ] > maxb ) { maxb = border[ order[ ii ] ]; }
+   }
+   size_t esz = buf_double ? 8 : 4;
+   char* inbuf = (char*)malloc( esz * ( maxlen + 2 * maxb ));
+   char* outbuf = (char*)malloc( esz * maxlen );
+   void const* src = in;
+   int src_type = in_dtype;
+   int64_t const* src_strides = in_strides;
+   for( int rep = 0; rep < nproc; ++rep ) {
+      int pd = order[ rep ];
+      int last = ( rep == nproc - 1 );
+      void* dst = ( last || !use_intermediate ) ? out : inter;
+      int dst_type = ( last || !use_intermediate ) ? out_dtype : buf_type;
+      int64_t const* dst_strides = ( last || !use_intermediate ) ? out_strides : inter_strides;
+      size_t n = (size_t)sizes[ pd ];
+      size_t b = border[ pd ];
+      size_t nlines = npix / n;
+      float ff[ OR_MAX_FILTER ];
+      if( kind == 0 ) { for( size_t k = 0; k < F[ pd ]->dataSize; ++k ) { ff[ k ] = (float)F[ pd ]->f[ k ]; } }
+      int64_t coord[ OR_MAX_DIMS ] = { 0 };
+      for( size_t line = 0; line < nlines; ++line ) {
+         ptrdiff_t so = 0, dof = 0;
+         for( int d = 0; d < ndims; ++d ) { so += coord[ d ] * src_strides[ d ]; dof += coord[ d ] * dst_strides[ d ]; }
+         if( buf_double ) {
+            double* bb = (double*)inbuf + b;
+            double* o = (double*)outbuf;
+            for( size_t i = 0; i < n; ++i ) { bb[ i ] = get_sample( src, src_type, so + (ptrdiff_t)i * src_strides[ pd ] ); }
+            or_expand_buffer_f64( bb, 1, n, b, b, bcs[ pd ] );
+            if( kind == 0 ) { general_line_f64( bb, o, n, F[ pd ], F[ pd ]->f ); } else { uniform_line_f64( bb, o, n, usize[ pd ] ); }
+            for( size_t i = 0; i < n; ++i ) { put_sample( dst, dst_type, dof + (ptrdiff_t)i * dst_strides[ pd ], o[ i ] ); }
+         } else {
+            float* bb = (float*)inbuf + b;
+            float* o = (float*)outbuf;
+            for( size_t i = 0; i < n; ++i ) { bb[ i ] = (float)get_sample( src, src_type, so + (ptrdiff_t)i * src_strides[ pd ] ); }
+            or_expand_buffer_f32( bb, 1, n, b, b, bcs[ pd ] );
+            if( kind == 0 ) { general_line_f32( bb, o, n, F[ pd ], ff ); } else { uniform_line_f32( bb, o, n, usize[ pd ] ); }
+            for( size_t i = 0; i < n; ++i ) { put_sample( dst, dst_type, dof + (ptrdiff_t)i * dst_strides[ pd ], (double)o[ i ] ); }
+         }
+         for( int d = 0; d < ndims; ++d ) {
+            if( d == pd ) { continue; }
+            if( ++coord[ d ] < sizes[ d ] ) { break; }
+            coord[ d ] = 0;
+         }
+      }
+      src = dst;
+      src_type = dst_type;
+      src_strides = dst_strides;
+   }
+   free( inbuf );
+   free( outbuf );
+   free( inter );
+   return OR_OK;
+}
+
+int or_separable_convolution( void const* in, int in_dtype, int ndims, int64_t const* sizes, int64_t const* in_strides,
+                              void* out, int out_dtype, int64_t const* out_strides, int nfilters,
+                              double const* const* data, int const* lens, long const* origins, int const* symmetries,
+                              int const* bcs, int const* process ) {
+   if( ndims < 1 || ndims > OR_MAX_DIMS || ( nfilters != 1 && nfilters != ndims )) { return OR_ERR_ARG; }
+   or_ifilter* fs = (or_ifilter*)calloc( (size_t)nfilters, sizeof( or_ifilter ));
+   or_ifilter const* F[ OR_MAX_DIMS ];
+   size_t border[ OR_MAX_DIMS ];
+   int proc[ OR_MAX_DIMS ];
+   int st = OR_OK;
+   for( int i = 0; i < nfilters && st == OR_OK; ++i ) {
+      st = intern_filter( data[ i ], (size_t)lens[ i ], origins[ i ], symmetries[ i ], &fs[ i ] );
+   }
+   if( st != OR_OK ) { free( fs ); return st; }
+   for( int d = 0; d < ndims; ++d ) {
+      or_ifilter const* f = &fs[ nfilters == 1 ? 0 : d ];
+      F[ d ] = f;
+      size_t b = f->origin;
+      border[ d ] = f->size == 0 ? 0 : ( b > f->size - b - 1 ? b : f->size - b - 1 );
+      proc[ d ] = process ? process[ d ] : 1;
+      /* IsMeaninglessFilter (convolution.cpp:304-314): size 0, or a single unit tap (compared in the
+       * buffer precision). */
+      int meaningless = f->size == 0 || ( f->size == 1 && ( or_suggest_flex( in_dtype ) == OR_DFLOAT
+                                                            ? f->f[ 0 ] == 1.0 : (float)f->f[ 0 ] == 1.0f ));
+      if( meaningless ) { proc[ d ] = 0; }
+   }
+   st = separable_driver( in, in_dtype, ndims, sizes, in_strides, out, out_dtype, out_strides, proc, border, bcs, 0, F, NULL );
+   free( fs );
+   return st;
+}
+
+int or_uniform_rect( void const* in, int in_dtype, int ndims, int64_t const* sizes, int64_t const* in_strides,
+                     void* out, int out_dtype, int64_t const* out_strides, int64_t const* filter_sizes, int const* bcs ) {
+   if( ndims < 1 || ndims > OR_MAX_DIMS ) { return OR_ERR_ARG; }
+   int proc[ OR_MAX_DIMS ];
+   size_t border[ OR_MAX_DIMS ], usize[ OR_MAX_DIMS ];
+   for( int d = 0; d < ndims; ++d ) {
+      proc[ d ] = filter_sizes[ d ] > 1 && sizes[ d ] > 1;
+      usize[ d ] = proc[ d ] ? (size_t)filter_sizes[ d ] : 1;
+      border[ d ] = proc[ d ] ? usize[ d ] / 2 : 0;
+   }
+   return separable_driver( in, in_dtype, ndims, sizes, in_strides, out, out_dtype, out_strides, proc, border, bcs, 1, NULL, usize );
 }

@@ -67,6 +67,23 @@ int or_separable_fir( void const* in, int in_dtype, int ndims, int64_t const* si
                       void* out, int out_dtype, int64_t const* out_strides,
                       double const* const* taps, int const* lens, int const* odd, int const* bcs );
 
+/* Filter symmetry (dip::OneDimensionalFilter::symmetry: "general", "even", "odd", "d-even",
+ * "d-odd"; "conj" and "d-conj" are "even" and "d-even" for real filters). */
+enum { OR_SYM_GENERAL = 0, OR_SYM_EVEN = 1, OR_SYM_ODD = 2, OR_SYM_D_EVEN = 3, OR_SYM_D_ODD = 4 };
+
+/* dip::SeparableConvolution (src/linear/convolution.cpp:319-421) with real filters as given to
+ * DIPlib: per filter the data (lens[i] values, up to 4096), origin (-1: centre) and symmetry;
+ * `nfilters` 1 (used on every axis) or ndims.  `process` (NULL: all axes). */
+int or_separable_convolution( void const* in, int in_dtype, int ndims, int64_t const* sizes, int64_t const* in_strides,
+                              void* out, int out_dtype, int64_t const* out_strides, int nfilters,
+                              double const* const* data, int const* lens, long const* origins, int const* symmetries,
+                              int const* bcs, int const* process );
+
+/* dip::Uniform with a rectangular kernel (src/linear/uniform.cpp:33-86): per-axis filter sizes
+ * (axes with size <= 1 unfiltered), running-sum line filter. */
+int or_uniform_rect( void const* in, int in_dtype, int ndims, int64_t const* sizes, int64_t const* in_strides,
+                     void* out, int out_dtype, int64_t const* out_strides, int64_t const* filter_sizes, int const* bcs );
+
 /* Output/compute type rule: DataType::SuggestFlex, src/library/datatype.cpp:109-124. */
 int or_suggest_flex( int dtype );
 

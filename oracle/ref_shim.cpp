@@ -8,6 +8,7 @@
 //   dip::MakeHalfGaussian    src/linear/gauss.cpp:151-165
 //   dip::detail::ExpandBuffer src/library/copy_buffer.cpp:751-813
 //   dip::ReadPixelWithBoundaryCondition src/library/boundary.cpp:47-128
+//   dip::SeparableConvolution src/linear/convolution.cpp:319-421, dip::Uniform src/linear/uniform.cpp:147-163
 //
 // Sizes and strides are given in DIPlib order (x first), in samples.  Data type codes are the
 // ones of include/dipcu.h (DIPCU_BIN .. DIPCU_DFLOAT).  Every entry point returns 0 on success
@@ -22,6 +23,7 @@
 #include "diplib/analysis.h"
 #include "diplib/boundary.h"
 #include "diplib/generation.h"
+#include "diplib/kernel.h"
 #include "diplib/library/copy_buffer.h"
 #include "diplib/linear.h"
 #include "diplib/multithreading.h"
@@ -94,6 +96,58 @@ void CopyOut( dip::Image const& img, void* out ) {
 } // namespace
 
 extern "C" {
+
+// dip::SeparableConvolution with real filters: `nfilters` filters, filter i = lens[i] values of
+// `data[i]`, origin origins[i], symmetry string syms (newline-separated); `bcs` as in dipref_gauss;
+// `process` (nullptr: all axes).  The output (the reference's own, normal strides) goes to `out`;
+// its type to *out_dtype.
+int dipref_separable_convolution(
+      void const* in, int in_dtype, int ndims, int64_t const* sizes, int64_t const* strides, int nfilters,
+      double const* const* data, int const* lens, long const* origins, char const* syms,
+      char const* bcs, int has_bcs, int const* process, void* out, int* out_dtype, char* err, int errlen ) {
+   try {
+      dip::Image img = Wrap( in, in_dtype, ndims, sizes, strides );
+      dip::StringArray sy = SplitList( syms, true );
+      dip::OneDimensionalFilterArray fa( static_cast< dip::uint >( nfilters ));
+      for( int ii = 0; ii < nfilters; ++ii ) {
+         fa[ ii ].filter.assign( data[ ii ], data[ ii ] + lens[ ii ] );
+         fa[ ii ].origin = origins[ ii ];
+         fa[ ii ].symmetry = sy[ static_cast< dip::uint >( ii ) ];
+      }
+      dip::BooleanArray pr;
+      if( process ) {
+         pr.resize( static_cast< dip::uint >( ndims ));
+         for( int ii = 0; ii < ndims; ++ii ) { pr[ ii ] = process[ ii ] != 0; }
+      }
+      dip::Image res;
+      dip::SeparableConvolution( img, res, fa, SplitList( bcs, has_bcs != 0 ), pr );
+      *out_dtype = TypeToCode( res.DataType() );
+      CopyOut( res, out );
+      return 0;
+   } catch( dip::Error const& e ) {
+      SetErr( err, errlen, e.what() );
+      return 1;
+   }
+}
+
+// dip::Uniform with a rectangular kernel of per-axis sizes `fsizes` (ndims values).
+int dipref_uniform(
+      void const* in, int in_dtype, int ndims, int64_t const* sizes, int64_t const* strides, double const* fsizes,
+      char const* bcs, int has_bcs, void* out, int* out_dtype, char* err, int errlen ) {
+   try {
+      dip::Image img = Wrap( in, in_dtype, ndims, sizes, strides );
+      dip::FloatArray fs( static_cast< dip::uint >( ndims ));
+      for( int ii = 0; ii < ndims; ++ii ) { fs[ ii ] = fsizes[ ii ]; }
+      dip::Image res;
+      dip::Uniform( img, res, dip::Kernel( fs, dip::S::RECTANGULAR ), SplitList( bcs, has_bcs != 0 ));
+      *out_dtype = TypeToCode( res.DataType() );
+      CopyOut( res, out );
+      return 0;
+   } catch( dip::Error const& e ) {
+      SetErr( err, errlen, e.what() );
+      return 1;
+   }
+}
 
 int dipref_set_threads( int n ) {
    dip::SetNumberOfThreads( static_cast< dip::uint >( n < 0 ? 0 : n ));

@@ -54,3 +54,21 @@ def test_batch_axis(cuda):
     ref = oracle.gauss_fir(x, [6.0, 4.0, 0.0], [2, 1, 0], ["periodic", "mirror", "mirror"], 3.0)
     got = dip().GaussFIR(x, [6.0, 4.0, 0.0], [2, 1, 0], ["periodic", "mirror", "mirror"], 3.0)
     assert_close(got, ref, x, "batch axis")
+
+
+@pytest.mark.parametrize("sig,ords,bcs", [((8.0, 8.0), (0, 2), ("mirror", "periodic")),
+                                          ((4.0, 6.0), (1, 0), ("add zeros", "asym mirror")),
+                                          ((2.0, 2.0), (0, 0), ("periodic", "mirror"))])
+def test_rows_tma_cannot_address(cuda, sig, ords, bcs):
+    """Views whose row stride is not a multiple of 16 bytes: the stages are filled by per-thread
+    asynchronous copies instead of TMA."""
+    import torch
+    from tests.test_gauss_gpu import to_dev
+    rng = np.random.default_rng(21)
+    big = rng.random((310, 333), dtype=np.float32)
+    view = to_dev(big)[3:300, 1:330]                      # row stride 333 floats, origin 4-byte aligned
+    x = np.ascontiguousarray(big[3:300, 1:330])
+    ref = oracle.gauss_fir(x, list(sig), list(ords), list(bcs), 3.0)
+    out = torch.empty((297, 329), device="cuda")
+    dip().GaussFIR(view, list(sig), list(ords), list(bcs), 3.0, out=out)
+    assert_close(out.cpu().numpy(), ref, x, str((sig, ords, bcs)))
