@@ -44,9 +44,13 @@ int intern( dipcu_filter_1d const& fin, bool dbl, AxisFilter& af, bool& meaningl
    }
    if( size == 1 && f[ 0 ] == 1.0 ) { meaningless = true; }
    af.mode = 1;
-   af.lo = origin;
-   af.hi = size - 1 - origin;
-   af.h = std::max( af.lo, af.hi );                          // the border (convolution.cpp:364-379)
+   // Tap span relative to the output sample: [-origin, size-1-origin], except for the two
+   // even-sized symmetric kinds, whose loop (convolution.cpp:256-283) pairs in[r+k] with in[r-1-k],
+   // r = i - origin + ds - 1, and so reads from i - origin - 1 to i - origin + size - 2.
+   bool const dsym = fin.symmetry == DIPCU_SYM_D_EVEN || fin.symmetry == DIPCU_SYM_D_ODD;
+   af.lo = dsym ? origin + 1 : origin;
+   af.hi = dsym ? size - 2 - origin : size - 1 - origin;
+   af.h = std::max( af.lo, af.hi );                          // covers the border of convolution.cpp:364-379
    af.full.assign( static_cast< size_t >( size ), 0.0 );
    auto at = [ & ]( int64_t j ) -> double& { return af.full[ static_cast< size_t >( j + af.lo ) ]; };
    switch( fin.symmetry ) {
@@ -71,6 +75,14 @@ int intern( dipcu_filter_1d const& fin, bool dbl, AxisFilter& af, bool& meaningl
             at( r - 1 - k ) = s * f[ static_cast< size_t >( k ) ];
          }
          break;
+      }
+   }
+   if( af.hi < 0 ) {                   // the span ends left of the output sample: pad with zero taps
+      af.full.resize( af.full.size() + static_cast< size_t >( -af.hi ), 0.0 );
+      af.hi = 0;
+      af.h = std::max( af.lo, af.hi );
+      if( static_cast< int64_t >( af.full.size() ) > kGeneralMaxTaps ) {
+         return record_error( DIPCU_ERR_KERNEL_TOO_LARGE, "filter longer than 256 taps" );
       }
    }
    return DIPCU_OK;

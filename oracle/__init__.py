@@ -238,6 +238,179 @@ def uniform(x: np.ndarray, sizes, bcs: Sequence[str] = (), out_dtype=None) -> np
     return out
 
 
+def optimal_dft_size(n: int, max_factor: int = 5) -> int:
+    """GetOptimalDFTSize(n, larger=true, maxFactor) (src/transform/dft_optimal_size.cpp:168-184): the
+    smallest size >= n whose prime factors are all <= max_factor."""
+    primes = [p_ for p_ in (2, 3, 5, 7, 11) if p_ <= max_factor]
+    m = max(1, int(n))
+    while True:
+        r = m
+        for p_ in primes:
+            while r % p_ == 0:
+                r //= p_
+        if r == 1:
+            return m
+        m += 1
+
+
+def window_origin(image_size: int, window_size: int) -> int:
+    """GetWindowOrigin for CENTER (src/library/image_manip.cpp:557-566)."""
+    return (image_size - window_size) // 2 + int((image_size % 2 == 0) and (window_size % 2 == 1))
+
+
+def _gaussft_lut(n: int, sigma: float, order: int, truncation: float, dt_double: bool) -> np.ndarray:
+    """GaussFTLineFilter's look-up table (src/linear/gauss.cpp:296-343) for one axis, centred
+    coordinates (origin n // 2), in the computation precision."""
+    ft = np.float64 if dt_double else np.float32
+    ct = np.complex128 if dt_double else np.complex64
+    lut = np.zeros(n, ct)
+    origin = n // 2
+    b = ft(2.0 * np.pi * sigma) / ft(n)
+    b = -ft(0.5) * b * b
+    if b == 0:
+        nh = n
+    else:
+        nh = int(oracle_lib().or_half_gaussian_size(float(n) / (2.0 * np.pi * sigma), order, truncation, int(dt_double)))
+    begin, end = max(0, origin - nh), min(n, origin + nh + 1)
+    x = (np.arange(begin, end) - origin).astype(ft)
+    if order > 0:
+        a = ct(complex(0.0, float(ft(2.0 * np.pi) / ft(n)))) ** order
+        val = a * (x.astype(ct) ** order)
+        if b != 0:
+            val = val * np.exp(b * x * x)
+        lut[begin:end] = val
+    else:
+        lut[begin:end] = np.exp(b * x * x) if b != 0 else 1
+    return lut
+
+
+def gauss_ft(x: np.ndarray, sigmas: Sequence[float] = (1.0,), orders: Sequence[int] = (0,),
+             truncation: float = 3.0, bcs: Sequence[str] | None = None) -> np.ndarray:
+    """dip::GaussFT (src/linear/gauss.cpp:397-487) for real input, spatial in and out, restated with
+    numpy's FFT in double precision: the input (extended by the boundary condition to an optimal DFT
+    size when `bcs` is given, centred as ExtendImageToSize places it) is transformed, multiplied by
+    each axis' Gaussian (derivative) look-up table at the centred frequency, transformed back (real
+    part, scaled by 1/N) and cropped back to the input's sizes."""
+    nd = x.ndim
+    sig = [float(v) for v in _broadcast(sigmas, nd, 1.0)]     # DIPlib order (x first)
+    ords = [int(v) for v in _broadcast(orders, nd, 0)]
+    dims = list(reversed(x.shape))                             # DIPlib order
+    for d in range(nd):
+        if dims[d] == 1:
+            sig[d], ords[d] = 0.0, 0
+        elif sig[d] < 0:
+            sig[d] = 0.0
+    out_dt = suggest_flex(x.dtype)
+    if not any(sig) and not any(ords):
+        return x.astype(out_dt)
+    dt_double = out_dt == np.float64
+    img = x.astype(np.float64)
+    origins = [0] * nd
+    if bcs:
+        bcl = _broadcast(bcs, nd, "mirror")
+        new = []
+        for d in range(nd):
+            h = int(oracle_lib().or_half_gaussian_size(sig[d], ords[d], truncation, int(x.dtype == np.float64)))
+            new.append(optimal_dft_size(dims[d] + 2 * h, 5))
+        for d in range(nd):
+            ax = nd - 1 - d
+            o = window_origin(new[d], dims[d])
+            origins[d] = o
+            idx = np.arange(new[d]) - o
+            src = np.array([_map_index(int(j), dims[d], bcl[d]) for j in idx])
+            sgn = np.array([_map_sign(int(j), dims[d], bcl[d]) for j in idx], dtype=np.float64)
+            img = np.take(img, np.where(src < 0, 0, src), axis=ax)
+            shape = [1] * nd
+            shape[ax] = new[d]
+            img = img * np.where(src < 0, 0.0, sgn).reshape(shape)
+    F = np.fft.fftn(np.fft.ifftshift(img))                   # spatial origin at index n // 2
+    # The reference's real-to-complex transform (src/transform/fourier.cpp:86-96, 387-441) runs along
+    # one dimension r (the first with more than 2 samples, all strides being normal); for an odd size
+    # along r its half-line shift leaves the outermost frequency unconjugated, so that the spectrum it
+    # produces holds the planes x_r = +M and x_r = -M (M = (N_r - 1) / 2) swapped.  Its inverse is a
+    # complex-to-real transform that uses only the half x_r <= 0.  Both are restated here.
+    sizes_dip = [img.shape[nd - 1 - d] for d in range(nd)]
+    r = 0
+    for d in range(1, nd):
+        if sizes_dip[r] <= 2 and sizes_dip[d] > 2:
+            r = d
+    axr = nd - 1 - r
+    nr = img.shape[axr]
+    if nr % 2 == 1 and nr > 2:
+        m = (nr - 1) // 2
+        idx = [slice(None)] * nd
+        idx[axr] = m
+        pos = F[tuple(idx)].copy()
+        idx2 = list(idx)
+        idx2[axr] = nr - m                       # x_r = -M in the unshifted layout
+        F[tuple(idx)] = F[tuple(idx2)]
+        F[tuple(idx2)] = pos
+    for d in range(nd):
+        ax = nd - 1 - d
+        n = img.shape[ax]
+        lut_c = _gaussft_lut(n, sig[d], ords[d], truncation, dt_double).astype(np.complex128)
+        k = np.arange(n)
+        lut_u = lut_c[(k + n // 2) % n]
+        shape = [1] * nd
+        shape[ax] = n
+        F = F * lut_u.reshape(shape)
+    # Hermitian completion of the half x_r <= 0 (unshifted: 0 and nr - nr // 2 .. nr - 1)
+    H = F.copy()
+    for xr in range(1, (nr + 1) // 2):
+        src = [slice(None)] * nd
+        src[axr] = nr - xr
+        part = np.conj(F[tuple(src)])
+        # negate the other frequencies: index -k mod n along every other axis
+        for ax in range(nd):
+            if ax != axr:
+                part = np.roll(np.flip(part, axis=ax if ax < axr else ax - 1), 1, axis=ax if ax < axr else ax - 1)
+        dst = [slice(None)] * nd
+        dst[axr] = xr
+        H[tuple(dst)] = part
+    res = np.fft.fftshift(np.real(np.fft.ifftn(H)))
+    sl = tuple(slice(origins[nd - 1 - ax], origins[nd - 1 - ax] + x.shape[ax]) for ax in range(nd))
+    return res[sl].astype(out_dt)
+
+
+def _map_index(j: int, n: int, bc: str) -> int:
+    """Source sample of extended position j (index-mapping conditions; -1: "add zeros")."""
+    if 0 <= j < n:
+        return j
+    code = bc_code(bc)
+    if code == 5:
+        return -1
+    if n == 1:
+        return 0
+    if code in (0, 1):
+        p_ = n - 1
+        k = -j if j < 0 else j - p_
+        t = k % (2 * p_)
+        if t > p_:
+            t = 2 * p_ - t
+        return t if j < 0 else p_ - t
+    if code in (3, 4):
+        return j % n
+    if code == 8:
+        return 0 if j < 0 else n - 1
+    raise ValueError("boundary condition not supported by the FT restatement: " + bc)
+
+
+def _map_sign(j: int, n: int, bc: str) -> float:
+    if 0 <= j < n:
+        return 1.0
+    code = bc_code(bc)
+    if n == 1:
+        return -1.0 if code in (1, 4) else 1.0
+    if code == 1:
+        p_ = n - 1
+        k = -j if j < 0 else j - p_
+        return -1.0 if ((k - 1) // p_) % 2 == 0 else 1.0
+    if code == 4:
+        k = -j if j < 0 else j - (n - 1)
+        return -1.0 if ((k - 1) // n) % 2 == 0 else 1.0
+    return 1.0
+
+
 def separable_fir(x: np.ndarray, taps, odd, bcs, out_dtype=None) -> np.ndarray:
     """The restated dip::SeparableConvolution with given EVEN/ODD half kernels, centre tap first
     (per axis, DIPlib order; None leaves an axis unfiltered)."""

@@ -26,6 +26,7 @@
 #include "diplib/kernel.h"
 #include "diplib/library/copy_buffer.h"
 #include "diplib/linear.h"
+#include "diplib/transform.h"
 #include "diplib/multithreading.h"
 
 namespace {
@@ -88,8 +89,16 @@ dip::Image Wrap( void const* data, int dtype, int ndims, int64_t const* sizes, i
 }
 
 void CopyOut( dip::Image const& img, void* out ) {
-   // `img` is freshly forged, so it has normal strides (contiguous, x fastest, tensor interleaved).
-   DIP_THROW_IF( !img.HasNormalStrides(), "unexpected strides" );
+   // Normal strides (contiguous, x fastest, tensor interleaved); a result with other strides (e.g. a
+   // cropped view) is copied into such an image first.
+   if( !img.HasNormalStrides() ) {
+      dip::Image tmp;
+      tmp.ReForge( img.Sizes(), img.TensorElements(), img.DataType() );
+      DIP_THROW_IF( !tmp.HasNormalStrides(), "unexpected strides" );
+      tmp.Copy( img );
+      std::memcpy( out, tmp.Origin(), tmp.NumberOfSamples() * tmp.DataType().SizeOf() );
+      return;
+   }
    std::memcpy( out, img.Origin(), img.NumberOfSamples() * img.DataType().SizeOf() );
 }
 
@@ -141,6 +150,25 @@ int dipref_uniform(
       dip::Image res;
       dip::Uniform( img, res, dip::Kernel( fs, dip::S::RECTANGULAR ), SplitList( bcs, has_bcs != 0 ));
       *out_dtype = TypeToCode( res.DataType() );
+      CopyOut( res, out );
+      return 0;
+   } catch( dip::Error const& e ) {
+      SetErr( err, errlen, e.what() );
+      return 1;
+   }
+}
+
+// dip::FourierTransform of a real sfloat image into an scomplex one (interleaved re, im; normal
+// strides), options newline-separated ("" for the forward transform).
+int dipref_fourier_transform( float const* in, int ndims, int64_t const* sizes, char const* options, float* out,
+                              char* err, int errlen ) {
+   try {
+      dip::Image img = Wrap( in, 9, ndims, sizes, nullptr );
+      dip::StringArray opts = SplitList( options, options && options[ 0 ] );
+      dip::StringSet os( opts.begin(), opts.end() );
+      dip::Image res;
+      dip::FourierTransform( img, res, os );
+      res.Convert( dip::DT_SCOMPLEX );
       CopyOut( res, out );
       return 0;
    } catch( dip::Error const& e ) {

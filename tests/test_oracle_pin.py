@@ -126,3 +126,62 @@ def test_reference_one_thread_equals_all_threads():
     finally:
         oracle.ref_set_threads(0)
     assert np.array_equal(one, many)
+
+
+def test_separable_convolution_and_uniform_pinned_to_the_reference():
+    """The oracle's general SeparableConvolution (every real symmetry, origins, one or per-axis
+    filters, process flags) and rectangular Uniform (running sum) equal the reference's own
+    dip::SeparableConvolution / dip::Uniform bit for bit."""
+    if not oracle.ref_available():
+        pytest.skip("reference build not present")
+    rng = np.random.default_rng(44)
+    syms = ["general", "even", "odd", "d-even", "d-odd", "conj", "d-conj"]
+    bcs_all = ["mirror", "asym mirror", "periodic", "asym periodic", "add zeros", "add max", "add min", "zero order",
+               "first order", "second order", "third order"]
+    for case in range(50):
+        nd = int(rng.integers(1, 4))
+        shape = tuple(int(v) for v in rng.integers(1, 30, nd))
+        dt = [np.float32, np.float64, np.uint16, np.int32, np.uint8][int(rng.integers(0, 5))]
+        x = (rng.random(shape) * 100).astype(dt)
+        nf = 1 if rng.random() < 0.3 else nd
+        filters = []
+        for _ in range(nf):
+            n = int(rng.integers(1, 8))
+            sym = syms[int(rng.integers(0, len(syms)))]
+            filters.append({"filter": list(rng.standard_normal(n)),
+                            "origin": int(rng.integers(-1, n)) if sym == "general" else -1, "symmetry": sym})
+        bcs = [bcs_all[int(rng.integers(0, len(bcs_all)))] for _ in range(nd)]
+        process = None if rng.random() < 0.7 else [bool(v) for v in rng.integers(0, 2, nd)]
+        ref = oracle.ref_separable_convolution(x, filters, bcs, process)
+        got = oracle.separable_convolution(x, filters, bcs, process)
+        np.testing.assert_array_equal(got, ref, err_msg=f"separable case {case}")
+        sizes = [int(v) for v in rng.integers(1, 10, nd)]
+        np.testing.assert_array_equal(oracle.uniform(x, sizes, bcs), oracle.ref_uniform(x, sizes, bcs),
+                                      err_msg=f"uniform case {case}")
+
+
+def test_gauss_ft_pinned_to_the_reference():
+    """The oracle's dip::GaussFT restatement (boundary extension to a 5-smooth DFT size, centred
+    transform, the Gaussian look-up table, real inverse, crop) equals the reference's
+    dip::Gauss(method "FT") to float rounding, for even and odd transform sizes (the odd sizes
+    exercise the reference's half-line shift, which swaps the outermost frequency planes along
+    its real-to-complex dimension)."""
+    if not oracle.ref_available():
+        pytest.skip("reference build not present")
+    rng = np.random.default_rng(12)
+    cases = [((40,), [0.5], [0], ["mirror"]), ((41,), [0.5], [0], ["periodic"]), ((38,), [1.0], [1], ["mirror"]),
+             ((40, 50), [0.5, 0.6], [0, 0], ["mirror"]), ((21, 30, 17), [0.6, 2.0, 0.6], [0, 1, 2], ["periodic"]),
+             ((64,), [0.4], [5], ["add zeros"]), ((31, 28), [1.0, 0.5], [2, 3], ["mirror"]),
+             ((33, 41), [0.7, 0.5], [1, 4], ["zero order"]), ((40, 40), [0.5, 0.5], [1, 1], ["mirror"]),
+             ((9, 40, 7), [0.5, 0.5, 0.5], [1, 0, 1], ["asym mirror"]), ((41, 2), [0.5, 0.5], [0, 1], ["mirror"]),
+             ((43, 43), [0.5, 1.5], [1, 2], ["mirror", "periodic"])]
+    for shape, sig, o, bcs in cases:
+        x = rng.random(shape).astype(np.float32)
+        ref = oracle.ref_gauss(x, sig, o, bcs, 3.0, method="FT")
+        got = oracle.gauss_ft(x, sig, o, 3.0, bcs)
+        assert ref.dtype == np.float32
+        err = np.abs(ref.astype(np.float64) - got).max() / max(1.0, float(np.abs(ref).max()))
+        assert err < 2e-6, (shape, sig, o, bcs, err)
+    x = rng.random((40, 33))
+    ref = oracle.ref_gauss(x, [0.5, 0.5], [1, 0], ["mirror"], 3.0, method="FT")
+    np.testing.assert_allclose(oracle.gauss_ft(x, [0.5, 0.5], [1, 0], 3.0, ["mirror"]), ref, rtol=0, atol=1e-13)
