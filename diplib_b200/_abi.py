@@ -66,6 +66,13 @@ SIGNATURES = {
                                                    _P(ctypes.c_int32), _P(ctypes.c_uint8), ctypes.c_void_p]),
     "dipcu_uniform": (ctypes.c_int, [_P(ImageDesc), _P(ImageDesc), _P(ctypes.c_double), _P(ctypes.c_int32),
                                      ctypes.c_void_p]),
+    "dipcu_gauss_fir_multi": (ctypes.c_int, [_P(ImageDesc), _P(ImageDesc), ctypes.c_int, _P(ctypes.c_uint32), ctypes.c_int,
+                                             ctypes.c_int32, _P(ctypes.c_double), _P(ctypes.c_int32), ctypes.c_double,
+                                             ctypes.c_void_p]),
+    "dipcu_gauss_fir_multi_supported": (ctypes.c_int, [_P(ImageDesc), _P(ctypes.c_uint32), ctypes.c_int, _P(ctypes.c_double),
+                                                       _P(ctypes.c_int32), ctypes.c_double]),
+    "dipcu_gauss_ft": (ctypes.c_int, [_P(ImageDesc), _P(ImageDesc), _P(ctypes.c_double), _P(ctypes.c_uint32),
+                                      ctypes.c_double, _P(ctypes.c_int32), ctypes.c_int, ctypes.c_void_p]),
     "dipcu_gauss_fir_backward": (ctypes.c_int, [_P(ImageDesc), _P(ImageDesc), _P(ImageDesc), ctypes.c_void_p,
                                                 _P(ctypes.c_double), _P(ctypes.c_uint32), _P(ctypes.c_int32),
                                                 ctypes.c_double, ctypes.c_void_p]),

@@ -67,7 +67,7 @@ def build(verbose: bool = False) -> str:
     with concurrent.futures.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
         objs = list(ex.map(lambda s: _compile(s, verbose), sources()))
     if not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs):
-        cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs]
+        cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcufft"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")

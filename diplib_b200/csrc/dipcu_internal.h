@@ -165,6 +165,15 @@ int build_filters( dipcu_image_desc const* in, double const* sigmas, uint32_t co
 // Framework::Separable's pass order: processed axes by input stride, stable.
 std::vector< int > pass_order( dipcu_image_desc const* in, std::vector< AxisFilter > const& f );
 
+// Several GaussFIR outputs of `in` (sizes and boundary conditions shared, `ncomp` order vectors of
+// ndims entries) from one read of it, by the multi-output tile kernel (multi_deriv.cu).  `mode`:
+// 0 the components (nout = ncomp), 1 their symmetric products in DIPlib's symmetric-matrix order
+// (nout = ncomp (ncomp + 1) / 2), 2 their sum, 3 the square root of their sum of squares (nout = 1).
+// Returns -1 when the kernel does not take the case (2D/3D float computation, index-mapping or
+// "add zeros" boundary conditions on filtered axes, half-widths up to 8, up to 6 components).
+int multi_gauss_fir( dipcu_image_desc const* in, dipcu_image_desc const* outs, int nout, uint32_t const* orders, int ncomp,
+                     int mode, double const* sigmas, int32_t const* bcs, double truncation, cudaStream_t stream );
+
 // Copies `in` to `out` with the type conversion (no axis filtered).
 int run_convert( dipcu_image_desc const* in, dipcu_image_desc const* out, cudaStream_t stream );
 

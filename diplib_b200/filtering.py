@@ -208,6 +208,10 @@ def GaussFIR(in_, sigmas: Iterable[float] | float = (1.0,), derivativeOrder: Ite
     return _to_host(res) if was_numpy else res
 
 
+def _as_list(v) -> list:
+    return [v] if isinstance(v, str) else list(v)
+
+
 def _prepare_out(x: torch.Tensor, out):
     """(result tensor, tensor to copy it into afterwards or None) for an optional `out`, with
     DIPlib's rules: the output's type is kept when given (protected output), and an output sharing
@@ -298,17 +302,53 @@ def Uniform(in_, kernel=7, boundaryCondition=(), *, shape: str = "rectangular", 
     return _to_host(res) if was_numpy else res
 
 
+def GaussFT(in_, sigmas: Iterable[float] | float = (1.0,), derivativeOrder: Iterable[int] | int = (0,),
+            truncation: float = 3.0, inRepresentation: str = "spatial", outRepresentation: str = "spatial",
+            boundaryCondition: Iterable[str] | str = (), *, out=None):
+    """dip::GaussFT (include/diplib/linear.h:365-390, src/linear/gauss.cpp:397-487) with spatial
+    input and output.  ``boundaryCondition`` empty: the transform covers exactly the image; else
+    the image is first extended by it (one value for all axes, or one per axis).  ``out`` as in
+    GaussFIR."""
+    for rep in (inRepresentation, outRepresentation):
+        if rep not in ("spatial", "frequency"):
+            raise ParameterError("Invalid flag: " + rep)
+    if inRepresentation != "spatial" or outRepresentation != "spatial":
+        raise NotImplementedError("GaussFT on the B200 path takes and returns spatial images")
+    x, was_numpy = _to_device(in_)
+    if x.dtype.is_complex:
+        raise NotImplementedError("complex images are outside the B200 real-valued path")
+    nd = max(1, x.dim())
+    sig = [float(s) for s in _array_use_parameter(sigmas, nd, 1.0)]
+    ords = [int(o) for o in _array_use_parameter(derivativeOrder, nd, 0)]
+    if any(o < 0 for o in ords):
+        raise ParameterError("derivative orders must be non-negative")
+    bcl = list(boundaryCondition) if not isinstance(boundaryCondition, str) else [boundaryCondition]
+    bcs = [BoundaryConditionFromString(b) for b in _array_use_parameter(bcl, nd, "")] if bcl else []
+    res, target = _prepare_out(x, out)
+    din, dout = image_desc(x), image_desc(res)
+    _run(x, _abi.lib().dipcu_gauss_ft, ctypes.byref(din), ctypes.byref(dout), (ctypes.c_double * nd)(*sig),
+         (ctypes.c_uint32 * nd)(*ords), float(truncation), (ctypes.c_int32 * max(1, len(bcs)))(*bcs), len(bcs))
+    if target is not None:
+        target.copy_(res)
+        res = target
+    return _to_host(res) if was_numpy else res
+
+
 def Gauss(in_, sigmas=(1.0,), derivativeOrder=(0,), method: str = "best", boundaryCondition=(),
           truncation: float = 3.0, *, out=None):
     """dip::Gauss (src/linear/derivative.cpp:62-86): the "gauss" prefix is stripped and "best"
-    resolved by BestGaussMethod; this implementation provides the FIR method."""
+    resolved by BestGaussMethod; this implementation provides the FIR and FT methods."""
     m = method[5:] if method[:5] == "gauss" else method
     x_nd = max(1, (in_.dim() if isinstance(in_, torch.Tensor) else np.asarray(in_).ndim))
     if m == "best":
         m = BestGaussMethod(_array_use_parameter(sigmas, x_nd, 1.0), _array_use_parameter(derivativeOrder, x_nd, 0))
     if m in ("FIR", "fir"):
         return GaussFIR(in_, sigmas, derivativeOrder, boundaryCondition, truncation, out=out)
-    if m in ("FT", "ft", "IIR", "iir"):
+    if m in ("FT", "ft"):
+        # For GaussFT the empty boundary condition is not dip::Gauss's default (derivative.cpp:76-79).
+        bc = boundaryCondition if len(_as_list(boundaryCondition)) else ["default"]
+        return GaussFT(in_, sigmas, derivativeOrder, truncation, "spatial", "spatial", bc, out=out)
+    if m in ("IIR", "iir"):
         raise NotImplementedError(f"Gauss method {method!r} (resolved to {m!r}) is outside the B200 FIR path")
     raise ParameterError("Invalid flag: " + m)
 

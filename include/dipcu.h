@@ -127,6 +127,38 @@ typedef struct {
 int dipcu_separable_convolution( dipcu_image_desc const* in, dipcu_image_desc const* out, dipcu_filter_1d const* filters,
                                  int nfilters, int32_t const* bcs, uint8_t const* process, void* stream );
 
+/* Several Gaussian derivatives of one image from one read of it: the components of dip::Gradient,
+ * dip::Hessian and dip::Laplace (src/linear/derivative.cpp:142-172, 330-418 in DIPlib), which the
+ * reference computes as one dip::GaussFIR call each.  `orders` holds ncomp order vectors of ndims
+ * entries; sigmas, boundary conditions and truncation are shared (ndims values each) and each
+ * component equals dipcu_gauss_fir with its orders.  `mode` 0 writes the components (nout =
+ * ncomp), 1 their symmetric products g_i g_j in DIPlib's symmetric-matrix order (diagonal first,
+ * then the upper triangle column by column; nout = ncomp (ncomp + 1) / 2; dip::StructureTensor's
+ * products), 2 their sum (dip::Laplace), 3 the square root of their sum of squares
+ * (dip::GradientMagnitude); nout = 1 for modes 2 and 3.  `outs` are nout output images of the
+ * input's sizes, any type (clamp_cast on the write).  Taken: 2D and 3D images whose computation
+ * type is sfloat, index-mapping or "add zeros" boundary conditions on the filtered axes,
+ * half-widths up to 8, up to 6 components (dipcu_gauss_fir_multi_supported says so, without
+ * recording an error); other cases are DIPCU_ERR_INVALID_ARG. */
+int dipcu_gauss_fir_multi( dipcu_image_desc const* in, dipcu_image_desc const* outs, int nout, uint32_t const* orders,
+                           int ncomp, int32_t mode, double const* sigmas, int32_t const* bcs, double truncation, void* stream );
+int dipcu_gauss_fir_multi_supported( dipcu_image_desc const* in, uint32_t const* orders, int ncomp, double const* sigmas,
+                                     int32_t const* bcs, double truncation );
+
+/* dip::GaussFT with spatial input and output (src/linear/gauss.cpp:397-487 in DIPlib): the
+ * Gaussian (derivative) filter computed by multiplication in the Fourier domain.  `sigmas` and
+ * `orders` hold ndims values (a negative sigma means no smoothing; an axis of size 1 is not
+ * filtered; any derivative order).  With nbcs == ndims the image is first extended by those
+ * boundary conditions to 5-smooth transform sizes that hold twice the half Gaussian size on each
+ * side (as dip::Gauss does, which passes "default", i.e. mirror, when given none); with nbcs == 0
+ * the transform covers exactly the image (periodic).  Extension supports the index-mapping
+ * conditions and "add zeros" (DIPCU_ERR_UNSUPPORTED_BC otherwise).  Images of 1 to 3 dimensions.
+ * Computation in dip::DataType::SuggestComplex of the input (double for 32/64-bit integers and
+ * dfloat, else float); output type as dipcu_gauss_fir.  The transforms are cuFFT's; the outputs
+ * follow the reference's own transform, including its treatment of odd transform lengths. */
+int dipcu_gauss_ft( dipcu_image_desc const* in, dipcu_image_desc const* out, double const* sigmas, uint32_t const* orders,
+                    double truncation, int32_t const* bcs, int nbcs, void* stream );
+
 /* dip::Uniform with a rectangular kernel (src/linear/uniform.cpp:68-86, 147-163 in DIPlib): `sizes`
  * holds the kernel's per-axis sizes (ndims values; a size above 1 is truncated to an integer, as
  * dip::Kernel::Sizes does, others leave the axis unfiltered); the mean over the window

@@ -285,7 +285,7 @@ def _gaussft_lut(n: int, sigma: float, order: int, truncation: float, dt_double:
 
 
 def gauss_ft(x: np.ndarray, sigmas: Sequence[float] = (1.0,), orders: Sequence[int] = (0,),
-             truncation: float = 3.0, bcs: Sequence[str] | None = None) -> np.ndarray:
+             truncation: float = 3.0, bcs: Sequence[str] | None = None, rdim: int | None = None) -> np.ndarray:
     """dip::GaussFT (src/linear/gauss.cpp:397-487) for real input, spatial in and out, restated with
     numpy's FFT in double precision: the input (extended by the boundary condition to an optimal DFT
     size when `bcs` is given, centred as ExtendImageToSize places it) is transformed, multiplied by
@@ -334,6 +334,8 @@ def gauss_ft(x: np.ndarray, sigmas: Sequence[float] = (1.0,), orders: Sequence[i
     for d in range(1, nd):
         if sizes_dip[r] <= 2 and sizes_dip[d] > 2:
             r = d
+    if rdim is not None:          # the axis the reference picks for an input with other strides
+        r = rdim
     axr = nd - 1 - r
     nr = img.shape[axr]
     if nr % 2 == 1 and nr > 2:

@@ -178,8 +178,8 @@ def test_gauss_best_method_dispatch(cuda):
     ref = oracle.gauss_fir(x, [2.0], [0], ["mirror"], 3.0)
     assert_close(dip().Gauss(x, 2.0), ref, x, "best")
     assert_close(dip().Gauss(x, [2.0], [0], "gaussFIR"), ref, x, "gaussFIR")
-    with pytest.raises(NotImplementedError):
-        dip().Gauss(x, [0.5])
+    # sigma < 0.8 resolves to the FT method ("default" boundary condition), sigma > 10 to IIR
+    assert_close(dip().Gauss(x, [0.5]), oracle.gauss_ft(x, [0.5], [0], 3.0, ["mirror"]), x, "best -> FT")
 
 
 def test_device_weights_match_oracle(cuda):
