@@ -27,6 +27,10 @@ ERR_TIMEOUT = 6
 ERR_SIZES_DONT_MATCH = 7
 ERR_KERNEL_TOO_LARGE = 8
 
+# dipcu_gauss_iir design methods
+IIR_DISCRETE_TIME_FIT = 0
+IIR_FORWARD_BACKWARD = 1
+
 
 class ImageDesc(ctypes.Structure):
     _fields_ = [
@@ -71,6 +75,9 @@ SIGNATURES = {
                                              ctypes.c_void_p]),
     "dipcu_gauss_fir_multi_supported": (ctypes.c_int, [_P(ImageDesc), _P(ctypes.c_uint32), ctypes.c_int, _P(ctypes.c_double),
                                                        _P(ctypes.c_int32), ctypes.c_double]),
+    "dipcu_gauss_iir": (ctypes.c_int, [_P(ImageDesc), _P(ImageDesc), _P(ctypes.c_double), _P(ctypes.c_uint32),
+                                       _P(ctypes.c_int32), _P(ctypes.c_uint32), ctypes.c_int32, ctypes.c_double,
+                                       ctypes.c_void_p]),
     "dipcu_gauss_ft": (ctypes.c_int, [_P(ImageDesc), _P(ImageDesc), _P(ctypes.c_double), _P(ctypes.c_uint32),
                                       ctypes.c_double, _P(ctypes.c_int32), ctypes.c_int, ctypes.c_void_p]),
     "dipcu_gauss_fir_backward": (ctypes.c_int, [_P(ImageDesc), _P(ImageDesc), _P(ImageDesc), ctypes.c_void_p,

@@ -24,8 +24,9 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
 
 
 # Per-file flags.  k_weights.cu: no FMA contraction, so that the device weights follow the
-# reference's double operation order exactly (they must equal DIPlib's taps bit for bit).
-FILE_FLAGS = {"k_weights.cu": ["-fmad=false"]}
+# reference's double operation order exactly (they must equal DIPlib's taps bit for bit);
+# gauss_iir.cu: each recursion step is the reference's sequence of double operations.
+FILE_FLAGS = {"k_weights.cu": ["-fmad=false"], "gauss_iir.cu": ["-fmad=false"]}
 
 
 def nvcc() -> str:

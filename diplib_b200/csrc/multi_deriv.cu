@@ -5,7 +5,7 @@
 //
 // One CTA per output tile (32 x TY x TZ samples, x y z):
 //   1. the input tile plus its halo, extended by the boundary condition (an index mapping per
-//      axis, or zeros), is read once into shared memory as float;
+//      axis, or zeros), is read once into shared memory as float (batches of loads in flight);
 //   2. z passes: every z order any component needs, over the tile's x-y halo region (each thread
 //      one (x, y) column, its z window in registers, all z orders from one load of the window);
 //   3. y passes: every (y order, z order) pair any component needs, over the x halo region;
@@ -35,6 +35,7 @@ constexpr int kMdMaxOrd = 4;     // distinct filters per axis
 constexpr int kMdTX = 32;        // tile width
 constexpr int kMdR = 8;          // outputs per thread in the x pass
 constexpr int kMdThreads = 256;
+constexpr int kMdLoadBatch = 8;  // tile elements per thread whose loads are in flight together
 
 struct MdArgs {
    void const* src;
@@ -57,6 +58,7 @@ struct MdArgs {
    int32_t dst_dt[ kMdMaxComp ];
    int64_t ds[ kMdMaxComp ][ 3 ];
    int32_t off_a, off_b;                // shared-memory offsets (floats) of the z- and y-pass buffers
+   int32_t all_float;                   // every output is sfloat
 };
 
 // Source index of extended position j along an axis of n samples (-1: a zero of "add zeros").
@@ -80,10 +82,11 @@ template< int HB, int TY, int TZ >
 __global__ void __launch_bounds__( kMdThreads ) multi_deriv_kernel( MdArgs const __grid_constant__ a ) {
    constexpr int HZ = TZ > 1 ? HB : 0;
    constexpr int W0 = kMdTX + 2 * HB, W1 = TY + 2 * HB, W2 = TZ + 2 * HZ;
+   constexpr int YP = W0 | 1;       // row stride of the y-pass buffers (odd: conflict-free x pass)
    extern __shared__ float md_smem[];
    float* const tin = md_smem;                          // [W2][W1][W0]
    float* const za = TZ > 1 ? md_smem + a.off_a : tin;  // [nord_z][TZ][W1][W0]
-   float* const yb = md_smem + a.off_b;                 // [ncombo][TZ][TY][W0]
+   float* const yb = md_smem + a.off_b;                 // [ncombo][TZ][TY][YP]
    int const tid = static_cast< int >( threadIdx.x );
 
    int64_t t = blockIdx.x;
@@ -93,19 +96,39 @@ __global__ void __launch_bounds__( kMdThreads ) multi_deriv_kernel( MdArgs const
    int const tz = static_cast< int >( t / a.tiles[ 1 ] );
    int const x0 = tx * kMdTX, y0 = ty * TY, z0 = tz * TZ;
 
-   // 1. input tile with halo
-   for( int e = tid; e < W0 * W1 * W2; e += kMdThreads ) {
-      int const i = e % W0, j = ( e / W0 ) % W1, k = e / ( W0 * W1 );
-      bool n0, n1, n2;
-      int64_t const sx = md_map( x0 - HB + i, a.n[ 0 ], a.bc[ 0 ], &n0 );
-      int64_t const sy = md_map( y0 - HB + j, a.n[ 1 ], a.bc[ 1 ], &n1 );
-      int64_t const sz = TZ > 1 ? md_map( z0 - HZ + k, a.n[ 2 ], a.bc[ 2 ], &n2 ) : ( n2 = false, z0 );
-      float v = 0.f;
-      if( sx >= 0 && sy >= 0 && sz >= 0 ) {
-         v = load_as< float >( a.src, a.src_dt, sx * a.ss[ 0 ] + sy * a.ss[ 1 ] + sz * a.ss[ 2 ] );
-         if( n0 != ( n1 != n2 )) { v = -v; }
+   // 1. input tile with halo: each thread a batch of kMdLoadBatch elements whose loads are all
+   //    issued before any is stored (the loads' latency overlaps), source rows mapped through the
+   //    boundary condition, columns directly where the tile lies inside the image along x
+   {
+      bool const xin = x0 - HB >= 0 && x0 - HB + W0 <= a.n[ 0 ];
+      bool const fsrc = a.src_dt == DT_SFLOAT;
+      constexpr int NE = W0 * W1 * W2;
+      for( int e0 = 0; e0 < NE; e0 += kMdThreads * kMdLoadBatch ) {
+         float v[ kMdLoadBatch ];
+#pragma unroll
+         for( int u = 0; u < kMdLoadBatch; ++u ) {
+            int const e = e0 + u * kMdThreads + tid;
+            v[ u ] = 0.f;
+            if( e < NE ) {
+               int const i = e % W0, j = ( e / W0 ) % W1, k = e / ( W0 * W1 );
+               bool n0 = false, n1, n2;
+               int64_t const sy = md_map( y0 - HB + j, a.n[ 1 ], a.bc[ 1 ], &n1 );
+               int64_t const sz = TZ > 1 ? md_map( z0 - HZ + k, a.n[ 2 ], a.bc[ 2 ], &n2 ) : ( n2 = false, z0 );
+               int64_t sx = x0 - HB + i;
+               if( !xin ) { sx = md_map( sx, a.n[ 0 ], a.bc[ 0 ], &n0 ); }
+               if( sx >= 0 && sy >= 0 && sz >= 0 ) {
+                  int64_t const off = sx * a.ss[ 0 ] + sy * a.ss[ 1 ] + sz * a.ss[ 2 ];
+                  float const t = fsrc ? __ldg( static_cast< float const* >( a.src ) + off ) : load_as< float >( a.src, a.src_dt, off );
+                  v[ u ] = ( n0 != ( n1 != n2 )) ? -t : t;
+               }
+            }
+         }
+#pragma unroll
+         for( int u = 0; u < kMdLoadBatch; ++u ) {
+            int const e = e0 + u * kMdThreads + tid;
+            if( e < NE ) { tin[ e ] = v[ u ]; }
+         }
       }
-      tin[ e ] = v;
    }
    __syncthreads();
 
@@ -140,9 +163,9 @@ __global__ void __launch_bounds__( kMdThreads ) multi_deriv_kernel( MdArgs const
             if( a.combo_z[ b ] != s ) { continue; }
             float const* const tp = a.taps[ 1 ][ a.combo_y[ b ]];
             bool const odd = a.fodd[ 1 ][ a.combo_y[ b ]] != 0;
-            float* const dst = yb + ( b * TZ + z ) * TY * W0 + i;
+            float* const dst = yb + ( b * TZ + z ) * TY * YP + i;
 #pragma unroll
-            for( int y = 0; y < TY; ++y ) { dst[ y * W0 ] = md_tap< HB >( v, y + HB, tp, odd ); }
+            for( int y = 0; y < TY; ++y ) { dst[ y * YP ] = md_tap< HB >( v, y + HB, tp, odd ); }
          }
       }
    }
@@ -150,6 +173,7 @@ __global__ void __launch_bounds__( kMdThreads ) multi_deriv_kernel( MdArgs const
 
    // 4. x passes and the epilogue: row (y, z), segment of kMdR outputs
    constexpr int SEGS = kMdTX / kMdR;
+   // a warp: 4 segments x 8 rows; with the odd row stride YP its reads fall in distinct banks
    for( int task = tid; task < SEGS * TY * TZ; task += kMdThreads ) {
       int const seg = task % SEGS, y = ( task / SEGS ) % TY, z = task / ( SEGS * TY );
       int const xo = x0 + seg * kMdR, yo = y0 + y, zo = z0 + z;
@@ -162,7 +186,7 @@ __global__ void __launch_bounds__( kMdThreads ) multi_deriv_kernel( MdArgs const
       }
       for( int b = 0; b < a.ncombo; ++b ) {
          float v[ kMdR + 2 * HB ];
-         float const* const src = yb + ( b * TZ + z ) * TY * W0 + y * W0 + seg * kMdR;
+         float const* const src = yb + ( b * TZ + z ) * TY * YP + y * YP + seg * kMdR;
 #pragma unroll
          for( int k = 0; k < kMdR + 2 * HB; ++k ) { v[ k ] = src[ k ]; }
 #pragma unroll
@@ -175,8 +199,11 @@ __global__ void __launch_bounds__( kMdThreads ) multi_deriv_kernel( MdArgs const
          }
       }
       int const nr = a.n[ 0 ] - xo < kMdR ? a.n[ 0 ] - xo : kMdR;
+      // sfloat outputs take plain stores
       auto store = [ & ]( int q, int r, float val ) {
-         store_from< float >( a.dst[ q ], a.dst_dt[ q ], ( xo + r ) * a.ds[ q ][ 0 ] + yo * a.ds[ q ][ 1 ] + zo * a.ds[ q ][ 2 ], val );
+         int64_t const off = ( xo + r ) * a.ds[ q ][ 0 ] + yo * a.ds[ q ][ 1 ] + zo * a.ds[ q ][ 2 ];
+         if( a.all_float ) { static_cast< float* >( a.dst[ q ] )[ off ] = val; }
+         else { store_from< float >( a.dst[ q ], a.dst_dt[ q ], off, val ); }
       };
       for( int r = 0; r < kMdR; ++r ) {
          if( r >= nr ) { break; }
@@ -290,7 +317,8 @@ int md_run( MdArgs& a, cudaStream_t stream ) {
    constexpr int W0 = kMdTX + 2 * HB, W1 = TY + 2 * HB, W2 = TZ + 2 * HZ;
    int64_t const tin = static_cast< int64_t >( W0 ) * W1 * W2;
    int64_t const za = TZ > 1 ? static_cast< int64_t >( a.nord[ 2 ] ) * TZ * W1 * W0 : 0;
-   int64_t const yb = static_cast< int64_t >( a.ncombo ) * TZ * TY * W0;
+   constexpr int YP = W0 | 1;
+   int64_t const yb = static_cast< int64_t >( a.ncombo ) * TZ * TY * YP;
    a.off_a = static_cast< int32_t >( tin );
    // in 3D the y-pass buffers may reuse the input tile (dead after the z passes); in 2D the y
    // passes read the input tile itself
@@ -334,9 +362,11 @@ int multi_gauss_fir( dipcu_image_desc const* in, dipcu_image_desc const* outs, i
    if( int st = md_build( in, orders, ncomp, sigmas, bcs, truncation, a, hb )) { return st; }
    a.mode = mode;
    a.nout = nout;
+   a.all_float = 1;
    for( int q = 0; q < nout; ++q ) {
       a.dst[ q ] = outs[ q ].data;
       a.dst_dt[ q ] = outs[ q ].dtype;
+      a.all_float = a.all_float && outs[ q ].dtype == DT_SFLOAT;
       for( int d = 0; d < 3; ++d ) { a.ds[ q ][ d ] = d < in->ndims ? outs[ q ].strides[ d ] : 0; }
    }
    if( in->ndims == 3 ) { return hb == 4 ? md_run< 4, 8, 8 >( a, stream ) : md_run< 8, 8, 4 >( a, stream ); }

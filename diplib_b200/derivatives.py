@@ -1,6 +1,10 @@
 """dip::Gradient, dip::GradientMagnitude, dip::Hessian and dip::Laplace (src/linear/derivative.cpp)
-with the Gaussian methods, on the B200 Gaussian FIR path: each component is one GaussFIR call
-through the C-ABI, written straight into its slice of the output.
+with the Gaussian methods, on the B200 Gaussian FIR path.  Where the multi-output tile kernel takes
+the case (2D/3D input computed in sfloat, index-mapping or "add zeros" boundary conditions,
+half-widths up to 8, all components resolving to the FIR method) every component, or their sum
+(Laplace) or root of the summed squares (GradientMagnitude), comes from ONE launch that reads the
+input once (``dipcu_gauss_fir_multi``); otherwise each component is one GaussFIR call through the
+C-ABI, written straight into its slice of the output, as the reference computes them.
 
 Tensor outputs come back planar, the component axis first: ``Gradient`` gives ``(m,) + shape``
 for the m axes FindGradientDimensions keeps; ``Hessian`` gives ``(m(m+1)/2,) + shape`` in DIPlib's
@@ -10,9 +14,13 @@ is the reverse of the array's (x is the last array axis) and per-axis parameters
 """
 from __future__ import annotations
 
+import ctypes
+
 import torch
 
-from .filtering import ParameterError, _array_use_parameter, _to_device, _to_host, flex_dtype, Derivative
+from . import _abi
+from .filtering import (BestGaussMethod, BoundaryConditionFromString, ParameterError, _array_use_parameter, _run,
+                        _to_device, _to_host, flex_dtype, image_desc, Derivative)
 
 __all__ = ["Gradient", "GradientMagnitude", "Hessian", "Laplace", "find_gradient_dimensions"]
 
@@ -48,6 +56,40 @@ def _order(nd: int, counts: dict) -> list:
     return o
 
 
+# dipcu_gauss_fir_multi modes
+_COMPONENTS, _PRODUCTS, _SUM, _MAGNITUDE = 0, 1, 2, 3
+
+
+def _multi(x: torch.Tensor, orders: list, mode: int, sg: list, method: str, boundaryCondition, truncation: float,
+           outs: list) -> bool:
+    """All components (or their sum / magnitude) from one read of `x` by the multi-output tile
+    kernel, when it takes the case; False (nothing written) when the caller must filter per
+    component.  Every component must resolve to the FIR method, as dip::Derivative would pick it."""
+    m = method[5:] if method[:5] == "gauss" else method
+    for o in orders:
+        if m == "best":
+            if BestGaussMethod(sg, o) != "fir":
+                return False
+        elif m not in ("fir", "FIR"):
+            return False
+    nd = max(1, x.dim())
+    if nd not in (2, 3) or x.dim() != nd:
+        return False
+    bcs = [BoundaryConditionFromString(b) for b in _array_use_parameter(boundaryCondition, nd, "")]
+    din = image_desc(x)
+    flat = [int(v) for o in orders for v in o]
+    c_ord = (ctypes.c_uint32 * len(flat))(*flat)
+    c_sig = (ctypes.c_double * nd)(*sg)
+    c_bc = (ctypes.c_int32 * nd)(*bcs)
+    lib = _abi.lib()
+    if not lib.dipcu_gauss_fir_multi_supported(ctypes.byref(din), c_ord, len(orders), c_sig, c_bc, float(truncation)):
+        return False
+    douts = (_abi.ImageDesc * len(outs))(*[image_desc(o) for o in outs])
+    _run(x, lib.dipcu_gauss_fir_multi, ctypes.byref(din), douts, len(outs), c_ord, len(orders), mode, c_sig, c_bc,
+         float(truncation))
+    return True
+
+
 def Gradient(in_, sigmas=(1.0,), method: str = "best", boundaryCondition=(), process=(), truncation: float = 3.0):
     """dip::Gradient (src/linear/derivative.cpp:142-172): the first derivative along every kept
     axis, stacked on a leading component axis."""
@@ -55,8 +97,10 @@ def Gradient(in_, sigmas=(1.0,), method: str = "best", boundaryCondition=(), pro
     x, was_numpy, dims, sg = _setup(in_, sigmas, process)
     nd = max(1, x.dim())
     out = torch.empty((len(dims),) + tuple(x.shape), dtype=flex_dtype(x.dtype), device=x.device)
-    for c, d in enumerate(dims):
-        Derivative(x, _order(nd, {d: 1}), sg, method, boundaryCondition, truncation, out=out[c])
+    orders = [_order(nd, {d: 1}) for d in dims]
+    if not _multi(x, orders, _COMPONENTS, sg, method, boundaryCondition, truncation, list(out)):
+        for c, o in enumerate(orders):
+            Derivative(x, o, sg, method, boundaryCondition, truncation, out=out[c])
     return _to_host(out) if was_numpy else out
 
 
@@ -67,6 +111,11 @@ def GradientMagnitude(in_, sigmas=(1.0,), method: str = "best", boundaryConditio
     _check_method(method)
     x, was_numpy, dims, sg = _setup(in_, sigmas, process)
     nd = max(1, x.dim())
+    if len(dims) > 1:
+        out = torch.empty(tuple(x.shape), dtype=flex_dtype(x.dtype), device=x.device)
+        if _multi(x, [_order(nd, {d: 1}) for d in dims], _MAGNITUDE, sg, method, boundaryCondition, truncation,
+                  [out]):
+            return _to_host(out) if was_numpy else out
     out = Derivative(x, _order(nd, {dims[0]: 1}), sg, method, boundaryCondition, truncation)
     if len(dims) == 1:
         out.abs_()
@@ -89,9 +138,10 @@ def Hessian(in_, sigmas=(1.0,), method: str = "best", boundaryCondition=(), proc
     m = len(dims)
     pairs = [(i, i) for i in range(m)] + [(i, j) for j in range(1, m) for i in range(j)]
     out = torch.empty((len(pairs),) + tuple(x.shape), dtype=flex_dtype(x.dtype), device=x.device)
-    for c, (i, j) in enumerate(pairs):
-        counts = {dims[i]: 2} if i == j else {dims[i]: 1, dims[j]: 1}
-        Derivative(x, _order(nd, counts), sg, method, boundaryCondition, truncation, out=out[c])
+    orders = [_order(nd, {dims[i]: 2} if i == j else {dims[i]: 1, dims[j]: 1}) for i, j in pairs]
+    if not _multi(x, orders, _COMPONENTS, sg, method, boundaryCondition, truncation, list(out)):
+        for c, o in enumerate(orders):
+            Derivative(x, o, sg, method, boundaryCondition, truncation, out=out[c])
     return _to_host(out) if was_numpy else out
 
 
@@ -101,6 +151,10 @@ def Laplace(in_, sigmas=(1.0,), method: str = "best", boundaryCondition=(), proc
     _check_method(method)
     x, was_numpy, dims, sg = _setup(in_, sigmas, process)
     nd = max(1, x.dim())
+    if len(dims) > 1:
+        out = torch.empty(tuple(x.shape), dtype=flex_dtype(x.dtype), device=x.device)
+        if _multi(x, [_order(nd, {d: 2}) for d in dims], _SUM, sg, method, boundaryCondition, truncation, [out]):
+            return _to_host(out) if was_numpy else out
     out = Derivative(x, _order(nd, {dims[0]: 2}), sg, method, boundaryCondition, truncation)
     if len(dims) > 1:
         tmp = torch.empty_like(out)

@@ -145,6 +145,20 @@ int dipcu_gauss_fir_multi( dipcu_image_desc const* in, dipcu_image_desc const* o
 int dipcu_gauss_fir_multi_supported( dipcu_image_desc const* in, uint32_t const* orders, int ncomp, double const* sigmas,
                                      int32_t const* bcs, double truncation );
 
+/* dip::GaussIIR (src/linear/gaussiir.cpp:725-790, include/diplib/linear.h:407-428 in DIPlib): the
+ * recursive Gaussian (derivative) filter of van Vliet, Young and Verbeek, orders 0-4 per axis,
+ * computed in dfloat like the reference (intermediates of the pass chain in dfloat, output
+ * clamp_cast to `out`'s type, normally dip::DataType::SuggestFlex of the input).  `filter_orders`:
+ * the recursion order per axis (1-5; NULL: the reference's default, order + 3 and 5 above order 2);
+ * `design`: DIPCU_IIR_DISCRETE_TIME_FIT ("discrete time fit", the reference's default) or
+ * DIPCU_IIR_FORWARD_BACKWARD ("forward backward").  Every boundary condition but "already
+ * expanded".  Scan lines and the intermediate are stream-ordered allocations. */
+#define DIPCU_IIR_DISCRETE_TIME_FIT 0
+#define DIPCU_IIR_FORWARD_BACKWARD 1
+int dipcu_gauss_iir( dipcu_image_desc const* in, dipcu_image_desc const* out, double const* sigmas,
+                     uint32_t const* orders, int32_t const* bcs, uint32_t const* filter_orders, int32_t design,
+                     double truncation, void* stream );
+
 /* dip::GaussFT with spatial input and output (src/linear/gauss.cpp:397-487 in DIPlib): the
  * Gaussian (derivative) filter computed by multiplication in the Fourier domain.  `sigmas` and
  * `orders` hold ndims values (a negative sigma means no smoothing; an axis of size 1 is not

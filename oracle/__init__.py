@@ -182,6 +182,33 @@ def gauss_fir(x: np.ndarray, sigmas: Sequence[float] = (1.0,), orders: Sequence[
     return out
 
 
+def gauss_iir(x: np.ndarray, sigmas: Sequence[float] = (1.0,), orders: Sequence[int] = (0,),
+              bcs: Sequence[str] = (), filter_orders: Sequence[int] | None = None,
+              design: str = "discrete time fit", truncation: float = 3.0, out_dtype=None) -> np.ndarray:
+    """The restated dip::GaussIIR on a numpy array (parameters in DIPlib order, x first)."""
+    nd = x.ndim
+    sig = _broadcast(sigmas, nd, 1.0)
+    ords = _broadcast(orders, nd, 0)
+    bcl = _broadcast(bcs, nd, "mirror")
+    out_dt = suggest_flex(x.dtype) if out_dtype is None else np.dtype(out_dtype)
+    out = np.zeros(x.shape, out_dt)
+    sizes, in_strides = _dip_geometry(x)
+    _, out_strides = _dip_geometry(out)
+    fo = None if not filter_orders else (ctypes.c_uint * nd)(*_broadcast(filter_orders, nd, 3))
+    if design not in ("discrete time fit", "forward backward"):
+        raise ValueError("Invalid flag: " + design)
+    lib = oracle_lib()
+    lib.or_gauss_iir.restype = ctypes.c_int
+    st = lib.or_gauss_iir(
+        ctypes.c_void_p(x.ctypes.data), DTYPE_CODES[x.dtype], nd, sizes, in_strides,
+        ctypes.c_void_p(out.ctypes.data), DTYPE_CODES[out_dt], out_strides,
+        (ctypes.c_double * nd)(*sig), (ctypes.c_uint * nd)(*ords), (ctypes.c_int * nd)(*[bc_code(b) for b in bcl]),
+        fo, int(design == "forward backward"), ctypes.c_double(truncation))
+    if st != 0:
+        raise RuntimeError(f"or_gauss_iir failed ({st})")
+    return out
+
+
 SYMMETRIES = {"": 0, "general": 0, "even": 1, "odd": 2, "conj": 1, "d-even": 3, "d-odd": 4, "d-conj": 3}
 
 
@@ -564,6 +591,29 @@ def ref_gauss(x: np.ndarray, sigmas: Sequence[float] = (1.0,), orders: Sequence[
     if rc != 0:
         raise RuntimeError(errbuf.value.decode())
     if not protect and code.value != DTYPE_CODES[res_dt]:
+        raise RuntimeError(f"unexpected output type code {code.value}")
+    return out
+
+
+def ref_gauss_iir(x: np.ndarray, sigmas: Sequence[float] = (1.0,), orders: Sequence[int] = (0,),
+                  bcs: Sequence[str] | None = None, filter_orders: Sequence[int] = (),
+                  design: str = "discrete time fit", truncation: float = 3.0) -> np.ndarray:
+    """dip::GaussIIR of the reference on a numpy array (`bcs=None`: an empty array)."""
+    nd = x.ndim
+    sizes, st = _dip_geometry(x)
+    errbuf = ctypes.create_string_buffer(512)
+    sig, ords, fo = list(sigmas), list(orders), list(filter_orders)
+    out = np.zeros(x.shape, suggest_flex(x.dtype))
+    code = ctypes.c_int(0)
+    bc_str = "\n".join(bcs) if bcs else ""
+    rc = ref_lib().dipref_gauss_iir(
+        ctypes.c_void_p(x.ctypes.data), DTYPE_CODES[x.dtype], nd, sizes, st,
+        (ctypes.c_double * max(1, len(sig)))(*sig), len(sig), (ctypes.c_uint32 * max(1, len(ords)))(*ords), len(ords),
+        bc_str.encode(), int(bcs is not None and len(bcs) > 0), (ctypes.c_uint32 * max(1, len(fo)))(*fo), len(fo),
+        design.encode(), ctypes.c_double(truncation), ctypes.c_void_p(out.ctypes.data), ctypes.byref(code), errbuf, 512)
+    if rc != 0:
+        raise RuntimeError(errbuf.value.decode())
+    if code.value != DTYPE_CODES[out.dtype]:
         raise RuntimeError(f"unexpected output type code {code.value}")
     return out
 

@@ -685,16 +685,21 @@ static void uniform_line_##SUFFIX( T const* in, T* out, size_t length, size_t fi
 DEFINE_GENERAL_LINE( f32, float )
 DEFINE_GENERAL_LINE( f64, double )
 
+typedef struct or_iir_params or_iir_params;
+static void iir_line( double const* in, double* out, size_t length, or_iir_params const* P, double* p1 );
+
 /* Framework::Separable (framework_separable.cpp:35-431) around a per-axis line filter: kind 0 the
- * interned filters `F`, kind 1 the rectangular uniform filter of `usize[d]` samples. */
+ * interned filters `F`, kind 1 the rectangular uniform filter of `usize[d]` samples, kind 2 the
+ * recursive Gaussian of `I[d]` (a dfloat buffer whatever the input type, the filter writing the
+ * output buffer's border too: gaussiir.cpp:770-787). */
 static int separable_driver( void const* in, int in_dtype, int ndims, int64_t const* sizes, int64_t const* in_strides,
                              void* out, int out_dtype, int64_t const* out_strides, int const* process_in,
                              size_t const* border, int const* bcs, int kind, or_ifilter const* const* F,
-                             size_t const* usize ) {
+                             size_t const* usize, or_iir_params const* const* I ) {
    if( ndims < 1 || ndims > OR_MAX_DIMS || dtype_size( in_dtype ) == 0 || dtype_size( out_dtype ) == 0 ) {
       return OR_ERR_ARG;
    }
-   int buf_type = or_suggest_flex( in_dtype );
+   int buf_type = kind == 2 ? OR_DFLOAT : or_suggest_flex( in_dtype );
    int buf_double = ( buf_type == OR_DFLOAT );
    int process[ OR_MAX_DIMS ];
    size_t npix = 1;
@@ -742,7 +747,8 @@ static int separable_driver( void const* in, int in_dtype, int ndims, int64_t co
    }
    size_t esz = buf_double ? 8 : 4;
    char* inbuf = (char*)malloc( esz * ( maxlen + 2 * maxb ));
-   char* outbuf = (char*)malloc( esz * maxlen );
+   char* outbuf = (char*)malloc( esz * ( maxlen + 2 * maxb ));
+   double* scan = kind == 2 ? (double*)malloc( sizeof( double ) * ( maxlen + 2 * maxb )) : NULL;
    void const* src = in;
    int src_type = in_dtype;
    int64_t const* src_strides = in_strides;
@@ -766,7 +772,9 @@ static int separable_driver( void const* in, int in_dtype, int ndims, int64_t co
             double* o = (double*)outbuf;
             for( size_t i = 0; i < n; ++i ) { bb[ i ] = get_sample( src, src_type, so + (ptrdiff_t)i * src_strides[ pd ] ); }
             or_expand_buffer_f64( bb, 1, n, b, b, bcs[ pd ] );
-            if( kind == 0 ) { general_line_f64( bb, o, n, F[ pd ], F[ pd ]->f ); } else { uniform_line_f64( bb, o, n, usize[ pd ] ); }
+            if( kind == 0 ) { general_line_f64( bb, o, n, F[ pd ], F[ pd ]->f ); }
+            else if( kind == 1 ) { uniform_line_f64( bb, o, n, usize[ pd ] ); }
+            else { iir_line( bb - b, o, n + 2 * b, I[ pd ], scan ); o += b; }
             for( size_t i = 0; i < n; ++i ) { put_sample( dst, dst_type, dof + (ptrdiff_t)i * dst_strides[ pd ], o[ i ] ); }
          } else {
             float* bb = (float*)inbuf + b;
@@ -789,6 +797,7 @@ static int separable_driver( void const* in, int in_dtype, int ndims, int64_t co
    free( inbuf );
    free( outbuf );
    free( inter );
+   free( scan );
    return OR_OK;
 }
 
@@ -818,7 +827,7 @@ int or_separable_convolution( void const* in, int in_dtype, int ndims, int64_t c
                                                             ? f->f[ 0 ] == 1.0 : (float)f->f[ 0 ] == 1.0f ));
       if( meaningless ) { proc[ d ] = 0; }
    }
-   st = separable_driver( in, in_dtype, ndims, sizes, in_strides, out, out_dtype, out_strides, proc, border, bcs, 0, F, NULL );
+   st = separable_driver( in, in_dtype, ndims, sizes, in_strides, out, out_dtype, out_strides, proc, border, bcs, 0, F, NULL, NULL );
    free( fs );
    return st;
 }
@@ -833,5 +842,310 @@ int or_uniform_rect( void const* in, int in_dtype, int ndims, int64_t const* siz
       usize[ d ] = proc[ d ] ? (size_t)filter_sizes[ d ] : 1;
       border[ d ] = proc[ d ] ? usize[ d ] / 2 : 0;
    }
-   return separable_driver( in, in_dtype, ndims, sizes, in_strides, out, out_dtype, out_strides, proc, border, bcs, 1, NULL, usize );
+   return separable_driver( in, in_dtype, ndims, sizes, in_strides, out, out_dtype, out_strides, proc, border, bcs, 1, NULL, usize, NULL );
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* dip::GaussIIR (src/linear/gaussiir.cpp)                                                     */
+/* ------------------------------------------------------------------------------------------ */
+
+#define OR_IIR_MAX 6
+
+typedef struct { double re, im; } or_cplx;
+
+static or_cplx cmul( or_cplx a, or_cplx b ) { or_cplx r = { a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re }; return r; }
+static or_cplx cadd( or_cplx a, or_cplx b ) { or_cplx r = { a.re + b.re, a.im + b.im }; return r; }
+
+/* GaussIIRParams, gaussiir.cpp:38-48. */
+struct or_iir_params {
+   size_t border;
+   size_t num[ 6 ], den[ 6 ];                      /* iir_order_num, iir_order_den */
+   double a1[ OR_IIR_MAX ], a2[ OR_IIR_MAX ], b1[ OR_IIR_MAX ], b2[ OR_IIR_MAX ];
+   double cc;
+};
+
+/* FillPoleCoefficients, gaussiir.cpp:84-211: pp[1..nn], pp[0].re = nn; *fb set to 1 when the
+ * forward-backward design is used. */
+static void iir_fill_poles( size_t nn, or_cplx* pp, unsigned order, int* fb ) {
+   static double const dtf5[ 3 ][ 10 ] = {
+      { 0.85991, 1.45235, 0.85991, -1.45235, 1.60953, 0.83009, 1.60953, -0.83009, 1.87040, 0.0 },
+      { 0.70237, 1.38717, 0.70237, -1.38717, 1.43280, 0.77903, 1.43280, -0.77903, 1.70346, 0.0 },
+      { 0.70381, 1.38271, 0.70381, -1.38271, 1.42239, 0.77978, 1.42239, -0.77978, 1.69319, 0.0 } };
+   static double const dtf4[ 3 ][ 8 ] = {
+      { 1.13231, 1.28122, 1.13231, -1.28122, 1.78532, 0.46766, 1.78532, -0.46766 },
+      { 1.04198, 1.25046, 1.04198, -1.25046, 1.69337, 0.45006, 1.69337, -0.45006 },
+      { 0.94576, 1.21364, 0.94576, -1.21364, 1.59892, 0.42668, 1.59892, -0.42668 } };
+   static double const dtf3[ 3 ][ 6 ] = {
+      { 1.41650, 1.00829, 1.41650, -1.00829, 1.86131, 0.0 },
+      { 1.32094, 0.97057, 1.32094, -0.97057, 1.77635, 0.0 },
+      { 1.21969, 0.91724, 1.21969, -0.91724, 1.69485, 0.0 } };
+   static double const dtf2[ 4 ] = { 1.69580, 0.59955, 1.69580, -0.59955 };
+   static double const fb5[ 10 ] = { 2.19406, 1.90251, 2.19406, -1.90251, 2.31029, 0.598022, 2.31029, -0.598022, 7.64071, 0.0 };
+   static double const fb4[ 8 ] = { 2.06954, 1.90416, 2.06954, -1.90416, 2.18403, 0.593635, 2.18403, -0.593635 };
+   static double const as3[ 6 ] = { 2.1078345, 1.4058574, 2.1078345, -1.4058574, 2.1668048, 0.0 };
+   double const* t = NULL;
+   size_t o = order > 2 ? 0 : order;       /* the tables' "default" rows are order 0 */
+   if( !*fb ) {
+      switch( nn ) {
+         case 5: t = dtf5[ o ]; break;
+         case 4: t = dtf4[ o ]; break;
+         case 3: t = dtf3[ o ]; break;
+         case 2: t = dtf2; break;
+         case 1: { static double const one[ 2 ] = { 2.0, 0.0 }; t = one; break; }
+         default: *fb = 1; nn = 3; t = as3; break;
+      }
+   } else {
+      switch( nn ) {
+         case 5: t = fb5; break;
+         case 4: t = fb4; break;
+         default: nn = 3; t = as3; break;
+      }
+   }
+   pp[ 0 ].re = (double)nn;
+   pp[ 0 ].im = 0.0;
+   for( size_t m = 1; m <= nn; ++m ) { pp[ m ].re = t[ 2 * ( m - 1 ) ]; pp[ m ].im = t[ 2 * ( m - 1 ) + 1 ]; }
+}
+
+/* A pole raised to 1/q in polar form, as q2sigma and the pole scaling (gaussiir.cpp:61-68, 318-323). */
+static or_cplx iir_pole_pow( or_cplx p, double q ) {
+   double modulus = sqrt( p.re * p.re + p.im * p.im );
+   double phase = atan( p.im / p.re );
+   modulus = exp( log( modulus ) / q );
+   phase = phase / q;
+   or_cplx r = { modulus * cos( phase ), modulus * sin( phase ) };
+   return r;
+}
+
+/* q2sigma, gaussiir.cpp:55-82. */
+static double iir_q2sigma( size_t nn, or_cplx const* pp, double q ) {
+   double var = 0.0;
+   for( size_t mm = 1; mm <= ( nn - ( nn & 1u )); mm += 2 ) {
+      or_cplx r = iir_pole_pow( pp[ mm ], q );
+      double d = 1 - 2 * r.re + r.re * r.re + r.im * r.im;
+      d *= d;
+      var += ( 4 * ( r.re + ( r.re - 2 ) * ( r.re * r.re + r.im * r.im ))) / d;
+   }
+   if( nn & 1u ) {
+      double re = iir_pole_pow( pp[ nn ], q ).re;
+      var += ( 2 * re ) / (( re - 1 ) * ( re - 1 ));
+   }
+   return sqrt( var );
+}
+
+/* FilterCoefficients, gaussiir.cpp:213-239: bb[nn - mm] accumulates the products of mm poles with
+ * decreasing indices, in the recursion's order. */
+static void iir_esym( size_t mm, size_t nn, or_cplx const* pp, size_t start, size_t stop, or_cplx tmp, or_cplx* bb ) {
+   if( start == mm && stop == nn ) {
+      tmp.re = 1.0; tmp.im = 0.0;
+      bb[ nn - mm ].re = 0.0; bb[ nn - mm ].im = 0.0;
+   }
+   if( start > 1 ) {
+      for( size_t ii = start; ii <= stop; ++ii ) { iir_esym( mm, nn, pp, start - 1, ii - 1, cmul( tmp, pp[ ii ] ), bb ); }
+   } else if( start == 1 ) {
+      for( size_t ii = start; ii <= stop; ++ii ) { bb[ nn - mm ] = cadd( cmul( tmp, pp[ ii ] ), bb[ nn - mm ] ); }
+   } else if( start == 0 && mm == 0 ) {
+      bb[ nn ].re = 1.0; bb[ nn ].im = 0.0;
+   }
+}
+
+/* FillGaussIIRParams, gaussiir.cpp:241-446. */
+static int iir_design( double sigma, unsigned order, size_t filter_order, int fb, double truncation, or_iir_params* P ) {
+   if( order > 4 ) { return OR_ERR_ORDER; }
+   if( truncation <= 0.0 ) { truncation = 3; }
+   truncation = truncation < max_gauss_truncation( 0 ) ? truncation : max_gauss_truncation( 0 );
+   memset( P, 0, sizeof( *P ));
+   size_t b = (size_t)( sigma * truncation + 0.5 );
+   P->border = b > 5 ? b : 5;
+   or_cplx pp[ 10 ];
+   iir_fill_poles( filter_order, pp, order, &fb );
+   size_t nn = (size_t)pp[ 0 ].re;
+   double q = 0;
+   if( fb ) {
+      double q0term = -sigma * sigma, q1term = 0.0, q2term = 0.0;
+      for( size_t mm = 1; mm <= ( nn - ( nn & 1u )); mm += 2 ) {
+         double re = pp[ mm ].re, im = pp[ mm ].im;
+         double t1 = 4 * ( -1 + 3 * re - 3 * re * re - im * im + re * ( re * re + im * im ));
+         double t2 = 4 * ( 1 - 2 * re + re * re - im * im );
+         double d = 1 - 2 * re + re * re + im * im;
+         d *= d;
+         q1term += t1 / d;
+         q2term += t2 / d;
+      }
+      if( nn & 1u ) {
+         double d = pp[ nn ].re - 1.0;
+         q1term += 2.0 / d;
+         q2term += 2.0 / ( d * d );
+      }
+      double t = sqrt( q1term * q1term - 4.0 * q2term * q0term );
+      double r1 = ( -q1term + t ) / ( 2 * q2term );
+      double r2 = ( -q1term - t ) / ( 2 * q2term );
+      q = r1 > r2 ? r1 : r2;
+      for( size_t mm = 1; mm <= nn; ++mm ) {
+         or_cplx np = { 1.0 + ( pp[ mm ].re - 1.0 ) / q, pp[ mm ].im / q };
+         pp[ mm ] = np;
+      }
+   } else {
+      q = sigma / 2.0;
+      double q0 = q;
+      double qs = iir_q2sigma( nn, pp, q );
+      size_t n_iter = 0;
+      while( fabs( sigma - qs ) > 0.000001 && n_iter < 100 ) {
+         q += q0 - qs / 2.0;
+         qs = iir_q2sigma( nn, pp, q );
+         ++n_iter;
+      }
+      for( size_t mm = 1; mm <= nn; ++mm ) { pp[ mm ] = iir_pole_pow( pp[ mm ], q ); }
+   }
+   or_cplx bb[ 10 ];
+   or_cplx zero = { 0.0, 0.0 };
+   for( size_t mm = 0; mm <= nn; ++mm ) { iir_esym( mm, nn, pp, mm, nn, zero, bb ); }
+   for( size_t mm = 0; mm <= nn; ++mm ) {
+      double s = pow( -1.0, (double)( nn - mm )) / bb[ 0 ].re;
+      bb[ nn - mm ].re *= s;
+      bb[ nn - mm ].im *= s;
+      P->b1[ nn - mm ] = P->b2[ nn - mm ] = bb[ nn - mm ].re;
+   }
+   P->cc = 0.0;
+   for( size_t mm = 0; mm <= nn; ++mm ) { P->cc += P->b1[ mm ]; }
+   P->cc = P->cc * P->cc;
+   P->den[ 0 ] = nn; P->den[ 1 ] = 1; P->den[ 2 ] = nn;
+   P->den[ 3 ] = nn; P->den[ 4 ] = 1; P->den[ 5 ] = nn;
+   static double const A1[ 5 ][ 3 ] = { { 1, 0, 0 }, { 0.5, 0, -0.5 }, { 1, -1, 0 }, { 1, -2, 1 }, { 1, -2, 1 } };
+   static double const A2[ 5 ][ 3 ] = { { 1, 0, 0 }, { 0, 1, 0 }, { -1, 1, 0 }, { -0.5, 0, 0.5 }, { 1, -2, 1 } };
+   for( int k = 0; k < 3; ++k ) { P->a1[ k ] = A1[ order ][ k ]; P->a2[ k ] = A2[ order ][ k ]; }
+   for( int j = 0; j < 6; ++j ) { P->num[ j ] = OR_IIR_MAX + 1; }
+   for( size_t jj = 0; jj < OR_IIR_MAX; ++jj ) {
+      if( P->a1[ jj ] != 0.0 && P->num[ 1 ] > OR_IIR_MAX ) { P->num[ 1 ] = jj; }
+      if( P->a2[ jj ] != 0.0 && P->num[ 4 ] > OR_IIR_MAX ) { P->num[ 4 ] = jj; }
+   }
+   for( size_t jj = OR_IIR_MAX; jj > 0; ) {
+      --jj;
+      if( P->a1[ jj ] != 0.0 && P->num[ 2 ] > OR_IIR_MAX ) { P->num[ 2 ] = jj; }
+      if( P->a2[ jj ] != 0.0 && P->num[ 5 ] > OR_IIR_MAX ) { P->num[ 5 ] = jj; }
+   }
+   P->num[ 0 ] = P->num[ 2 ];
+   P->num[ 3 ] = P->num[ 5 ];
+   return OR_OK;
+}
+
+/* GaussIIRLineFilter::Filter, gaussiir.cpp:465-712, restated: `in` and `out` are the whole
+ * buffers (border included, `length` samples), `p1` scratch of `length`.  The reference writes
+ * out the recursions of orders 3-5 for order 0 (both scans) and for the derivative forms of its
+ * default orders; those start from a constant history R (the first / last value over the
+ * coefficients' sum), the generic scans set their first `order` values to R instead.  After an
+ * unrolled scan the reference finishes the line with the generic form (the same arithmetic up to
+ * rounding of the derivative's difference, kept here as the reference has it). */
+static void iir_line( double const* p0, double* p2, size_t length, or_iir_params const* P, double* p1 ) {
+   double const* a1 = P->a1;
+   double const* a2 = P->a2;
+   double const* b1 = P->b1;
+   double const* b2 = P->b2;
+   double const c = P->cc;
+   size_t const* MA = P->num;
+   size_t const* AR = P->den;
+   size_t order1 = AR[ 0 ] > MA[ 0 ] ? AR[ 0 ] : MA[ 0 ];
+   size_t order2 = AR[ 3 ] > MA[ 3 ] ? AR[ 3 ] : MA[ 3 ];
+   int copy_f = MA[ 0 ] == 0 && a1[ 0 ] == 1.0;
+   int copy_b = MA[ 3 ] == 0 && a2[ 0 ] == 1.0;
+   double const dsum1 = 1.0 + b1[ 1 ] + b1[ 2 ] + b1[ 3 ] + b1[ 4 ] + b1[ 5 ];
+   double const dsum2 = 1.0 + b2[ 1 ] + b2[ 2 ] + b2[ 3 ] + b2[ 4 ] + b2[ 5 ];
+   size_t nn1 = AR[ 2 ];
+   /* forward: which written-out form applies */
+   int fform = 0;                    /* 0 generic, 1 copy, 2 half difference (order 1), 3 difference (order 2) */
+   if( order1 >= 3 && order1 <= 5 ) {
+      if( copy_f ) { fform = 1; }
+      else if( order1 == 4 && a1[ 0 ] == 0.5 && a1[ 1 ] == 0.0 && a1[ 2 ] == -0.5 && a1[ 3 ] == 0.0 ) { fform = 2; }
+      else if( order1 == 5 && a1[ 0 ] == 1.0 && a1[ 1 ] == -1.0 && a1[ 2 ] == 0.0 && a1[ 3 ] == 0.0 ) { fform = 3; }
+   }
+   double R;
+   size_t ii = 0, s = 0, stop = 0;
+   if( fform == 1 ) { R = p0[ 0 ] / dsum1; s = 0; }
+   else if( fform == 2 ) { R = ( p0[ 1 ] - p0[ 0 ] ) / dsum1; s = 2; }
+   else if( fform == 3 ) { R = ( p0[ 1 ] - p0[ 0 ] ) / dsum1; s = 1; }
+   else {
+      double val = 0.0;
+      for( size_t jj = MA[ 1 ]; jj <= MA[ 2 ]; ++jj ) { val += a1[ jj ] * p0[ MA[ 2 ] - jj ]; }
+      R = val / dsum1;
+      s = order1;
+   }
+   for( ii = 0; ii < s; ++ii ) { p1[ ii ] = R; }
+   stop = s;                         /* the written-out scan covers [s, stop) */
+   if( fform ) { while( stop < length - order1 ) { stop += order1; } }
+   for( ii = s; ii < length; ++ii ) {
+      double val;
+      if( ii < stop && fform == 1 ) { val = p0[ ii ]; }
+      else if( ii < stop && fform == 2 ) { val = 0.5 * ( p0[ ii ] - p0[ ii - 2 ] ); }
+      else if( ii < stop && fform == 3 ) { val = p0[ ii ] - p0[ ii - 1 ]; }
+      else if( copy_f ) { val = p0[ ii ]; }
+      else {
+         val = 0.0;
+         for( size_t jj = MA[ 1 ]; jj <= MA[ 2 ]; ++jj ) { val += a1[ jj ] * p0[ ii - jj ]; }
+      }
+      for( size_t jj = AR[ 1 ]; jj <= nn1; ++jj ) { val -= b1[ jj ] * ( ii >= jj ? p1[ ii - jj ] : R ); }
+      p1[ ii ] = val;
+   }
+   /* backward */
+   size_t nn2 = AR[ 5 ];
+   int bform = 0;
+   if( order2 >= 3 && order2 <= 5 ) {
+      if( copy_b ) { bform = 1; }
+      else if( order2 == 4 && a2[ 0 ] == 0.0 && a2[ 1 ] == 1.0 && a2[ 2 ] == 0.0 && a2[ 3 ] == 0.0 ) { bform = 2; }
+      else if( order2 == 5 && a2[ 0 ] == -1.0 && a2[ 1 ] == 1.0 && a2[ 2 ] == 0.0 && a2[ 3 ] == 0.0 ) { bform = 3; }
+   }
+   size_t top;                       /* p2[top + 1 .. length - 1] are set before the scan */
+   if( bform == 1 ) { R = c * p1[ length - 1 ] / dsum2; top = length - 1; }
+   else if( bform == 2 ) { R = c * p1[ length - 1 ] / dsum2; p2[ length - 1 ] = R; top = length - 2; }
+   else if( bform == 3 ) { R = c * ( -p1[ length - 2 ] + p1[ length - 1 ] ) / dsum2; p2[ length - 1 ] = R; top = length - 2; }
+   else {
+      double val = 0.0;
+      for( size_t jj = MA[ 4 ]; jj <= MA[ 5 ]; ++jj ) { val += a2[ jj ] * p1[ length - 1 - MA[ 5 ] + jj ]; }
+      R = val / dsum2;
+      for( ii = length - 1; ii > length - 1 - order2; --ii ) { p2[ ii ] = c * R; }
+      top = length - 1 - order2;
+   }
+   /* the written-out scan covers (low, top]: steps of order2 while the step's start is >= order2 */
+   size_t low = top + 1;
+   if( bform ) {
+      size_t i = top;
+      while( i >= order2 ) { i -= order2; }
+      low = i + 1;                   /* samples below `low` take the generic form */
+      if( top < order2 ) { low = top + 1; }
+   }
+   for( size_t k = top + 1; k-- > 0; ) {
+      double val;
+      int wo = bform && k >= low;
+      if( wo && bform == 1 ) { val = c * p1[ k ]; }
+      else if( wo && bform == 2 ) { val = c * p1[ k + 1 ]; }
+      else if( wo && bform == 3 ) { val = c * ( -p1[ k ] + p1[ k + 1 ] ); }
+      else if( copy_b ) { val = c * p1[ k ]; }
+      else {
+         val = 0.0;
+         for( size_t jj = MA[ 4 ]; jj <= MA[ 5 ]; ++jj ) { val += a2[ jj ] * p1[ k + jj ]; }
+         val = c * val;
+      }
+      for( size_t jj = AR[ 4 ]; jj <= nn2; ++jj ) { val -= b2[ jj ] * ( k + jj < length ? p2[ k + jj ] : R ); }
+      p2[ k ] = val;
+   }
+}
+
+int or_gauss_iir( void const* in, int in_dtype, int ndims, int64_t const* sizes, int64_t const* in_strides,
+                  void* out, int out_dtype, int64_t const* out_strides, double const* sigmas, unsigned const* orders,
+                  int const* bcs, unsigned const* filter_orders, int forward_backward, double truncation ) {
+   if( ndims < 1 || ndims > OR_MAX_DIMS ) { return OR_ERR_ARG; }
+   or_iir_params P[ OR_MAX_DIMS ];
+   or_iir_params const* I[ OR_MAX_DIMS ];
+   int proc[ OR_MAX_DIMS ];
+   size_t border[ OR_MAX_DIMS ];
+   for( int d = 0; d < ndims; ++d ) {
+      proc[ d ] = sigmas[ d ] > 0.0 && sizes[ d ] > 1;
+      border[ d ] = 0;
+      I[ d ] = &P[ d ];
+      if( !proc[ d ] ) { continue; }
+      size_t fo = filter_orders ? filter_orders[ d ] : ( orders[ d ] > 2 ? 5 : orders[ d ] + 3 );
+      int st = iir_design( sigmas[ d ], orders[ d ], fo, forward_backward, truncation, &P[ d ] );
+      if( st != OR_OK ) { return st; }
+      border[ d ] = P[ d ].border;
+   }
+   return separable_driver( in, in_dtype, ndims, sizes, in_strides, out, out_dtype, out_strides, proc, border, bcs,
+                            2, NULL, NULL, I );
 }

@@ -87,6 +87,13 @@ int or_uniform_rect( void const* in, int in_dtype, int ndims, int64_t const* siz
 /* Output/compute type rule: DataType::SuggestFlex, src/library/datatype.cpp:109-124. */
 int or_suggest_flex( int dtype );
 
+/* dip::GaussIIR (src/linear/gaussiir.cpp:725-790): recursive Gaussian (derivative) filter, orders
+ * 0-4, computed in dfloat.  `filter_orders` NULL: the reference's defaults; `forward_backward` 0:
+ * "discrete time fit", 1: "forward backward". */
+int or_gauss_iir( void const* in, int in_dtype, int ndims, int64_t const* sizes, int64_t const* in_strides,
+                  void* out, int out_dtype, int64_t const* out_strides, double const* sigmas, unsigned const* orders,
+                  int const* bcs, unsigned const* filter_orders, int forward_backward, double truncation );
+
 #ifdef __cplusplus
 }
 #endif

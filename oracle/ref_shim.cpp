@@ -9,6 +9,7 @@
 //   dip::detail::ExpandBuffer src/library/copy_buffer.cpp:751-813
 //   dip::ReadPixelWithBoundaryCondition src/library/boundary.cpp:47-128
 //   dip::SeparableConvolution src/linear/convolution.cpp:319-421, dip::Uniform src/linear/uniform.cpp:147-163
+//   dip::GaussIIR            src/linear/gaussiir.cpp:725-790
 //
 // Sizes and strides are given in DIPlib order (x first), in samples.  Data type codes are the
 // ones of include/dipcu.h (DIPCU_BIN .. DIPCU_DFLOAT).  Every entry point returns 0 on success
@@ -208,6 +209,33 @@ int dipref_gauss(
          *out_dtype = TypeToCode( res.DataType() );
          CopyOut( res, out );
       }
+      return 0;
+   } catch( dip::Error const& e ) {
+      SetErr( err, errlen, e.what() );
+      return 1;
+   }
+}
+
+// dip::GaussIIR: per-axis sigmas / orders (nsigmas / norders values, broadcast by the reference),
+// `forders` (nforders values, 0: the reference's defaults), `design` the design-method string.
+// The output (the reference's own, normal strides) goes to `out`, its type to *out_dtype.
+int dipref_gauss_iir(
+      void const* in, int in_dtype, int ndims, int64_t const* sizes, int64_t const* strides,
+      double const* sigmas, int nsigmas, uint32_t const* orders, int norders, char const* bcs, int has_bcs,
+      uint32_t const* forders, int nforders, char const* design, double truncation,
+      void* out, int* out_dtype, char* err, int errlen ) {
+   try {
+      dip::Image img = Wrap( in, in_dtype, ndims, sizes, strides );
+      dip::FloatArray s( static_cast< dip::uint >( nsigmas ));
+      for( int ii = 0; ii < nsigmas; ++ii ) { s[ ii ] = sigmas[ ii ]; }
+      dip::UnsignedArray o( static_cast< dip::uint >( norders ));
+      for( int ii = 0; ii < norders; ++ii ) { o[ ii ] = orders[ ii ]; }
+      dip::UnsignedArray fo( static_cast< dip::uint >( nforders ));
+      for( int ii = 0; ii < nforders; ++ii ) { fo[ ii ] = forders[ ii ]; }
+      dip::Image res;
+      dip::GaussIIR( img, res, s, o, SplitList( bcs, has_bcs != 0 ), fo, design, truncation );
+      *out_dtype = TypeToCode( res.DataType() );
+      CopyOut( res, out );
       return 0;
    } catch( dip::Error const& e ) {
       SetErr( err, errlen, e.what() );

@@ -180,6 +180,7 @@ def test_gauss_best_method_dispatch(cuda):
     assert_close(dip().Gauss(x, [2.0], [0], "gaussFIR"), ref, x, "gaussFIR")
     # sigma < 0.8 resolves to the FT method ("default" boundary condition), sigma > 10 to IIR
     assert_close(dip().Gauss(x, [0.5]), oracle.gauss_ft(x, [0.5], [0], 3.0, ["mirror"]), x, "best -> FT")
+    assert_close(dip().Gauss(x, [12.0], [1]), oracle.gauss_iir(x, [12.0], [1], ["mirror"]), x, "best -> IIR")
 
 
 def test_device_weights_match_oracle(cuda):
