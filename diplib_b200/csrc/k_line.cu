@@ -14,6 +14,7 @@
 // smallest-stride axis share a CTA so that global accesses stay coalesced.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdlib>
 
 #include "dipcu_common.cuh"
@@ -127,6 +128,12 @@ __global__ void __launch_bounds__( 256 ) line_pass_kernel( LineArgs< T, MAXH1 > 
 //     each owns one column and evaluates R_Y consecutive outputs along the processed axis from a
 //     register window of R_Y + 2 HB samples read straight from global memory (the window overlap
 //     of neighbouring blocks is served by L1/L2).
+//   * Along any other axis, vectorised (line_y4_kernel), where both images keep 16-byte alignment
+//     across the unit-stride axis: each thread owns a group of 4 adjacent columns and marches its
+//     z-chunk (the processed axis) in steps of RZ outputs: the step's RZ + 2 HB rows are read as
+//     float4 (one 16-byte load per row; the overlap with the previous step hits L1) and scattered
+//     into RZ float4 accumulators with the full (unfolded, sign-expanded) kernel taken from the
+//     kernel parameters, h exact up to 12 (buckets above).
 
 constexpr int kFastMaxH = 32;
 constexpr int kRX = 4;    // outputs per thread, line_x_kernel
@@ -296,6 +303,284 @@ __global__ void __launch_bounds__( 128 ) line_y_kernel( LineFastArgs const __gri
    }
 }
 
+struct LineY4Args {
+   float const* src;
+   float* dst;
+   int64_t n;                  // length along the processed axis
+   int64_t sa, da;             // strides along it (multiples of 4 samples)
+   int64_t ncomp4;             // 4-column groups along the unit-stride axis
+   int64_t ncols;              // ncomp4 x outer lines
+   int64_t chunk;              // outputs per thread along the axis (a multiple of RZ)
+   int32_t bc;
+   int32_t nod;
+   int64_t osz[ DIPCU_MAX_DIMS ], osst[ DIPCU_MAX_DIMS ], odst[ DIPCU_MAX_DIMS ];
+   float w[ 2 * kFastMaxH + 1 ];   // tap j (-h..h) at w[kFastMaxH + j]: sign-expanded, zero beyond h
+};
+
+template< int HB, int RZ >
+__global__ void __launch_bounds__( 128, HB <= 12 ? 3 : 2 ) line_y4_kernel( LineY4Args const __grid_constant__ a ) {
+   int64_t const col = static_cast< int64_t >( blockIdx.x ) * blockDim.x + threadIdx.x;
+   if( col >= a.ncols ) { return; }
+   int64_t const c4 = col % a.ncomp4;
+   int64_t u = col / a.ncomp4, sb = 4 * c4, db = 4 * c4;
+   for( int d = 0; d < a.nod; ++d ) {
+      int64_t const c = u % a.osz[ d ];
+      u /= a.osz[ d ];
+      sb += c * a.osst[ d ];
+      db += c * a.odst[ d ];
+   }
+   float const* const src = a.src + sb;
+   float* const dst = a.dst + db;
+   int64_t const zb = static_cast< int64_t >( blockIdx.y ) * a.chunk;
+   int64_t const ze = zb + a.chunk < a.n ? zb + a.chunk : a.n;
+   for( int64_t z0 = zb; z0 < ze; z0 += RZ ) {
+      float4 acc[ RZ ];
+#pragma unroll
+      for( int r = 0; r < RZ; ++r ) { acc[ r ] = make_float4( 0.f, 0.f, 0.f, 0.f ); }
+      bool const interior = z0 - HB >= 0 && z0 + RZ + HB <= a.n;
+      // every row of the step in flight before the arithmetic (windows up to 48 rows; longer
+      // kernels read each row as they go, their arithmetic covers the latency)
+      constexpr int NW = RZ + 2 * HB <= 48 ? RZ + 2 * HB : 1;
+      float4 win[ NW ];
+      auto row = [ & ]( int i ) -> float4 {
+         int64_t zi = z0 - HB + i;
+         if( interior ) { return __ldg( reinterpret_cast< float4 const* >( src + zi * a.sa )); }
+         bool neg = false;
+         if( zi < 0 || zi >= a.n ) { zi = a.bc == BC_ADD_ZEROS ? -1 : bc_map_index( zi, a.n, a.bc, &neg ); }
+         float4 const v = zi < 0 ? make_float4( 0.f, 0.f, 0.f, 0.f ) : __ldg( reinterpret_cast< float4 const* >( src + zi * a.sa ));
+         return neg ? make_float4( -v.x, -v.y, -v.z, -v.w ) : v;
+      };
+      if( NW == 1 ) {
+      } else if( interior ) {
+         float const* p = src + ( z0 - HB ) * a.sa;
+#pragma unroll
+         for( int i = 0; i < NW; ++i ) { win[ i ] = __ldg( reinterpret_cast< float4 const* >( p + i * a.sa )); }
+      } else {
+#pragma unroll
+         for( int i = 0; i < NW; ++i ) { win[ i ] = row( i ); }
+      }
+#pragma unroll
+      for( int i = 0; i < RZ + 2 * HB; ++i ) {
+         float4 const v = NW == 1 ? row( i ) : win[ i < NW ? i : 0 ];
+#pragma unroll
+         for( int r = 0; r < RZ; ++r ) {
+            int const j = i - HB - r;
+            if( j < -HB || j > HB ) { continue; }
+            float const w = a.w[ kFastMaxH + j ];
+            acc[ r ].x = fmaf( w, v.x, acc[ r ].x );
+            acc[ r ].y = fmaf( w, v.y, acc[ r ].y );
+            acc[ r ].z = fmaf( w, v.z, acc[ r ].z );
+            acc[ r ].w = fmaf( w, v.w, acc[ r ].w );
+         }
+      }
+#pragma unroll
+      for( int r = 0; r < RZ; ++r ) {
+         if( z0 + r < ze ) { *reinterpret_cast< float4* >( dst + ( z0 + r ) * a.da ) = acc[ r ]; }
+      }
+   }
+}
+
+int sm_count_line() {
+   static std::atomic< int > n{ 0 };
+   if( n.load() == 0 ) {
+      int dev = 0, v = 0;
+      cudaGetDevice( &dev );
+      cudaDeviceGetAttribute( &v, cudaDevAttrMultiProcessorCount, dev );
+      n.store( v > 0 ? v : 148 );
+   }
+   return n.load();
+}
+
+// Ring variant of line_y4_kernel for half-widths up to 10 and the boundary conditions that keep
+// the sample's sign: each thread streams its own column group's rows into a private ring of
+// kY4Ring shared-memory rows with 16-byte asynchronous copies (zero fill for "add zeros"), kY4Pd
+// blocks of RZ4 rows ahead of the block it computes, so every row is read from memory once per
+// chunk and the copies in flight need no registers.  A thread reads only its own ring slots, so
+// cp.async.wait_group is the only synchronisation.
+constexpr int kY4Ring = 32;         // ring rows per thread (16 bytes each)
+constexpr int kY4Rz = 4;            // outputs per step
+constexpr int kY4Pd = 2;            // blocks in flight beyond the step's window (deeper rings with
+                                    // fewer threads per SM measured slower)
+constexpr int kY4Threads = 128;     // 64 KB of ring per CTA, 3 CTAs per SM
+
+template< int HB >
+__global__ void __launch_bounds__( kY4Threads ) line_y4r_kernel( LineY4Args const __grid_constant__ a ) {
+   constexpr int RZ = kY4Rz, NBW = ( 2 * HB + RZ + RZ - 1 ) / RZ;     // blocks a step reads
+   static_assert(( NBW + kY4Pd ) * RZ <= kY4Ring, "ring holds the window and the blocks in flight" );
+   extern __shared__ __align__( 16 ) float4 y4ring[];    // [kY4Ring][kY4Threads]
+   int const tid = static_cast< int >( threadIdx.x );
+   int64_t const col = static_cast< int64_t >( blockIdx.x ) * kY4Threads + tid;
+   bool const live = col < a.ncols;
+   int64_t sb = 0, db = 0;
+   if( live ) {
+      int64_t const c4 = col % a.ncomp4;
+      int64_t u = col / a.ncomp4;
+      sb = 4 * c4;
+      db = 4 * c4;
+      for( int d = 0; d < a.nod; ++d ) {
+         int64_t const c = u % a.osz[ d ];
+         u /= a.osz[ d ];
+         sb += c * a.osst[ d ];
+         db += c * a.odst[ d ];
+      }
+   }
+   float const* const src = a.src + sb;
+   float* const dst = a.dst + db;
+   int64_t const zb = static_cast< int64_t >( blockIdx.y ) * a.chunk;
+   int64_t const ze = zb + a.chunk < a.n ? zb + a.chunk : a.n;
+   int64_t const nsteps = ( ze - zb + RZ - 1 ) / RZ;
+   // block q: rows zb - HB + q RZ .. + RZ - 1, ring slots (q RZ + i) mod kY4Ring
+   auto issue = [ & ]( int64_t q ) {
+      if( live && q < nsteps + NBW - 1 ) {
+#pragma unroll
+         for( int i = 0; i < RZ; ++i ) {
+            int64_t z = zb - HB + q * RZ + i;
+            int bytes = 16;
+            if( z < 0 || z >= a.n ) {
+               if( a.bc == BC_ADD_ZEROS ) { bytes = 0; z = 0; }
+               else { bool neg; z = bc_map_index( z, a.n, a.bc, &neg ); }
+            }
+            float4* const slot = &y4ring[ (( q * RZ + i ) & ( kY4Ring - 1 )) * kY4Threads + tid ];
+            asm volatile( "cp.async.cg.shared.global [%0], [%1], 16, %2;" :: "r"( smem_u32( slot )),
+                          "l"( src + z * a.sa ), "r"( bytes ) : "memory" );
+         }
+      }
+      asm volatile( "cp.async.commit_group;" ::: "memory" );
+   };
+#pragma unroll
+   for( int q = 0; q < NBW + kY4Pd - 1; ++q ) { issue( q ); }
+   for( int64_t s = 0; s < nsteps; ++s ) {
+      issue( s + NBW + kY4Pd - 1 );
+      asm volatile( "cp.async.wait_group %0;" :: "n"( kY4Pd ) : "memory" );
+      if( !live ) { continue; }
+      float4 acc[ RZ ];
+#pragma unroll
+      for( int r = 0; r < RZ; ++r ) { acc[ r ] = make_float4( 0.f, 0.f, 0.f, 0.f ); }
+      int const base = static_cast< int >(( s * RZ ) & ( kY4Ring - 1 ));
+#pragma unroll
+      for( int i = 0; i < RZ + 2 * HB; ++i ) {
+         float4 const v = y4ring[ (( base + i ) & ( kY4Ring - 1 )) * kY4Threads + tid ];
+#pragma unroll
+         for( int r = 0; r < RZ; ++r ) {
+            int const j = i - HB - r;
+            if( j < -HB || j > HB ) { continue; }
+            float const w = a.w[ kFastMaxH + j ];
+            acc[ r ].x = fmaf( w, v.x, acc[ r ].x );
+            acc[ r ].y = fmaf( w, v.y, acc[ r ].y );
+            acc[ r ].z = fmaf( w, v.z, acc[ r ].z );
+            acc[ r ].w = fmaf( w, v.w, acc[ r ].w );
+         }
+      }
+      int64_t const z0 = zb + s * RZ;
+#pragma unroll
+      for( int r = 0; r < RZ; ++r ) {
+         if( z0 + r < ze ) { *reinterpret_cast< float4* >( dst + ( z0 + r ) * a.da ) = acc[ r ]; }
+      }
+   }
+   asm volatile( "cp.async.wait_group 0;" ::: "memory" );
+}
+
+template< int HB >
+cudaError_t launch_y4r( LineY4Args& a, cudaStream_t stream ) {
+   // chunks along the axis for ~14 resident warps per SM over the column groups
+   int64_t const want = static_cast< int64_t >( sm_count_line()) * 14 * 32;
+   int64_t nch = ( want + a.ncols - 1 ) / a.ncols;
+   int64_t const maxch = ( a.n + kY4Rz - 1 ) / kY4Rz;
+   nch = nch < 1 ? 1 : ( nch > maxch ? maxch : nch );
+   a.chunk = (( a.n + nch - 1 ) / nch + kY4Rz - 1 ) / kY4Rz * kY4Rz;
+   nch = ( a.n + a.chunk - 1 ) / a.chunk;
+   int64_t const gx = ( a.ncols + kY4Threads - 1 ) / kY4Threads;
+   if( gx > 0x7fffffff || nch > 65535 ) { return cudaErrorNotSupported; }
+   constexpr int smem = kY4Ring * kY4Threads * 16;
+   {
+      // the opt-in above the 48 KB default, once per device
+      static std::atomic< uint64_t > done{ 0 };
+      int dev = 0;
+      cudaGetDevice( &dev );
+      uint64_t const bit = 1ull << ( dev & 63 );
+      if( !( done.load() & bit )) {
+         if( cudaFuncSetAttribute( line_y4r_kernel< HB >, cudaFuncAttributeMaxDynamicSharedMemorySize, smem ) != cudaSuccess ) {
+            cudaGetLastError();
+            return cudaErrorNotSupported;
+         }
+         done.fetch_or( bit );
+      }
+   }
+   line_y4r_kernel< HB ><<< dim3( static_cast< unsigned >( gx ), static_cast< unsigned >( nch )), kY4Threads, smem, stream >>>( a );
+   count_launch();
+   return cudaGetLastError();
+}
+
+template< int HB >
+cudaError_t launch_y4_bucket( LineY4Args& a, cudaStream_t stream ) {
+   if constexpr( HB <= 10 ) {
+      if( a.bc == BC_SYMMETRIC_MIRROR || a.bc == BC_PERIODIC || a.bc == BC_ZERO_ORDER_EXTRAPOLATE || a.bc == BC_ADD_ZEROS ) {
+         return launch_y4r< HB >( a, stream );
+      }
+   }
+   constexpr int RZ = HB <= 12 ? 8 : 16;
+   // enough threads for ~16 warps per SM over the chunks along the axis
+   int64_t const want = 148 * 16 * 32;
+   int64_t nch = ( want + a.ncols - 1 ) / a.ncols;
+   int64_t const maxch = ( a.n + RZ - 1 ) / RZ;
+   nch = nch < 1 ? 1 : ( nch > maxch ? maxch : nch );
+   a.chunk = (( a.n + nch - 1 ) / nch + RZ - 1 ) / RZ * RZ;
+   nch = ( a.n + a.chunk - 1 ) / a.chunk;
+   int64_t const gx = ( a.ncols + 127 ) / 128;
+   if( gx > 0x7fffffff || nch > 65535 ) { return cudaErrorNotSupported; }
+   line_y4_kernel< HB, RZ ><<< dim3( static_cast< unsigned >( gx ), static_cast< unsigned >( nch )), 128, 0, stream >>>( a );
+   count_launch();
+   return cudaGetLastError();
+}
+
+// The vectorised outer-axis pass, or cudaErrorNotSupported when the layout does not keep every
+// 4-column group 16-byte aligned in both images.
+cudaError_t launch_line_y4( LineFastArgs const& f, cudaStream_t stream ) {
+   if( f.comp < 0 || f.ncomp % 4 != 0 || ( reinterpret_cast< uintptr_t >( f.src ) & 15 ) ||
+       ( reinterpret_cast< uintptr_t >( f.dst ) & 15 )) {
+      return cudaErrorNotSupported;
+   }
+   LineY4Args a{};
+   a.src = f.src;
+   a.dst = f.dst;
+   a.n = f.n;
+   a.sa = f.sst[ f.axis ];
+   a.da = f.dstst[ f.axis ];
+   if( a.sa % 4 || a.da % 4 || a.sa <= 0 ) { return cudaErrorNotSupported; }
+   a.ncomp4 = f.ncomp / 4;
+   a.ncols = a.ncomp4 * f.nouter;
+   a.bc = f.bc;
+   a.nod = f.nod;
+   for( int d = 0; d < f.nod; ++d ) {
+      if( f.osst[ d ] % 4 || f.odst[ d ] % 4 ) { return cudaErrorNotSupported; }
+      a.osz[ d ] = f.osz[ d ];
+      a.osst[ d ] = f.osst[ d ];
+      a.odst[ d ] = f.odst[ d ];
+   }
+   for( int j = -kFastMaxH; j <= kFastMaxH; ++j ) {
+      int const k = j < 0 ? -j : j;
+      float const t = k <= f.h ? f.taps[ k ] : 0.f;
+      a.w[ kFastMaxH + j ] = ( f.odd && j < 0 ) ? -t : t;
+   }
+   switch( f.h ) {
+      case 0: case 1: return launch_y4_bucket< 1 >( a, stream );
+      case 2: return launch_y4_bucket< 2 >( a, stream );
+      case 3: return launch_y4_bucket< 3 >( a, stream );
+      case 4: return launch_y4_bucket< 4 >( a, stream );
+      case 5: return launch_y4_bucket< 5 >( a, stream );
+      case 6: return launch_y4_bucket< 6 >( a, stream );
+      case 7: return launch_y4_bucket< 7 >( a, stream );
+      case 8: return launch_y4_bucket< 8 >( a, stream );
+      case 9: return launch_y4_bucket< 9 >( a, stream );
+      case 10: return launch_y4_bucket< 10 >( a, stream );
+      case 11: return launch_y4_bucket< 11 >( a, stream );
+      case 12: return launch_y4_bucket< 12 >( a, stream );
+      default:
+         return f.h <= 16 ? launch_y4_bucket< 16 >( a, stream ) : f.h <= 24 ? launch_y4_bucket< 24 >( a, stream )
+                                                                 : launch_y4_bucket< 32 >( a, stream );
+   }
+}
+
 // CTA width (32, 64 or 128 threads) that leaves the fewest idle threads for `n` items of
 // `per` outputs per thread; the widest on ties.
 int fast_width( int64_t n, int per ) {
@@ -384,6 +669,10 @@ cudaError_t launch_line_fast( LinePass const& p, cudaStream_t stream ) {
       a.osz[ 0 ] = 1;
       a.osst[ 0 ] = 0;
       a.odst[ 0 ] = 0;
+   }
+   if( !along ) {
+      cudaError_t const e = launch_line_y4( a, stream );
+      if( e != cudaErrorNotSupported ) { return e; }
    }
    // Buckets at the half-widths of sigma 4 and 8 with order 0 (12, 24) as well as the powers of two.
    int const hb = p.h <= 4 ? 4 : p.h <= 8 ? 8 : p.h <= 12 ? 12 : p.h <= 16 ? 16 : p.h <= 24 ? 24 : 32;
