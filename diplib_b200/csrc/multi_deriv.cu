@@ -8,7 +8,8 @@
 //      axis, or zeros), is read once into shared memory as float (batches of loads in flight);
 //   2. z passes: every z order any component needs, over the tile's x-y halo region (each thread
 //      one (x, y) column, its z window in registers, all z orders from one load of the window);
-//   3. y passes: every (y order, z order) pair any component needs, over the x halo region;
+//   3. y passes: every (y order, z order) pair any component needs, over the x halo region (a
+//      thread per column and segment of 8 rows);
 //   4. x passes: each thread a segment of 8 outputs of one row, every component from the
 //      y-filtered buffers, then the epilogue: the components themselves, their symmetric products
 //      (DIPlib's symmetric-matrix order), their sum, or the square root of the sum of squares.
@@ -36,6 +37,7 @@ constexpr int kMdTX = 32;        // tile width
 constexpr int kMdR = 8;          // outputs per thread in the x pass
 constexpr int kMdThreads = 256;
 constexpr int kMdLoadBatch = 8;  // tile elements per thread whose loads are in flight together
+constexpr int kMdYS = 8;         // rows per thread in the y pass
 
 struct MdArgs {
    void const* src;
@@ -148,24 +150,25 @@ __global__ void __launch_bounds__( kMdThreads ) multi_deriv_kernel( MdArgs const
       __syncthreads();
    }
 
-   // 3. y passes: column (i, z) of the x halo region, every (y, z) pair
-   for( int col = tid; col < W0 * TZ; col += kMdThreads ) {
-      int const i = col % W0, z = col / W0;
+   // 3. y passes: column (i, z) of the x halo region and a segment of kMdYS rows, every (y, z) pair
+   constexpr int YSEG = TY / kMdYS;
+   for( int task = tid; task < W0 * TZ * YSEG; task += kMdThreads ) {
+      int const i = task % W0, z = ( task / W0 ) % TZ, ys = task / ( W0 * TZ );
       for( int s = 0; s < ( TZ > 1 ? a.nord[ 2 ] : 1 ); ++s ) {
          bool need = false;
          for( int b = 0; b < a.ncombo; ++b ) { need = need || a.combo_z[ b ] == s; }
          if( !need ) { continue; }
-         float v[ W1 ];
-         float const* const src = za + ( s * TZ + z ) * W0 * W1 + i;
+         float v[ kMdYS + 2 * HB ];
+         float const* const src = za + ( s * TZ + z ) * W0 * W1 + ys * kMdYS * W0 + i;
 #pragma unroll
-         for( int j = 0; j < W1; ++j ) { v[ j ] = src[ j * W0 ]; }
+         for( int j = 0; j < kMdYS + 2 * HB; ++j ) { v[ j ] = src[ j * W0 ]; }
          for( int b = 0; b < a.ncombo; ++b ) {
             if( a.combo_z[ b ] != s ) { continue; }
             float const* const tp = a.taps[ 1 ][ a.combo_y[ b ]];
             bool const odd = a.fodd[ 1 ][ a.combo_y[ b ]] != 0;
-            float* const dst = yb + ( b * TZ + z ) * TY * YP + i;
+            float* const dst = yb + ( b * TZ + z ) * TY * YP + ys * kMdYS * YP + i;
 #pragma unroll
-            for( int y = 0; y < TY; ++y ) { dst[ y * YP ] = md_tap< HB >( v, y + HB, tp, odd ); }
+            for( int y = 0; y < kMdYS; ++y ) { dst[ y * YP ] = md_tap< HB >( v, y + HB, tp, odd ); }
          }
       }
    }
@@ -370,7 +373,7 @@ int multi_gauss_fir( dipcu_image_desc const* in, dipcu_image_desc const* outs, i
       for( int d = 0; d < 3; ++d ) { a.ds[ q ][ d ] = d < in->ndims ? outs[ q ].strides[ d ] : 0; }
    }
    if( in->ndims == 3 ) { return hb == 4 ? md_run< 4, 8, 8 >( a, stream ) : md_run< 8, 8, 4 >( a, stream ); }
-   return hb == 4 ? md_run< 4, 16, 1 >( a, stream ) : md_run< 8, 16, 1 >( a, stream );
+   return hb == 4 ? md_run< 4, 64, 1 >( a, stream ) : md_run< 8, 64, 1 >( a, stream );
 }
 
 bool multi_gauss_fir_supported( dipcu_image_desc const* in, uint32_t const* orders, int ncomp, double const* sigmas,

@@ -1,10 +1,15 @@
 """dip::Gradient, dip::GradientMagnitude, dip::Hessian and dip::Laplace (src/linear/derivative.cpp)
-with the Gaussian methods, on the B200 Gaussian FIR path.  Where the multi-output tile kernel takes
-the case (2D/3D input computed in sfloat, index-mapping or "add zeros" boundary conditions,
-half-widths up to 8, all components resolving to the FIR method) every component, or their sum
-(Laplace) or root of the summed squares (GradientMagnitude), comes from ONE launch that reads the
-input once (``dipcu_gauss_fir_multi``); otherwise each component is one GaussFIR call through the
-C-ABI, written straight into its slice of the output, as the reference computes them.
+with the Gaussian methods, on the B200 Gaussian FIR path: each component is one GaussFIR call
+through the C-ABI, written straight into its slice of the output, as the reference computes them.
+
+``USE_MULTI_OUTPUT = True`` routes the cases the multi-output tile kernel takes (2D/3D input
+computed in sfloat, index-mapping or "add zeros" boundary conditions, half-widths up to 8, all
+components resolving to the FIR method) through ONE launch that reads the input once
+(``dipcu_gauss_fir_multi``): every component, or their sum (Laplace) or root of the summed squares
+(GradientMagnitude).  It is off by default because on a B200 that kernel is slower than one
+launch of the tile kernels per component (4096^2 Gradient: 318 against 87 us; 192^3: 472 against
+130 us): its generic per-tile passes cost more instructions than the second read of the input
+saves.
 
 Tensor outputs come back planar, the component axis first: ``Gradient`` gives ``(m,) + shape``
 for the m axes FindGradientDimensions keeps; ``Hessian`` gives ``(m(m+1)/2,) + shape`` in DIPlib's
@@ -59,12 +64,16 @@ def _order(nd: int, counts: dict) -> list:
 # dipcu_gauss_fir_multi modes
 _COMPONENTS, _PRODUCTS, _SUM, _MAGNITUDE = 0, 1, 2, 3
 
+USE_MULTI_OUTPUT = False
+
 
 def _multi(x: torch.Tensor, orders: list, mode: int, sg: list, method: str, boundaryCondition, truncation: float,
            outs: list) -> bool:
     """All components (or their sum / magnitude) from one read of `x` by the multi-output tile
     kernel, when it takes the case; False (nothing written) when the caller must filter per
     component.  Every component must resolve to the FIR method, as dip::Derivative would pick it."""
+    if not USE_MULTI_OUTPUT:
+        return False
     m = method[5:] if method[:5] == "gauss" else method
     for o in orders:
         if m == "best":

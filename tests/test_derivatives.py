@@ -111,13 +111,15 @@ def _launches():
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("case", range(len(MULTI_CASES)))
-def test_multi_output_kernel_matches_oracle(cuda, case):
+def test_multi_output_kernel_matches_oracle(cuda, case, monkeypatch):
     """Gradient, Hessian, Laplace and GradientMagnitude each from ONE launch of the multi-output
     tile kernel (counted by the library's launch counter), against the oracle's compositions of
     the restated GaussFIR (pinned bit-exact to the reference's own functions above)."""
     import torch
 
     import diplib_b200 as dip
+    from diplib_b200 import derivatives
+    monkeypatch.setattr(derivatives, "USE_MULTI_OUTPUT", True)
     shape, sg, bc, dt = MULTI_CASES[case]
     x = _input(shape, dt, 80 + case)
     xt = x                      # numpy in: staged to the device by the function, numpy out
@@ -191,12 +193,14 @@ def test_multi_output_products_through_the_c_abi(cuda):
 
 
 @pytest.mark.gpu
-def test_derivatives_fall_back_per_component_beyond_the_multi_kernel(cuda):
+def test_derivatives_fall_back_per_component_beyond_the_multi_kernel(cuda, monkeypatch):
     """Half-widths above 8 (sigma 4): the multi-output kernel declines and every component is its
     own GaussFIR call, still against the oracle."""
     import torch
 
     import diplib_b200 as dip
+    from diplib_b200 import derivatives
+    monkeypatch.setattr(derivatives, "USE_MULTI_OUTPUT", True)
     x = _input((40, 52), np.float32, 3)
     xt = torch.from_numpy(x).cuda()
     n0 = _launches()
