@@ -593,8 +593,67 @@ int fast_width( int64_t n, int per ) {
    return best;
 }
 
+// Short lines along the unit-stride axis (n <= 32 RX): a warp per line, lane l the outputs
+// l RX .. l RX + RX - 1 from a window of RX + 2 HB staged samples.  Each warp stages its next line
+// (asynchronous 4-byte copies, the boundary extension at the line ends) while it filters the
+// current one, in its own two buffers: no block barrier, many lines in flight per SM.
+constexpr int kXwWarps = 8;
+
+template< int HB, int RX, bool ODD >
+__global__ void __launch_bounds__( kXwWarps * 32 ) line_xw_kernel( LineFastArgs const __grid_constant__ a ) {
+   constexpr int WB = ( 32 * RX + 2 * HB + 3 ) / 4 * 4;     // buffer floats per line
+   __shared__ __align__( 16 ) float buf[ kXwWarps ][ 2 ][ WB ];
+   int const lane = static_cast< int >( threadIdx.x ) & 31, warp = static_cast< int >( threadIdx.x ) >> 5;
+   int64_t const gw = static_cast< int64_t >( blockIdx.x ) * kXwWarps + warp;
+   int64_t const nw = static_cast< int64_t >( gridDim.x ) * kXwWarps;
+   int64_t const sa = a.sst[ a.axis ], da = a.dstst[ a.axis ];
+   int const W = static_cast< int >( a.n ) + 2 * HB;
+   auto issue = [ & ]( int64_t u, float* b ) {
+      if( u < a.nouter ) {
+         int64_t sb, db;
+         fast_decode( a, u, sb, db );
+         for( int e = lane; e < W; e += 32 ) { fast_stage( a, b + e, sb, sa, e - HB ); }
+      }
+      asm volatile( "cp.async.commit_group;" ::: "memory" );
+   };
+   issue( gw, buf[ warp ][ 0 ] );
+   int k = 0;
+   for( int64_t u = gw; u < a.nouter; u += nw, ++k ) {
+      issue( u + nw, buf[ warp ][ ( k + 1 ) & 1 ] );
+      asm volatile( "cp.async.wait_group 1;" ::: "memory" );
+      __syncwarp();
+      int64_t sb, db;
+      fast_decode( a, u, sb, db );
+      float const* const w = buf[ warp ][ k & 1 ] + lane * RX;
+      float v[ RX + 2 * HB ];
+#pragma unroll
+      for( int q = 0; q < RX + 2 * HB; ++q ) { v[ q ] = w[ q ]; }
+#pragma unroll
+      for( int r = 0; r < RX; ++r ) {
+         int64_t const i = static_cast< int64_t >( lane ) * RX + r;
+         if( i < a.n ) { a.dst[ db + i * da ] = fast_tap_sum< HB, ODD >( a, v + HB + r ); }
+      }
+      __syncwarp();   // this buffer is refilled two lines later
+   }
+   asm volatile( "cp.async.wait_group 0;" ::: "memory" );
+}
+
+template< int HB, int RX >
+cudaError_t launch_xw( LineFastArgs const& a, cudaStream_t stream ) {
+   int64_t const want = static_cast< int64_t >( sm_count_line()) * 8;
+   int64_t const blocks = ( a.nouter + kXwWarps - 1 ) / kXwWarps;
+   int64_t const gx = blocks < want ? blocks : want;
+   if( a.odd ) { line_xw_kernel< HB, RX, true ><<< static_cast< unsigned >( gx ), kXwWarps * 32, 0, stream >>>( a ); }
+   else { line_xw_kernel< HB, RX, false ><<< static_cast< unsigned >( gx ), kXwWarps * 32, 0, stream >>>( a ); }
+   count_launch();
+   return cudaGetLastError();
+}
+
 template< int HB >
 cudaError_t launch_fast_bucket( LineFastArgs const& a, bool along, cudaStream_t stream ) {
+   if( along && a.n <= 256 && a.nouter >= 1024 ) {
+      return a.n <= 128 ? launch_xw< HB, 4 >( a, stream ) : launch_xw< HB, 8 >( a, stream );
+   }
    if( along ) {
       int const nt = fast_width( a.n, kRX );
       int64_t const gx = ( a.n + nt * kRX - 1 ) / ( nt * kRX );
