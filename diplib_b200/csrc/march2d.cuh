@@ -180,10 +180,11 @@ __device__ __forceinline__ float m2_src_sample( M2Image const& im, int b, int ro
 // sample at window offset 4 m + e feeds output t with tap d = 4 m + e - t - LEAD; pairs with
 // |d| > LEAD (the window's corners) are skipped at compile time, so each output takes 2 LEAD + 1
 // FMAs (taps beyond hx are zero).
-template< typename TIn, int LQ >
+template< typename TIn, int LQ, int HX = 4 * LQ >
 __device__ __forceinline__ void m2_xphase( unsigned char const* stage, int rs, int warp, int lane, float const* wx,
                                            float ( &acc )[ kM2R / 8 ][ 4 ] ) {
    constexpr int RW = kM2R / 8, NQ = 1 + 2 * LQ, LEAD = 4 * LQ;
+   static_assert( HX <= LEAD, "the window holds the taps" );
    int const cb = 4 * lane;
 #pragma unroll
    for( int m = 0; m < NQ; ++m ) {
@@ -199,7 +200,7 @@ __device__ __forceinline__ void m2_xphase( unsigned char const* stage, int rs, i
 #pragma unroll
             for( int t = 0; t < 4; ++t ) {
                int const d = 4 * m + e - t - LEAD;
-               if( d < -LEAD || d > LEAD ) { continue; }
+               if( d < -HX || d > HX ) { continue; }   // taps beyond hx are zero: skipped at compile time
                acc[ i ][ t ] = fmaf( wv[ 4 + e - t ], qv[ e ], acc[ i ][ t ] );   // wx[4 + 4m + e - t]
             }
          }
@@ -522,7 +523,21 @@ __global__ void __launch_bounds__( kM2NT, 2 ) march2d_kernel( M2Args const __gri
 #pragma unroll
                   for( int t = 0; t < 4; ++t ) { acc[ i ][ t ] = 0.f; }
                }
-               switch( lead / 4 ) {
+               // small half-widths exact (the window's LEAD is rounded up to the TMA granule, the
+               // taps beyond hx are not evaluated); from LEAD 16 on the window's taps
+               switch( lead == 4 * (( hx + 3 ) / 4 ) && hx <= 12 ? 100 + hx : lead / 4 ) {
+                  case 101: m2_xphase< TIn, 1, 1 >( stage, rs, warp, lane, wx, acc ); break;
+                  case 102: m2_xphase< TIn, 1, 2 >( stage, rs, warp, lane, wx, acc ); break;
+                  case 103: m2_xphase< TIn, 1, 3 >( stage, rs, warp, lane, wx, acc ); break;
+                  case 104: m2_xphase< TIn, 1, 4 >( stage, rs, warp, lane, wx, acc ); break;
+                  case 105: m2_xphase< TIn, 2, 5 >( stage, rs, warp, lane, wx, acc ); break;
+                  case 106: m2_xphase< TIn, 2, 6 >( stage, rs, warp, lane, wx, acc ); break;
+                  case 107: m2_xphase< TIn, 2, 7 >( stage, rs, warp, lane, wx, acc ); break;
+                  case 108: m2_xphase< TIn, 2, 8 >( stage, rs, warp, lane, wx, acc ); break;
+                  case 109: m2_xphase< TIn, 3, 9 >( stage, rs, warp, lane, wx, acc ); break;
+                  case 110: m2_xphase< TIn, 3, 10 >( stage, rs, warp, lane, wx, acc ); break;
+                  case 111: m2_xphase< TIn, 3, 11 >( stage, rs, warp, lane, wx, acc ); break;
+                  case 112: m2_xphase< TIn, 3, 12 >( stage, rs, warp, lane, wx, acc ); break;
                   case 1: m2_xphase< TIn, 1 >( stage, rs, warp, lane, wx, acc ); break;
                   case 2: m2_xphase< TIn, 2 >( stage, rs, warp, lane, wx, acc ); break;
                   case 3: m2_xphase< TIn, 3 >( stage, rs, warp, lane, wx, acc ); break;
