@@ -8,7 +8,9 @@
 // the part of C^T y_bar that falls on the 2h halo positions is folded back onto the samples each
 // halo sample was made from, with the coefficients of E (host-computed from the same boundary code
 // the forward uses).  fold_kernel does that fold, one thread per line, or two (one per halo
-// side) when the two sides fold onto disjoint samples.
+// side) when the two sides fold onto disjoint samples; fold_fast_kernel, for float images whose
+// halo positions each take one sample (the index mappings on lines longer than twice the
+// half-width), keeps a side's samples and the taps in registers.
 //
 // dot_kernel reduces <a, b> over an image in double: the sigma gradient of axis a is
 // <y_bar, G_a'(x)>, with G_a' the forward filter whose axis-a taps are d(taps)/d(sigma).
@@ -105,6 +107,106 @@ __global__ void __launch_bounds__( 256 ) dot_kernel( ConvertArgs const __grid_co
    }
 }
 
+// Fast fold for single-source boundary conditions (every halo position takes one sample, as the
+// index mappings do when the line is longer than the half-width) and float images: a thread per
+// line side keeps the side's HB samples of g and the taps in registers; halo position k (k = 1..h
+// beyond the end) gathers z_k = sum_m w(k + m) g_m over the side's samples m = 0..h - k (m counted
+// from the end inwards) and adds c_k z_k to its source sample.  The same sums and targets as
+// fold_kernel, in float.
+template< int HB >
+struct FoldFastArgs {
+   float const* g;
+   float* xb;
+   int32_t ndims, axis;
+   int64_t sizes[ DIPCU_MAX_DIMS ];
+   int64_t gst[ DIPCU_MAX_DIMS ], xst[ DIPCU_MAX_DIMS ];
+   int64_t n, nlines;
+   int32_t h, odd;
+   float w[ HB + 1 ];                 // forward taps, centre first, zero beyond h
+   int32_t src[ 2 ][ HB ];            // [side][k - 1]: source sample of halo position k
+   float c[ 2 ][ HB ];                // its coefficient (0 beyond h)
+};
+
+template< int HB >
+__global__ void __launch_bounds__( 128 ) fold_fast_kernel( FoldFastArgs< HB > const __grid_constant__ a ) {
+   int64_t const tid = static_cast< int64_t >( blockIdx.x ) * blockDim.x + threadIdx.x;
+   int64_t const line = tid >> 1;
+   int const side = static_cast< int >( tid & 1 );     // 0: before sample 0, 1: after sample n - 1
+   if( line >= a.nlines ) { return; }
+   int64_t rem = line, gb = 0, xbb = 0;
+   for( int d = 0; d < a.ndims; ++d ) {
+      if( d == a.axis ) { continue; }
+      int64_t const c = rem % a.sizes[ d ];
+      rem /= a.sizes[ d ];
+      gb += c * a.gst[ d ];
+      xbb += c * a.xst[ d ];
+   }
+   int64_t const gs = a.gst[ a.axis ], xs = a.xst[ a.axis ];
+   // side samples, counted from the end inwards: m -> line sample m (side 0) or n - 1 - m (side 1)
+   int64_t const g0 = side ? gb + ( a.n - 1 ) * gs : gb;
+   int64_t const gstep = side ? -gs : gs;
+   float gv[ HB ];
+#pragma unroll
+   for( int m = 0; m < HB; ++m ) { gv[ m ] = m < a.h ? a.g[ g0 + m * gstep ] : 0.f; }
+   // the tap between halo position k (k beyond the end) and side sample m is at distance k + m; an
+   // odd kernel's tap w(j - t) has the sign of j - t: negative before the line, positive after it
+   float const sg = ( a.odd && !side ) ? -1.f : 1.f;
+#pragma unroll
+   for( int k = 1; k <= HB; ++k ) {
+      if( k > a.h ) { break; }
+      float z = 0.f;
+#pragma unroll
+      for( int m = 0; m + k <= HB; ++m ) { z = fmaf( a.w[ k + m ], gv[ m ], z ); }
+      float* const p = a.xb + xbb + static_cast< int64_t >( a.src[ side ][ k - 1 ] ) * xs;
+      *p += a.c[ side ][ k - 1 ] * sg * z;
+   }
+}
+
+// The fast fold when its conditions hold; cudaErrorNotSupported otherwise.
+template< int HB >
+cudaError_t run_fold_fast( FoldPass const& p, cudaStream_t s ) {
+   FoldFastArgs< HB > a{};
+   int64_t const n = p.sizes[ p.axis ];
+   if( p.compute_double || p.h < 1 || p.h > HB || n <= 2 * p.h || p.nentries != 2 * p.h ) { return cudaErrorNotSupported; }
+   for( int k = 0; k < p.nentries; ++k ) {
+      FoldEntry const& e = p.entries[ k ];
+      int side, kk;
+      if( e.j < 0 ) { side = 0; kk = -e.j; } else { side = 1; kk = static_cast< int >( e.j - ( n - 1 )); }
+      if( kk < 1 || kk > p.h || a.c[ side ][ kk - 1 ] != 0.f || e.c == 0.0 ) { return cudaErrorNotSupported; }   // one source per position
+      a.src[ side ][ kk - 1 ] = static_cast< int32_t >( e.i );
+      a.c[ side ][ kk - 1 ] = static_cast< float >( e.c );
+   }
+   for( int side = 0; side < 2; ++side ) {
+      for( int k = 0; k < p.h; ++k ) { if( a.c[ side ][ k ] == 0.f ) { return cudaErrorNotSupported; } }
+   }
+   // the two sides must fold onto disjoint samples (the two threads of a line write without atomics;
+   // within a side one thread does every read-modify-write in order)
+   for( int k = 0; k < p.h; ++k ) {
+      for( int m = 0; m < p.h; ++m ) {
+         if( a.src[ 0 ][ k ] == a.src[ 1 ][ m ] ) { return cudaErrorNotSupported; }
+      }
+   }
+   a.g = static_cast< float const* >( p.g );
+   a.xb = static_cast< float* >( p.xb );
+   a.ndims = p.ndims;
+   a.axis = p.axis;
+   a.n = n;
+   a.nlines = 1;
+   for( int d = 0; d < p.ndims; ++d ) {
+      a.sizes[ d ] = p.sizes[ d ];
+      a.gst[ d ] = p.gst[ d ];
+      a.xst[ d ] = p.xst[ d ];
+      if( d != p.axis ) { a.nlines *= p.sizes[ d ]; }
+   }
+   a.h = static_cast< int32_t >( p.h );
+   a.odd = p.odd;
+   for( int k = 0; k <= HB; ++k ) { a.w[ k ] = k <= p.h ? static_cast< float >( p.taps[ k ] ) : 0.f; }
+   int64_t const blocks = ( 2 * a.nlines + 127 ) / 128;
+   if( blocks > 0x7fffffff ) { return cudaErrorInvalidValue; }
+   fold_fast_kernel< HB ><<< static_cast< unsigned >( blocks ), 128, 0, s >>>( a ); count_launch();
+   return cudaGetLastError();
+}
+
 template< typename T >
 cudaError_t run_fold( FoldPass const& p, cudaStream_t s ) {
    FoldArgs< T > a{};
@@ -149,6 +251,11 @@ cudaError_t run_fold( FoldPass const& p, cudaStream_t s ) {
 
 cudaError_t launch_fold( FoldPass const& p, cudaStream_t stream ) {
    if( p.h < 0 || p.h > kFoldMaxHalf || p.nentries > kFoldMaxEntries ) { return cudaErrorInvalidValue; }
+   if( !p.compute_double && p.h >= 1 && p.h <= 16 ) {
+      cudaError_t const e = p.h <= 4 ? run_fold_fast< 4 >( p, stream ) : p.h <= 8 ? run_fold_fast< 8 >( p, stream )
+                                                                          : run_fold_fast< 16 >( p, stream );
+      if( e != cudaErrorNotSupported ) { return e; }
+   }
    return p.compute_double ? run_fold< double >( p, stream ) : run_fold< float >( p, stream );
 }
 

@@ -182,15 +182,16 @@ __device__ __forceinline__ void fast_decode( LineFastArgs const& a, int64_t u, i
    }
 }
 
+// Four partial sums (taps k mod 4), so that consecutive FMAs of one output do not wait on each other.
 template< int HB, bool ODD >
 __device__ __forceinline__ float fast_tap_sum( LineFastArgs const& a, float const* v ) {   // v[0] is the centre
-   float s0 = ODD ? 0.f : a.taps[ 0 ] * v[ 0 ], s1 = 0.f;
+   float s[ 4 ] = { ODD ? 0.f : a.taps[ 0 ] * v[ 0 ], 0.f, 0.f, 0.f };
 #pragma unroll
    for( int k = 1; k <= HB; ++k ) {
       float const p = ODD ? v[ k ] - v[ -k ] : v[ k ] + v[ -k ];
-      if( k & 1 ) { s1 = fmaf( a.taps[ k ], p, s1 ); } else { s0 = fmaf( a.taps[ k ], p, s0 ); }
+      s[ k & 3 ] = fmaf( a.taps[ k ], p, s[ k & 3 ] );
    }
-   return s0 + s1;
+   return ( s[ 0 ] + s[ 1 ] ) + ( s[ 2 ] + s[ 3 ] );
 }
 
 // Stages sample j of a line into `dst` (shared memory): an asynchronous 4-byte copy for samples
