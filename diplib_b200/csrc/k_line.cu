@@ -609,11 +609,26 @@ __global__ void __launch_bounds__( kXwWarps * 32 ) line_xw_kernel( LineFastArgs 
    int64_t const nw = static_cast< int64_t >( gridDim.x ) * kXwWarps;
    int64_t const sa = a.sst[ a.axis ], da = a.dstst[ a.axis ];
    int const W = static_cast< int >( a.n ) + 2 * HB;
+   static_assert( HB % 4 == 0 && RX % 4 == 0, "16-byte aligned staging and window reads" );
    auto issue = [ & ]( int64_t u, float* b ) {
       if( u < a.nouter ) {
          int64_t sb, db;
          fast_decode( a, u, sb, db );
-         for( int e = lane; e < W; e += 32 ) { fast_stage( a, b + e, sb, sa, e - HB ); }
+         // the line's 4-sample groups by 16-byte copies where its first sample is so aligned; the
+         // rest (boundary extension, tail) sample by sample
+         int e0 = 0, e1 = 0;                                  // [e0, e1): samples staged by the 16-byte copies
+         if( sa == 1 && ( reinterpret_cast< uintptr_t >( a.src + sb ) & 15 ) == 0 ) {
+            e1 = static_cast< int >( a.n ) & ~3;
+            for( int q = lane; 4 * q < e1; q += 32 ) {
+               asm volatile( "cp.async.cg.shared.global [%0], [%1], 16;" :: "r"( smem_u32( b + HB + 4 * q )),
+                             "l"( a.src + sb + 4 * q ) : "memory" );
+            }
+         }
+         for( int e = lane; e < W; e += 32 ) {
+            int const i = e - HB;
+            if( i >= e0 && i < e1 ) { continue; }
+            fast_stage( a, b + e, sb, sa, i );
+         }
       }
       asm volatile( "cp.async.commit_group;" ::: "memory" );
    };
@@ -625,10 +640,13 @@ __global__ void __launch_bounds__( kXwWarps * 32 ) line_xw_kernel( LineFastArgs 
       __syncwarp();
       int64_t sb, db;
       fast_decode( a, u, sb, db );
-      float const* const w = buf[ warp ][ k & 1 ] + lane * RX;
+      float4 const* const w4 = reinterpret_cast< float4 const* >( buf[ warp ][ k & 1 ] + lane * RX );
       float v[ RX + 2 * HB ];
 #pragma unroll
-      for( int q = 0; q < RX + 2 * HB; ++q ) { v[ q ] = w[ q ]; }
+      for( int q = 0; q < ( RX + 2 * HB ) / 4; ++q ) {
+         float4 const f = w4[ q ];
+         v[ 4 * q ] = f.x; v[ 4 * q + 1 ] = f.y; v[ 4 * q + 2 ] = f.z; v[ 4 * q + 3 ] = f.w;
+      }
 #pragma unroll
       for( int r = 0; r < RX; ++r ) {
          int64_t const i = static_cast< int64_t >( lane ) * RX + r;
