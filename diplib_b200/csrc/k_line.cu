@@ -596,20 +596,38 @@ int fast_width( int64_t n, int per ) {
 
 // Short lines along the unit-stride axis (n <= 32 RX): a warp per line, lane l the outputs
 // l RX .. l RX + RX - 1 from a window of RX + 2 HB staged samples.  Each warp stages its next line
-// (asynchronous 4-byte copies, the boundary extension at the line ends) while it filters the
-// current one, in its own two buffers: no block barrier, many lines in flight per SM.
+// (16-byte asynchronous copies, the boundary extension at the line ends sample by sample) three
+// lines ahead of the one it filters, in its own buffers: no block barrier, many lines in flight.
 constexpr int kXwWarps = 8;
+constexpr int kXwBuf = 4;           // line buffers per warp: three lines in flight while one is filtered
 
 template< int HB, int RX, bool ODD >
 __global__ void __launch_bounds__( kXwWarps * 32 ) line_xw_kernel( LineFastArgs const __grid_constant__ a ) {
    constexpr int WB = ( 32 * RX + 2 * HB + 3 ) / 4 * 4;     // buffer floats per line
-   __shared__ __align__( 16 ) float buf[ kXwWarps ][ 2 ][ WB ];
+   __shared__ __align__( 16 ) float buf[ kXwWarps ][ kXwBuf ][ WB ];
    int const lane = static_cast< int >( threadIdx.x ) & 31, warp = static_cast< int >( threadIdx.x ) >> 5;
    int64_t const gw = static_cast< int64_t >( blockIdx.x ) * kXwWarps + warp;
    int64_t const nw = static_cast< int64_t >( gridDim.x ) * kXwWarps;
    int64_t const sa = a.sst[ a.axis ], da = a.dstst[ a.axis ];
    int const W = static_cast< int >( a.n ) + 2 * HB;
    static_assert( HB % 4 == 0 && RX % 4 == 0, "16-byte aligned staging and window reads" );
+   // The boundary extension is the same for every line: its source samples once per CTA
+   // (sample index, -1 for a zero, bit 30 for a negated sample).
+   __shared__ int32_t smap[ WB ];
+   for( int e = static_cast< int >( threadIdx.x ); e < W; e += kXwWarps * 32 ) {
+      int64_t const i = e - HB;
+      int32_t m = static_cast< int32_t >( i );
+      if( i < 0 || i >= a.n ) {
+         if( a.bc == BC_ADD_ZEROS ) { m = -1; }
+         else {
+            bool neg;
+            m = static_cast< int32_t >( bc_map_index( i, a.n, a.bc, &neg ));
+            if( neg ) { m |= 1 << 30; }
+         }
+      }
+      smap[ e ] = m;
+   }
+   __syncthreads();
    auto issue = [ & ]( int64_t u, float* b ) {
       if( u < a.nouter ) {
          int64_t sb, db;
@@ -627,20 +645,25 @@ __global__ void __launch_bounds__( kXwWarps * 32 ) line_xw_kernel( LineFastArgs 
          for( int e = lane; e < W; e += 32 ) {
             int const i = e - HB;
             if( i >= e0 && i < e1 ) { continue; }
-            fast_stage( a, b + e, sb, sa, i );
+            int32_t const m = smap[ e ];
+            float const* const src = a.src + sb + static_cast< int64_t >( m & ~( 1 << 30 )) * sa;
+            if( m < 0 ) { b[ e ] = 0.f; }
+            else if( m & ( 1 << 30 )) { b[ e ] = -__ldg( src ); }
+            else { asm volatile( "cp.async.ca.shared.global [%0], [%1], 4;" :: "r"( smem_u32( b + e )), "l"( src ) : "memory" ); }
          }
       }
       asm volatile( "cp.async.commit_group;" ::: "memory" );
    };
-   issue( gw, buf[ warp ][ 0 ] );
+#pragma unroll
+   for( int j = 0; j < kXwBuf - 1; ++j ) { issue( gw + j * nw, buf[ warp ][ j ] ); }
    int k = 0;
    for( int64_t u = gw; u < a.nouter; u += nw, ++k ) {
-      issue( u + nw, buf[ warp ][ ( k + 1 ) & 1 ] );
-      asm volatile( "cp.async.wait_group 1;" ::: "memory" );
+      issue( u + ( kXwBuf - 1 ) * nw, buf[ warp ][ ( k + kXwBuf - 1 ) % kXwBuf ] );
+      asm volatile( "cp.async.wait_group %0;" :: "n"( kXwBuf - 1 ) : "memory" );
       __syncwarp();
       int64_t sb, db;
       fast_decode( a, u, sb, db );
-      float4 const* const w4 = reinterpret_cast< float4 const* >( buf[ warp ][ k & 1 ] + lane * RX );
+      float4 const* const w4 = reinterpret_cast< float4 const* >( buf[ warp ][ k % kXwBuf ] + lane * RX );
       float v[ RX + 2 * HB ];
 #pragma unroll
       for( int q = 0; q < ( RX + 2 * HB ) / 4; ++q ) {
@@ -652,7 +675,7 @@ __global__ void __launch_bounds__( kXwWarps * 32 ) line_xw_kernel( LineFastArgs 
          int64_t const i = static_cast< int64_t >( lane ) * RX + r;
          if( i < a.n ) { a.dst[ db + i * da ] = fast_tap_sum< HB, ODD >( a, v + HB + r ); }
       }
-      __syncwarp();   // this buffer is refilled two lines later
+      __syncwarp();   // this buffer is refilled kXwBuf lines later
    }
    asm volatile( "cp.async.wait_group 0;" ::: "memory" );
 }
