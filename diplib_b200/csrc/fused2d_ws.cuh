@@ -116,6 +116,10 @@ __global__ void __launch_bounds__( W2Geom< TIn, B, TYP >::NT, 2 ) fused2d_ws_ker
    uint32_t* const xfix = reinterpret_cast< uint32_t* >( rsgn + BH );            // [XFIX_MAX]
    float* const ot = reinterpret_cast< float* >( smem + G::OFF_OT + warp * G::OT_BYTES );   // [TY][TX]
 
+   // Programmatic dependent launch: the next launch in the stream may be scheduled now, and this
+   // grid touches global memory only once the previous one has completed and its writes are visible.
+   asm volatile( "griddepcontrol.launch_dependents;" ::: "memory" );
+   asm volatile( "griddepcontrol.wait;" ::: "memory" );
    if( tid == 0 ) { *abort = 0; }
    if( lane == 0 ) {
       for( int d = 0; d < SPW; ++d ) { mbar_init( &full[ d ], 1 ); }

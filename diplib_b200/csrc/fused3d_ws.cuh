@@ -208,6 +208,10 @@ __global__ void __launch_bounds__( W5Geom< TIn, HX, HY, HZ >::NT, W5Geom< TIn, H
       fence_mbar_init();
    }
    __syncthreads();
+   // Programmatic dependent launch: the next launch in the stream may be scheduled now; global
+   // memory is touched only after the previous grid has completed and its writes are visible.
+   asm volatile( "griddepcontrol.launch_dependents;" ::: "memory" );
+   asm volatile( "griddepcontrol.wait;" ::: "memory" );
 
    int const nx = a.n[ 0 ], ny = a.n[ 1 ], nz = a.n[ 2 ];
    int64_t const ub = ( static_cast< int64_t >( blockIdx.x ) * a.units ) / gridDim.x;

@@ -255,7 +255,19 @@ cudaError_t run3d_ws( FusedArgs& a, cudaStream_t s ) {
       int64_t max_ctas = z.units / ( 4 * HZ + 4 );   // keep chunks long against the 2*HZ halo planes
       if( nctas > max_ctas ) { nctas = max_ctas; }
       if( nctas < 1 ) { nctas = 1; }
-      kern<<< static_cast< unsigned >( nctas ), G::NT, smem, s >>>( z ); count_launch();
+      cudaLaunchConfig_t cfg{};
+      cfg.gridDim = dim3( static_cast< unsigned >( nctas ));
+      cfg.blockDim = dim3( G::NT );
+      cfg.dynamicSmemBytes = smem;
+      cfg.stream = s;
+      cudaLaunchAttribute attr[ 1 ];
+      attr[ 0 ].id = cudaLaunchAttributeProgrammaticStreamSerialization;   // see the 2D launch
+      attr[ 0 ].val.programmaticStreamSerializationAllowed = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      cudaError_t const le = cudaLaunchKernelEx( &cfg, kern, z );
+      count_launch();
+      if( le != cudaSuccess ) { return le; }
       return cudaGetLastError();
    }
 }
@@ -327,7 +339,23 @@ cudaError_t run2d_ws( FusedArgs& a, int32_t const* odd, cudaStream_t s ) {
    int64_t const need = ( z.ntiles + G::NW - 1 ) / G::NW;
    if( nctas > need ) { nctas = need; }
    if( nctas < 1 ) { nctas = 1; }
-   kern<<< static_cast< unsigned >( nctas ), G::NT, smem, s >>>( z ); count_launch();
+   {
+      // launched as a programmatic dependent of the previous kernel in the stream (the kernel waits
+      // for it before touching memory), so consecutive filters overlap their launch latency
+      cudaLaunchConfig_t cfg{};
+      cfg.gridDim = dim3( static_cast< unsigned >( nctas ));
+      cfg.blockDim = dim3( G::NT );
+      cfg.dynamicSmemBytes = smem;
+      cfg.stream = s;
+      cudaLaunchAttribute attr[ 1 ];
+      attr[ 0 ].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+      attr[ 0 ].val.programmaticStreamSerializationAllowed = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      cudaError_t const le = cudaLaunchKernelEx( &cfg, kern, z );
+      count_launch();
+      if( le != cudaSuccess ) { return le; }
+   }
    return cudaGetLastError();
 }
 
