@@ -632,8 +632,8 @@ B_SIGMAS = [0.8, 1.0, 2.0, 4.0, 8.0]
 B_BCS = ["mirror", "periodic", "add zeros"]
 B_CONFIG = {"workload": "batched dip::GaussFIR: 512 2D sfloat images, sides uniform 64..2048, sigma from "
                         "{0.8,1,2,4,8} per image, order per axis from {0,1,2}, boundary from {mirror, periodic, "
-                        "add zeros}, truncation 3; weights, the persistent tile kernel and the grouped "
-                        "warp-per-tile launches replayed as one CUDA graph, autotuned tiles",
+                        "add zeros}, truncation 3; the weights kernel and one persistent row-march launch over a "
+                        "device work queue, replayed as one CUDA graph, row runs autotuned per y half-width",
             "l2": "the batch holds 2.3 GB of input and 2.3 GB of output (> 126 MB L2)"}
 
 
@@ -676,7 +676,7 @@ def run_batch(args, embedded=False):
     line["config"]["plan"] = plan.info()
     ach = 8 * npx / (avg * 1e-3) / 1e9
     line["roofline"] = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
-                        "traffic": None, "peak_source": kind, "kernel": "whole batch run (grouped tile and line kernels)",
+                        "traffic": None, "peak_source": kind, "kernel": "whole batch run (weights + the persistent row-march launch)",
                         "bytes_per_voxel": 8, "avg_kernel_ms": avg}
     line["clocks"] = clk
     line["gpu_launches"] = plan.info()["kernels_per_run"] * args.steps   # all kernels of the captured graph
