@@ -185,6 +185,17 @@ def traffic_from_profiles():
     return None
 
 
+def read_overfetch_from_profiles(input_bytes):
+    """DRAM bytes read per headline launch (ncu) over the input's bytes: the halo re-reads."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            r = json.load(f).get("fused3d_u16_256_read_bytes_per_launch")
+        if r:
+            return r / input_bytes
+    return None
+
+
 def run_reference_arm(args):
     if int(os.environ.get("RANK", "0")) != 0:
         return 0
@@ -307,6 +318,7 @@ def run_gpu_arm(args):
         "config": dict(CONFIG, parallelism=f"replicas x{world}" if world > 1 else "single GPU"),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic_from_profiles(), "peak_source": peak_kind,
+                     "read_overfetch": read_overfetch_from_profiles(2 * int(np.prod(SHAPE))),
                      "kernel": "fused3d_ws_kernel (warp-specialised z-marching tile kernel)", "bytes_per_voxel": BYTES_PER_VOXEL,
                      "avg_kernel_ms": avg_kernel_ms},
         "e2e": e2e,
