@@ -1,7 +1,8 @@
 """Generates tests/golden/*.npz from the reference itself (oracle/_ref/libdipref.so, the
 unmodified DIPlib sources compiled by oracle/Makefile).  Run where the reference tree exists:
 
-    make -C oracle ref && python tests/golden/make_golden.py
+    make -C oracle ref && python tests/golden/make_golden.py            # every fixture
+    python tests/golden/make_golden.py --iir-only                       # gauss_iir_ref.npz alone
 
 The fixtures pin the C restatement (oracle/gauss_oracle.c) and the CUDA path on machines
 without the reference tree.  Inputs are regenerated from the stored seeds and shapes.
@@ -57,9 +58,36 @@ CASES = [
 ]
 
 
+# dip::GaussIIR cases: (name, seed, shape, dtype, sigmas, orders, bc list, filter orders, design)
+IIR_CASES = [
+    ("iir_d0_dtf", 31, (60, 70), "float32", [12.0, 3.0], [0, 0], ["mirror"], [], "discrete time fit"),
+    ("iir_d1_fb", 32, (45, 50), "uint16", [5.0, 11.0], [1, 0], ["periodic", "add zeros"], [], "forward backward"),
+    ("iir_d2_3d", 33, (14, 18, 22), "float64", [2.0, 6.0, 4.0], [2, 0, 1], ["asym mirror", "zero order", "third order"],
+     [], "discrete time fit"),
+    ("iir_d3_orders", 34, (40, 33), "float32", [7.0, 2.5], [3, 4], ["first order", "second order"], [4, 3],
+     "discrete time fit"),
+    ("iir_short", 35, (9, 200), "int32", [15.0, 1.5], [0, 1], ["antisym reflect", "asym periodic"], [1, 2],
+     "forward backward"),
+]
+
+
+def make_iir() -> None:
+    """gauss_iir_ref.npz only (the other fixtures untouched)."""
+    out = {}
+    for name, seed, shape, dtype, sig, ords, bcs, fo, dm in IIR_CASES:
+        x = make_input(seed, shape, dtype)
+        out[name] = oracle.ref_gauss_iir(x, sig, ords, bcs, fo, dm)
+    np.savez_compressed(os.path.join(HERE, "gauss_iir_ref.npz"), **out)
+
+
 def main() -> None:
     if not oracle.ref_available():
         raise SystemExit("oracle/_ref/libdipref.so is not built")
+    if "--iir-only" in sys.argv:
+        make_iir()
+        print("written to", HERE)
+        return
+    make_iir()
     out = {}
     for name, seed, shape, dtype, sig, ords, bcs, trunc in CASES:
         x = make_input(seed, shape, dtype)

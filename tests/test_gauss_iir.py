@@ -150,3 +150,32 @@ def test_gauss_iir_through_the_c_abi_with_strides_and_protected_output(cuda):
     assert _abi.lib().dipcu_gauss_iir(ctypes.byref(image_desc(xt)), ctypes.byref(image_desc(out)),
                                       (ctypes.c_double * 2)(*sg), (ctypes.c_uint32 * 2)(5, 0),
                                       (ctypes.c_int32 * 2)(*bcs), None, 0, 3.0, None) == _abi.ERR_INVALID_ARG
+
+
+def test_oracle_iir_matches_golden_fixtures():
+    """The restatement against fixtures generated from the compiled dip::GaussIIR
+    (tests/golden/make_golden.py): bit-exact, with no reference tree needed."""
+    import os
+
+    from tests.golden.make_golden import IIR_CASES, make_input
+    ref = np.load(os.path.join(os.path.dirname(__file__), "golden", "gauss_iir_ref.npz"))
+    for name, seed, shape, dtype, sig, ords, bcs, fo, dm in IIR_CASES:
+        x = make_input(seed, shape, dtype)
+        got = oracle.gauss_iir(x, sig, ords, bcs, fo or None, dm)
+        assert got.dtype == ref[name].dtype, name
+        assert np.array_equal(got, ref[name], equal_nan=True), (name, float(np.nanmax(np.abs(got - ref[name]))))
+
+
+@pytest.mark.gpu
+def test_gauss_iir_device_matches_golden_fixtures(cuda):
+    """The device filter against the reference's own outputs (golden fixtures), at the float bar."""
+    import os
+
+    import diplib_b200 as dip
+    from tests.golden.make_golden import IIR_CASES, make_input
+    ref = np.load(os.path.join(os.path.dirname(__file__), "golden", "gauss_iir_ref.npz"))
+    for name, seed, shape, dtype, sig, ords, bcs, fo, dm in IIR_CASES:
+        x = make_input(seed, shape, dtype)
+        got = dip.GaussIIR(x, sig, ords, bcs, fo, dm)
+        tol = 1e-5 * max(1.0, float(x.max()) - float(x.min()))
+        assert got.dtype == ref[name].dtype and np.abs(got.astype(np.float64) - ref[name]).max() <= tol, name
